@@ -1,0 +1,335 @@
+/*
+ * anu_pdhg.h - C ABI of the B200 (sm_100a) PDHG / PDLP engine.
+ *
+ * Drop-in for the first-order LP path of anukulan:
+ *   - solve_pdhg(const StandardLp&, const PdhgOptions&)   src/anukulan/pdhg.hpp:543
+ *   - evaluate_residual(lp, x, y)                         src/anukulan/pdhg.hpp:548
+ *   - estimate_matrix_norm(lp, iterations, tolerance)     src/anukulan/pdhg.hpp:580
+ *   - the LinAlgBackend seam                              src/anukulan/backend.hpp:24-215
+ * plus the batched case stack, the packed uneven batch and the adjoint, which
+ * have no counterpart in the reference.
+ *
+ * Conventions (all entry points):
+ *   - C linkage, plain pointers and sizes, no exceptions across the boundary.
+ *   - Every function returns an int status: ANU_OK (0) or an ANU_ERR_* code.
+ *     The message of the last failure on the calling thread is returned by
+ *     anu_last_error(). The reference throws std::runtime_error from
+ *     cuda_check (src/anukulan/cuda_backend.cu:32-37); here that becomes
+ *     ANU_ERR_CUDA plus the message.
+ *   - Host pointers unless the name says "device". Inputs are copied; the
+ *     caller keeps ownership of every array it passes.
+ *   - One CUDA stream per handle. A handle is not thread safe; distinct
+ *     handles may be used from distinct threads.
+ *   - There is no CPU fallback: without a usable CUDA device every compute
+ *     entry point returns ANU_ERR_NO_DEVICE.
+ */
+#ifndef ANU_PDHG_H
+#define ANU_PDHG_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ANU_PDHG_ABI_VERSION 1
+
+/* Return codes. */
+enum {
+  ANU_OK = 0,
+  ANU_ERR_INVALID = 1,   /* bad argument, shape or option */
+  ANU_ERR_CUDA = 2,      /* a CUDA runtime call failed */
+  ANU_ERR_NO_DEVICE = 3, /* no CUDA device */
+  ANU_ERR_MEMORY = 4,    /* device or host allocation failed */
+  ANU_ERR_DEVICE_WAIT = 5, /* a bounded device-side wait gave up */
+  ANU_ERR_INTERNAL = 6
+};
+
+/* PdhgStatus, src/anukulan/pdhg.hpp:417-423 (same order). */
+enum {
+  ANU_PDHG_OPTIMAL = 0,
+  ANU_PDHG_PRIMAL_INFEASIBLE = 1,
+  ANU_PDHG_ITERATION_LIMIT = 2,
+  ANU_PDHG_TIME_LIMIT = 3,
+  ANU_PDHG_NUMERICAL_ERROR = 4
+};
+
+/* PdhgOptions::Termination, src/anukulan/pdhg.hpp:372-373. */
+enum {
+  ANU_TERMINATION_FULL = 0,
+  ANU_TERMINATION_PRIMAL_FEASIBILITY = 1,
+  ANU_TERMINATION_DUAL_FEASIBILITY = 2
+};
+
+/* Arithmetic of the iteration (no counterpart in the reference, which is
+ * FP64 throughout). */
+enum {
+  ANU_PRECISION_FP64 = 0, /* matrix and iterates in FP64 */
+  ANU_PRECISION_FP32 = 1  /* matrix and iterates in FP32; checks, restart and
+                             termination decisions and refinement in FP64 */
+};
+
+/* Compressed sparse rows, SparseMatrix (src/anukulan/sparse.hpp:37-101):
+ * start[rows+1], index[nnz] (column indices, sorted and unique within a row),
+ * value[nnz]. Int is int32 as in the reference (sparse.hpp:11). */
+typedef struct anu_csr {
+  int32_t rows;
+  int32_t cols;
+  int32_t nnz;
+  const int32_t* start;
+  const int32_t* index;
+  const double* value;
+} anu_csr;
+
+/* StandardLp, src/anukulan/standard_form.hpp:23-66:
+ *   min c'x  s.t.  K_eq x = q_eq (first num_equalities rows),
+ *                  K_ineq x >= q_ineq (the rest),  lower <= x <= upper.
+ * Infinite bounds are +-INFINITY. The transpose the reference caches in
+ * StandardLp::kt is built by the engine. */
+typedef struct anu_lp {
+  anu_csr k;
+  const double* c;     /* n */
+  const double* q;     /* m */
+  const double* lower; /* n */
+  const double* upper; /* n */
+  int32_t num_equalities;
+  double objective_scale;  /* model objective = scale * c'x + offset */
+  double objective_offset;
+} anu_lp;
+
+/* PdhgOptions, src/anukulan/pdhg.hpp:19-415, field for field (bools as
+ * int32 0/1), followed by the engine's own additions. Fill it with
+ * anu_pdhg_default_options() and then change what differs. */
+typedef struct anu_pdhg_options {
+  double tolerance;                       /* 1e-6 */
+  double gap_tolerance;                   /* 0: same as tolerance */
+  int32_t max_iterations;                 /* 200000 */
+  double time_limit_seconds;              /* 300 */
+  int32_t termination_check_frequency;    /* 40 */
+  double absolute_tolerance;              /* 0 */
+  int32_t require_inf_norm_termination;   /* 1 */
+  int32_t adaptive_step_size;             /* 1 */
+  int32_t primal_weight_updates;          /* 1 */
+  int32_t restarts;                       /* 1 */
+  int32_t halpern;                        /* 1 */
+  int32_t halpern_restart;                /* 0 */
+  int32_t halpern_minimum_epoch;          /* 16 */
+  int32_t polish_feasibility;             /* 1 */
+  int32_t polish_first_iteration;         /* 100 */
+  double polish_iteration_factor;         /* 0.125 */
+  int32_t polish_minimum_iterations;      /* 40 */
+  int32_t polish_maximum_iterations;      /* 20000 */
+  int32_t polish_on_exit;                 /* 1 */
+  double reflection;                      /* 1.0 */
+  int32_t constant_step_size;             /* 1 */
+  double constant_step_scale;             /* 0.90 */
+  int32_t restart_on_fixed_point;         /* 1 */
+  int32_t pid_primal_weight;              /* 1 */
+  double primal_weight_kp;                /* 0.5 */
+  double primal_weight_ki;                /* 0.0 */
+  double primal_weight_kd;                /* 0.3 */
+  int32_t ruiz_iterations;                /* ScalingOptions: 10 */
+  int32_t pock_chambolle;                 /* ScalingOptions: 1 */
+  int32_t reuse_products;                 /* 1 */
+  int32_t detect_infeasibility;           /* 1 */
+  double infeasibility_tolerance;         /* 1e-8 */
+  int32_t termination;                    /* ANU_TERMINATION_FULL */
+  double known_matrix_norm;               /* 0: estimate it */
+  double initial_step_size;               /* 0: derive it */
+  double initial_primal_weight;           /* 0: derive it */
+  int32_t verbose;                        /* 0 */
+  int32_t log_frequency;                  /* 5000 */
+  /* PdhgOptions::stop: when *stop becomes nonzero the solve ends at the next
+   * check with ANU_PDHG_TIME_LIMIT. NULL: no cancellation. */
+  const volatile int32_t* stop;
+
+  /* --- engine additions, no counterpart in PdhgOptions --- */
+  int32_t precision;            /* ANU_PRECISION_FP64 (default) or _FP32 */
+  /* Outer iterative-refinement rounds after the first solve (FP32 only).
+   * Each round re-solves a correction LP built from the FP64 residuals of the
+   * current point. 0 = none. */
+  int32_t refinement_rounds;    /* 0 */
+  /* Relative KKT tolerance of each inner solve when refining; 0 means
+   * max(tolerance, 1e-6). */
+  double refinement_inner_tolerance;
+  int32_t device;               /* CUDA device ordinal, 0 */
+  int32_t use_graphs;           /* capture iteration chunks in CUDA graphs, 1 */
+} anu_pdhg_options;
+
+/* PdhgResidual, src/anukulan/pdhg.hpp:429-496. */
+typedef struct anu_pdhg_residual {
+  double primal_residual;
+  double dual_residual;
+  double primal_residual_inf;
+  double dual_residual_inf;
+  double primal_objective;
+  double dual_objective;
+  double absolute_gap;
+  double relative_primal;
+  double relative_dual;
+  double relative_gap;
+  double relative_primal_inf;
+  double relative_dual_inf;
+} anu_pdhg_residual;
+
+/* PdhgResult::Phases, src/anukulan/pdhg.hpp:516-536. */
+typedef struct anu_pdhg_phases {
+  double scaling;
+  double matrix_norm;
+  double setup;
+  double iterating;
+  double checks;
+  double polishing;
+} anu_pdhg_phases;
+
+/* PdhgResult, src/anukulan/pdhg.hpp:498-541. x and y are written to the
+ * caller's arrays; everything else is here. */
+typedef struct anu_pdhg_result {
+  int32_t status;            /* ANU_PDHG_* */
+  double objective;          /* model sense, including the offset */
+  int32_t iterations;
+  int32_t restarts;
+  int32_t polish_attempts;
+  int32_t polish_iterations;
+  int32_t polished;
+  double solve_seconds;
+  double matrix_norm_estimate;
+  double final_step_size;
+  double final_primal_weight;
+  anu_pdhg_phases phases;
+  anu_pdhg_residual residual;
+  /* ScalingReport, src/anukulan/scaling.hpp:36-44 */
+  double row_spread_before;
+  double row_spread_after;
+  double col_spread_before;
+  double col_spread_after;
+  /* engine additions */
+  int32_t refinement_rounds; /* outer refinement rounds actually run */
+  int32_t kernel_launches;   /* kernels this solve launched (graph nodes included) */
+  char message[160];
+} anu_pdhg_result;
+
+/* ---------------------------------------------------------------- basics */
+
+/* Version string of the library ("anu-pdhg-b200 <semver> sm_100a"). */
+const char* anu_pdhg_version(void);
+
+/* PdhgOptions{} defaults, src/anukulan/pdhg.hpp:19-415. */
+void anu_pdhg_default_options(anu_pdhg_options* options);
+
+/* Copies the last error message of this thread into buf (NUL terminated).
+ * Returns the code of that error, ANU_OK if there was none. */
+int anu_last_error(char* buf, int32_t size);
+
+/* Number of CUDA devices visible (0 when none). Never fails. */
+int32_t anu_device_count(void);
+
+/* ----------------------------------------------------------- single LP */
+
+/* solve_pdhg, src/anukulan/pdhg.hpp:543 / pdhg.cpp:377-1285.
+ * warm_x (n) and warm_y (m) may be NULL together (cold start) and follow
+ * PdhgOptions::warm_x/warm_y semantics. x (n) and y (m) receive the unscaled
+ * primal and dual solution. */
+int anu_pdhg_solve(const anu_lp* lp, const anu_pdhg_options* options,
+                   const double* warm_x, const double* warm_y, double* x,
+                   double* y, anu_pdhg_result* result);
+
+/* The same solve split in two, so the setup (scaling, upload, transpose,
+ * the ||K|| power iteration) can be paid once and the solve repeated with
+ * different starts. anu_pdhg_create does everything up to the loop; the
+ * handle owns its device memory and its stream. */
+typedef struct anu_pdhg anu_pdhg;
+int anu_pdhg_create(const anu_lp* lp, const anu_pdhg_options* options,
+                    anu_pdhg** handle);
+int anu_pdhg_run(anu_pdhg* handle, const double* warm_x, const double* warm_y,
+                 double* x, double* y, anu_pdhg_result* result);
+void anu_pdhg_destroy(anu_pdhg* handle);
+
+/* evaluate_residual, src/anukulan/pdhg.hpp:548 / pdhg.cpp:112-174: the FP64
+ * convergence measures of any primal-dual pair against the unscaled LP,
+ * computed on the device. */
+int anu_evaluate_residual(const anu_lp* lp, const double* x, const double* y,
+                          anu_pdhg_residual* out);
+
+/* estimate_matrix_norm, src/anukulan/pdhg.hpp:580 / pdhg.cpp:223-282: power
+ * iteration on K'K on the device, FP64. */
+int anu_estimate_matrix_norm(const anu_lp* lp, int32_t iterations,
+                             double tolerance, double* norm);
+
+/* ------------------------------------------------------ LinAlgBackend seam
+ * The coarse operations of LinAlgBackend (src/anukulan/backend.hpp:24-215) on
+ * device memory, so a thin C++ adapter can implement LinAlgBackend over this
+ * library and run the reference's own solve_pdhg on these kernels. Vectors
+ * are FP64 device arrays from anu_backend_allocate. Matrices are uploaded by
+ * anu_backend_prepare under the caller's identity key (SparseMatrix::id(),
+ * src/anukulan/sparse.hpp:51), never by address. All operations run on one
+ * library-owned stream and are complete when they return, like the
+ * reference's synchronous cudaMemcpy-based backend. */
+int anu_backend_allocate(int64_t n, double** device_ptr);        /* backend.hpp:50, zeroed */
+int anu_backend_deallocate(double* device_ptr);                  /* backend.hpp:51 */
+int anu_backend_upload(const double* host, double* device_ptr, int64_t n);    /* :52 */
+int anu_backend_download(const double* device_ptr, double* host, int64_t n);  /* :53 */
+int anu_backend_fill(double* device_ptr, int64_t n, double value);            /* :54 */
+int anu_backend_copy(const double* source, double* target, int64_t n);        /* :55 */
+int anu_backend_prepare(uint64_t id, const anu_csr* a);          /* backend.hpp:35 */
+int anu_backend_release(void);                                    /* backend.hpp:36 */
+int anu_backend_multiply(uint64_t id, const double* x, double* y);  /* :58, y = A x */
+int anu_backend_dot(const double* a, const double* b, int64_t n, double* out);  /* :64 */
+int anu_backend_two_norm(const double* a, int64_t n, double* out);              /* :65 */
+int anu_backend_inf_norm(const double* a, int64_t n, double* out);              /* :66 */
+int anu_backend_primal_update(int64_t n, double tau, double gamma, double halpern,
+                              const double* x, const double* c, const double* kt_y,
+                              const double* lower, const double* upper,
+                              const double* anchor, double* x_out, double* dx,
+                              double* x_bar);                     /* backend.hpp:89-93 */
+int anu_backend_dual_update(int64_t m, int64_t num_equalities, double sigma,
+                            double gamma, double halpern, const double* y,
+                            const double* q, const double* k_x_bar,
+                            const double* k_x, const double* anchor_y,
+                            const double* anchor_kx, double* y_out, double* dy,
+                            double* k_out, double* k_dx);         /* backend.hpp:114-119 */
+int anu_backend_accumulate(int64_t n, double weight, const double* v, double* sum); /* :123 */
+int anu_backend_scale_into(int64_t n, double weight, const double* sum, double* out); /* :126 */
+int anu_backend_weighted_norm_squared(int64_t n, int64_t m, const double* dx,
+                                      const double* dy, double omega,
+                                      double* out);               /* backend.hpp:129-130 */
+int anu_backend_step_size_terms(int64_t n, int64_t m, const double* dx,
+                                const double* dy, const double* k_dx, double omega,
+                                double* interaction, double* movement); /* :146-148 */
+/* ConvergenceProblem (backend.hpp:157-165) flattened; out[7] receives
+ * primal_sq, primal_inf, q_dot_y, dual_sq, dual_inf, bound_term, c_dot_x
+ * (ConvergenceTerms, backend.hpp:168-176). */
+int anu_backend_convergence_terms(int64_t n, int64_t m, const double* c,
+                                  const double* lower, const double* upper,
+                                  const double* q, const double* row_scale,
+                                  const double* col_scale, int64_t num_equalities,
+                                  const double* x, const double* k_x,
+                                  const double* y, const double* kt_y,
+                                  double* out);                   /* backend.hpp:198-202 */
+
+/* ------------------------------------------------------ batched case stack
+ * K cases that share K (the matrix) and differ in c, q, lower and upper.
+ * No counterpart in the reference, whose solve_pdhg takes one LP. The stack
+ * runs as one SpMM-shaped iteration over case-interleaved vectors: every
+ * nonzero of the matrix read serves all active cases. Each case keeps its own
+ * step size, primal weight, restarts and termination; a converged case is
+ * retired and its slot is free for anu_pdhg_batch_admit.
+ *
+ * Case arrays are case-major: c[k*n + j], q[k*m + i], and so on. A NULL case
+ * array means every case uses the base LP's vector. */
+typedef struct anu_pdhg_batch anu_pdhg_batch;
+int anu_pdhg_batch_create(const anu_lp* base, int32_t num_cases,
+                          const double* c, const double* q, const double* lower,
+                          const double* upper, const anu_pdhg_options* options,
+                          anu_pdhg_batch** handle);
+/* Runs every case to termination. x is num_cases*n, y is num_cases*m, results
+ * num_cases entries. */
+int anu_pdhg_batch_solve(anu_pdhg_batch* handle, double* x, double* y,
+                         anu_pdhg_result* results);
+void anu_pdhg_batch_destroy(anu_pdhg_batch* handle);
+
+#ifdef __cplusplus
+}  /* extern "C" */
+#endif
+
+#endif /* ANU_PDHG_H */

@@ -1,0 +1,217 @@
+"""Test infrastructure: ctypes loaders of the CPU checkers.
+
+* :func:`oracle_lib` - ``liboracle.so``, the C restatement of the reference
+  PDHG path (pdhg_oracle.c). Always present once built.
+* :func:`ref_lib` - ``_ref/libanuref.so``, the reference's own sources compiled
+  by oracle/Makefile, present where the reference tree was available at build
+  time (the built file travels with the working tree).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
+this package. The engine never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import time
+from typing import Optional
+
+import numpy as np
+
+from anukulan_b200.abi import (CLp, PdhgResult, Residual, anu_pdhg_options,
+                               anu_pdhg_residual, anu_pdhg_result, f64_ptr,
+                               make_options)
+from anukulan_b200.model import StandardLp
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libanuref.so")
+REF_SRC = "/root/reference/src/anukulan/pdhg.cpp"
+
+_oracle = None
+_ref = None
+
+_P = C.POINTER
+
+
+def build(with_reference: Optional[bool] = None) -> None:
+    """Builds liboracle.so, and _ref/libanuref.so when the reference sources
+    are present (or `with_reference` is True)."""
+    import subprocess
+    subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
+    if with_reference is None:
+        with_reference = os.path.exists(REF_SRC)
+    if with_reference:
+        subprocess.run(["make", "-s", "-j8", "-C", HERE, "ref"], check=True)
+
+
+def _declare(lib, name, restype, argtypes):
+    fn = getattr(lib, name)
+    fn.restype = restype
+    fn.argtypes = argtypes
+    return fn
+
+
+def oracle_lib():
+    global _oracle
+    if _oracle is None:
+        if not os.path.exists(ORACLE_SO):
+            build(with_reference=False)
+        lib = C.CDLL(ORACLE_SO)
+        _declare(lib, "oracle_pdhg_solve", C.c_int,
+                 [C.c_void_p, _P(anu_pdhg_options), _P(C.c_double), _P(C.c_double),
+                  _P(C.c_double), _P(C.c_double), _P(anu_pdhg_result)])
+        _declare(lib, "oracle_evaluate_residual", None,
+                 [C.c_void_p, _P(C.c_double), _P(C.c_double), _P(anu_pdhg_residual)])
+        _declare(lib, "oracle_estimate_matrix_norm", C.c_double,
+                 [C.c_void_p, C.c_int, C.c_double, C.c_int])
+        _declare(lib, "oracle_scale_lp", C.c_int,
+                 [C.c_void_p, C.c_int, C.c_int] + [_P(C.c_double)] * 8)
+        _declare(lib, "oracle_pdhg_solve_many", C.c_int,
+                 [C.c_int, C.c_void_p, _P(anu_pdhg_options), C.c_int,
+                  _P(_P(C.c_double)), _P(_P(C.c_double)), _P(anu_pdhg_result)])
+        _oracle = lib
+    return _oracle
+
+
+def have_reference() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def ref_lib():
+    global _ref
+    if _ref is None:
+        if not os.path.exists(REF_SO):
+            raise FileNotFoundError("oracle/_ref/libanuref.so is not built")
+        lib = C.CDLL(REF_SO)
+        _declare(lib, "ref_pdhg_solve", C.c_int,
+                 [C.c_void_p, _P(anu_pdhg_options), C.c_int, _P(C.c_double),
+                  _P(C.c_double), _P(C.c_double), _P(C.c_double), _P(anu_pdhg_result)])
+        _declare(lib, "ref_evaluate_residual", C.c_int,
+                 [C.c_void_p, _P(C.c_double), _P(C.c_double), _P(anu_pdhg_residual)])
+        _declare(lib, "ref_estimate_matrix_norm", C.c_double,
+                 [C.c_void_p, C.c_int, C.c_double, C.c_int])
+        _declare(lib, "ref_scale_lp", C.c_int,
+                 [C.c_void_p, C.c_int, C.c_int] + [_P(C.c_double)] * 8)
+        _declare(lib, "ref_simplex_solve", C.c_int,
+                 [C.c_void_p, C.c_double, _P(C.c_double), _P(C.c_double),
+                  _P(C.c_double), _P(C.c_int)])
+        _declare(lib, "ref_default_thread_count", C.c_int, [])
+        _ref = lib
+    return _ref
+
+
+def _opts(options=None, **kw) -> anu_pdhg_options:
+    if options is not None:
+        return options
+    return make_options(**kw)
+
+
+def oracle_solve(lp: StandardLp, options=None, warm_x=None, warm_y=None, **kw) -> PdhgResult:
+    """The restated solve_pdhg on the host."""
+    cl = CLp(lp)
+    o = _opts(options, **kw)
+    x = np.zeros(cl.n)
+    y = np.zeros(cl.m)
+    r = anu_pdhg_result()
+    wx = None if warm_x is None else np.ascontiguousarray(warm_x, np.float64)
+    wy = None if warm_y is None else np.ascontiguousarray(warm_y, np.float64)
+    oracle_lib().oracle_pdhg_solve(cl.ref(), C.byref(o), f64_ptr(wx), f64_ptr(wy),
+                                   f64_ptr(x), f64_ptr(y), C.byref(r))
+    return PdhgResult.from_c(r, x, y)
+
+
+def ref_solve(lp: StandardLp, options=None, threads: int = 1, warm_x=None, warm_y=None,
+              **kw) -> PdhgResult:
+    """The reference's own solve_pdhg (cpu_backend, or threaded_cpu_backend
+    when threads > 1; threads < 0 is the reference's default count)."""
+    cl = CLp(lp)
+    o = _opts(options, **kw)
+    x = np.zeros(cl.n)
+    y = np.zeros(cl.m)
+    r = anu_pdhg_result()
+    wx = None if warm_x is None else np.ascontiguousarray(warm_x, np.float64)
+    wy = None if warm_y is None else np.ascontiguousarray(warm_y, np.float64)
+    rc = ref_lib().ref_pdhg_solve(cl.ref(), C.byref(o), threads, f64_ptr(wx), f64_ptr(wy),
+                                  f64_ptr(x), f64_ptr(y), C.byref(r))
+    if rc != 0:
+        raise RuntimeError(r.message.decode())
+    return PdhgResult.from_c(r, x, y)
+
+
+def oracle_residual(lp: StandardLp, x, y) -> Residual:
+    cl = CLp(lp)
+    out = anu_pdhg_residual()
+    oracle_lib().oracle_evaluate_residual(cl.ref(), f64_ptr(np.ascontiguousarray(x, np.float64)),
+                                          f64_ptr(np.ascontiguousarray(y, np.float64)),
+                                          C.byref(out))
+    return Residual.from_c(out)
+
+
+def ref_residual(lp: StandardLp, x, y) -> Residual:
+    cl = CLp(lp)
+    out = anu_pdhg_residual()
+    ref_lib().ref_evaluate_residual(cl.ref(), f64_ptr(np.ascontiguousarray(x, np.float64)),
+                                    f64_ptr(np.ascontiguousarray(y, np.float64)),
+                                    C.byref(out))
+    return Residual.from_c(out)
+
+
+def oracle_matrix_norm(lp: StandardLp, iterations=200, tolerance=1e-8, scaled=False) -> float:
+    return oracle_lib().oracle_estimate_matrix_norm(CLp(lp).ref(), iterations, tolerance,
+                                                    int(scaled))
+
+
+def ref_matrix_norm(lp: StandardLp, iterations=200, tolerance=1e-8, scaled=False) -> float:
+    return ref_lib().ref_estimate_matrix_norm(CLp(lp).ref(), iterations, tolerance, int(scaled))
+
+
+def _scale(fn, lp: StandardLp, ruiz=10, pc=True):
+    cl = CLp(lp)
+    n, m, nnz = lp.num_cols, lp.num_rows, lp.k.nnz
+    out = dict(k_value=np.zeros(nnz), c=np.zeros(n), q=np.zeros(m), lower=np.zeros(n),
+               upper=np.zeros(n), row_scale=np.zeros(m), col_scale=np.zeros(n),
+               spreads=np.zeros(4))
+    fn(cl.ref(), ruiz, int(pc), *[f64_ptr(out[k]) for k in
+                                 ("k_value", "c", "q", "lower", "upper", "row_scale",
+                                  "col_scale", "spreads")])
+    return out
+
+
+def oracle_scale(lp: StandardLp, ruiz=10, pc=True) -> dict:
+    return _scale(oracle_lib().oracle_scale_lp, lp, ruiz, pc)
+
+
+def ref_scale(lp: StandardLp, ruiz=10, pc=True) -> dict:
+    return _scale(ref_lib().ref_scale_lp, lp, ruiz, pc)
+
+
+def ref_simplex(lp: StandardLp, time_limit: float = 300.0):
+    """The reference dual simplex (through solve_lp). Returns
+    (status, objective, iterations, x, y); status 0 is optimal."""
+    cl = CLp(lp)
+    x = np.zeros(cl.n)
+    y = np.zeros(cl.m)
+    obj = C.c_double(0.0)
+    its = C.c_int(0)
+    st = ref_lib().ref_simplex_solve(cl.ref(), time_limit, f64_ptr(x), f64_ptr(y),
+                                     C.byref(obj), C.byref(its))
+    return st, obj.value, its.value, x, y
+
+
+def oracle_solve_many(lps, options=None, threads: int = 1, **kw):
+    """Solves independent LPs on `threads` host threads; returns
+    (results, seconds)."""
+    o = _opts(options, **kw)
+    cls = [CLp(lp) for lp in lps]
+    arr = (type(cls[0].struct) * len(cls))(*[c.struct for c in cls])
+    xs = [np.zeros(c.n) for c in cls]
+    ys = [np.zeros(c.m) for c in cls]
+    xp = (_P(C.c_double) * len(cls))(*[f64_ptr(a) for a in xs])
+    yp = (_P(C.c_double) * len(cls))(*[f64_ptr(a) for a in ys])
+    res = (anu_pdhg_result * len(cls))()
+    t0 = time.perf_counter()
+    oracle_lib().oracle_pdhg_solve_many(len(cls), C.cast(arr, C.c_void_p), C.byref(o), threads,
+                                        xp, yp, res)
+    dt = time.perf_counter() - t0
+    return [PdhgResult.from_c(res[i], xs[i], ys[i]) for i in range(len(cls))], dt

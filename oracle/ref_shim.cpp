@@ -1,0 +1,252 @@
+// Test infrastructure, not product code: a C shim over the reference's own
+// PDHG path (anukulan, src/anukulan/*.cpp compiled unmodified from the
+// reference tree by oracle/Makefile into oracle/_ref/). The tests and the CPU
+// leg of bench.py load oracle/_ref/libanuref.so through ctypes to pin the
+// oracle restatement (oracle/pdhg_oracle.c) and the CUDA engine against the
+// reference itself. Nothing in the engine links or loads this.
+//
+// Options and results use the engine's own C structs (include/anu_pdhg.h),
+// which mirror PdhgOptions / PdhgResult field for field, so one options
+// object drives the reference, the oracle and the engine identically.
+
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "anu_pdhg.h"
+#include "anukulan/backend.hpp"
+#include "anukulan/model.hpp"
+#include "anukulan/pdhg.hpp"
+#include "anukulan/scaling.hpp"
+#include "anukulan/simplex.hpp"
+#include "anukulan/sparse.hpp"
+#include "anukulan/standard_form.hpp"
+#include "anukulan/threading.hpp"
+
+namespace {
+
+using anukulan::Int;
+
+anukulan::SparseMatrix csr_to_matrix(const anu_csr& a) {
+  std::vector<anukulan::Triplet> t;
+  t.reserve(static_cast<std::size_t>(a.nnz));
+  for (Int r = 0; r < a.rows; ++r) {
+    for (Int k = a.start[r]; k < a.start[r + 1]; ++k) {
+      t.push_back(anukulan::Triplet{r, a.index[k], a.value[k]});
+    }
+  }
+  return anukulan::SparseMatrix::from_triplets(a.rows, a.cols, std::move(t));
+}
+
+anukulan::StandardLp to_lp(const anu_lp& in) {
+  anukulan::StandardLp lp;
+  lp.k = csr_to_matrix(in.k);
+  lp.kt = lp.k.transpose();
+  const std::size_t n = static_cast<std::size_t>(in.k.cols);
+  const std::size_t m = static_cast<std::size_t>(in.k.rows);
+  lp.c.assign(in.c, in.c + n);
+  lp.q.assign(in.q, in.q + m);
+  lp.lower.assign(in.lower, in.lower + n);
+  lp.upper.assign(in.upper, in.upper + n);
+  lp.num_equalities = in.num_equalities;
+  lp.objective_scale = in.objective_scale;
+  lp.objective_offset = in.objective_offset;
+  lp.row_origin.resize(m);
+  for (std::size_t i = 0; i < m; ++i) {
+    lp.row_origin[i] = anukulan::StandardLp::RowOrigin{static_cast<Int>(i), 1.0};
+  }
+  return lp;
+}
+
+anukulan::PdhgOptions to_options(const anu_pdhg_options& o) {
+  anukulan::PdhgOptions p;
+  p.tolerance = o.tolerance;
+  p.gap_tolerance = o.gap_tolerance;
+  p.max_iterations = o.max_iterations;
+  p.time_limit_seconds = o.time_limit_seconds;
+  p.termination_check_frequency = o.termination_check_frequency;
+  p.absolute_tolerance = o.absolute_tolerance;
+  p.require_inf_norm_termination = o.require_inf_norm_termination != 0;
+  p.adaptive_step_size = o.adaptive_step_size != 0;
+  p.primal_weight_updates = o.primal_weight_updates != 0;
+  p.restarts = o.restarts != 0;
+  p.halpern = o.halpern != 0;
+  p.halpern_restart = o.halpern_restart != 0;
+  p.halpern_minimum_epoch = o.halpern_minimum_epoch;
+  p.polish_feasibility = o.polish_feasibility != 0;
+  p.polish_first_iteration = o.polish_first_iteration;
+  p.polish_iteration_factor = o.polish_iteration_factor;
+  p.polish_minimum_iterations = o.polish_minimum_iterations;
+  p.polish_maximum_iterations = o.polish_maximum_iterations;
+  p.polish_on_exit = o.polish_on_exit != 0;
+  p.reflection = o.reflection;
+  p.constant_step_size = o.constant_step_size != 0;
+  p.constant_step_scale = o.constant_step_scale;
+  p.restart_on_fixed_point = o.restart_on_fixed_point != 0;
+  p.pid_primal_weight = o.pid_primal_weight != 0;
+  p.primal_weight_kp = o.primal_weight_kp;
+  p.primal_weight_ki = o.primal_weight_ki;
+  p.primal_weight_kd = o.primal_weight_kd;
+  p.scaling.ruiz_iterations = o.ruiz_iterations;
+  p.scaling.pock_chambolle = o.pock_chambolle != 0;
+  p.reuse_products = o.reuse_products != 0;
+  p.detect_infeasibility = o.detect_infeasibility != 0;
+  p.infeasibility_tolerance = o.infeasibility_tolerance;
+  switch (o.termination) {
+    case ANU_TERMINATION_PRIMAL_FEASIBILITY:
+      p.termination = anukulan::PdhgOptions::Termination::kPrimalFeasibility;
+      break;
+    case ANU_TERMINATION_DUAL_FEASIBILITY:
+      p.termination = anukulan::PdhgOptions::Termination::kDualFeasibility;
+      break;
+    default:
+      p.termination = anukulan::PdhgOptions::Termination::kFull;
+  }
+  p.known_matrix_norm = o.known_matrix_norm;
+  p.initial_step_size = o.initial_step_size;
+  p.initial_primal_weight = o.initial_primal_weight;
+  p.verbose = o.verbose != 0;
+  p.log_frequency = o.log_frequency;
+  return p;
+}
+
+void copy_residual(const anukulan::PdhgResidual& r, anu_pdhg_residual* out) {
+  out->primal_residual = r.primal_residual;
+  out->dual_residual = r.dual_residual;
+  out->primal_residual_inf = r.primal_residual_inf;
+  out->dual_residual_inf = r.dual_residual_inf;
+  out->primal_objective = r.primal_objective;
+  out->dual_objective = r.dual_objective;
+  out->absolute_gap = r.absolute_gap;
+  out->relative_primal = r.relative_primal;
+  out->relative_dual = r.relative_dual;
+  out->relative_gap = r.relative_gap;
+  out->relative_primal_inf = r.relative_primal_inf;
+  out->relative_dual_inf = r.relative_dual_inf;
+}
+
+}  // namespace
+
+extern "C" {
+
+// The reference's solve_pdhg on cpu_backend() (threads <= 1) or
+// threaded_cpu_backend(threads). threads < 0 means default_thread_count().
+int ref_pdhg_solve(const anu_lp* lp_in, const anu_pdhg_options* opt_in,
+                   int threads, const double* warm_x, const double* warm_y,
+                   double* x, double* y, anu_pdhg_result* out) {
+  try {
+    const anukulan::StandardLp lp = to_lp(*lp_in);
+    anukulan::PdhgOptions options = to_options(*opt_in);
+    if (threads < 0) threads = anukulan::default_thread_count();
+    options.backend = threads <= 1 ? &anukulan::cpu_backend()
+                                   : &anukulan::threaded_cpu_backend(threads);
+    std::vector<double> wx, wy;
+    if (warm_x != nullptr && warm_y != nullptr) {
+      wx.assign(warm_x, warm_x + lp_in->k.cols);
+      wy.assign(warm_y, warm_y + lp_in->k.rows);
+      options.warm_x = &wx;
+      options.warm_y = &wy;
+    }
+    const anukulan::PdhgResult r = anukulan::solve_pdhg(lp, options);
+    std::memset(out, 0, sizeof(*out));
+    out->status = static_cast<int32_t>(r.status);
+    out->objective = r.objective;
+    out->iterations = r.iterations;
+    out->restarts = r.restarts;
+    out->polish_attempts = r.polish_attempts;
+    out->polish_iterations = r.polish_iterations;
+    out->polished = r.polished ? 1 : 0;
+    out->solve_seconds = r.solve_seconds;
+    out->matrix_norm_estimate = r.matrix_norm_estimate;
+    out->final_step_size = r.final_step_size;
+    out->final_primal_weight = r.final_primal_weight;
+    out->phases.scaling = r.phases.scaling;
+    out->phases.matrix_norm = r.phases.matrix_norm;
+    out->phases.setup = r.phases.setup;
+    out->phases.iterating = r.phases.iterating;
+    out->phases.checks = r.phases.checks;
+    out->phases.polishing = r.phases.polishing;
+    copy_residual(r.residual, &out->residual);
+    out->row_spread_before = r.scaling.row_spread_before;
+    out->row_spread_after = r.scaling.row_spread_after;
+    out->col_spread_before = r.scaling.col_spread_before;
+    out->col_spread_after = r.scaling.col_spread_after;
+    std::snprintf(out->message, sizeof(out->message), "%s", r.message.c_str());
+    for (std::size_t j = 0; j < r.x.size(); ++j) x[j] = r.x[j];
+    for (std::size_t i = 0; i < r.y.size(); ++i) y[i] = r.y[i];
+    return 0;
+  } catch (const std::exception& e) {
+    std::snprintf(out->message, sizeof(out->message), "exception: %s", e.what());
+    return 1;
+  }
+}
+
+int ref_evaluate_residual(const anu_lp* lp_in, const double* x, const double* y,
+                          anu_pdhg_residual* out) {
+  const anukulan::StandardLp lp = to_lp(*lp_in);
+  std::vector<double> vx(x, x + lp_in->k.cols), vy(y, y + lp_in->k.rows);
+  copy_residual(anukulan::evaluate_residual(lp, vx, vy), out);
+  return 0;
+}
+
+double ref_estimate_matrix_norm(const anu_lp* lp_in, int iterations, double tolerance,
+                                int scaled) {
+  anukulan::StandardLp lp = to_lp(*lp_in);
+  if (scaled) anukulan::scale_lp(&lp);
+  return anukulan::estimate_matrix_norm(lp, iterations, tolerance, nullptr);
+}
+
+// scale_lp (src/anukulan/scaling.cpp:75-100) with its default options: writes
+// the scaled K values in CSR order of the input (the input must already be in
+// from_triplets order: sorted unique columns, no zeros), the scaled c, q,
+// bounds and the two diagonals.
+int ref_scale_lp(const anu_lp* lp_in, int ruiz_iterations, int pock_chambolle,
+                 double* k_value, double* c, double* q, double* lower, double* upper,
+                 double* row_scale, double* col_scale, double* spreads) {
+  anukulan::StandardLp lp = to_lp(*lp_in);
+  if (lp.k.nnz() != lp_in->k.nnz) return 1;
+  anukulan::ScalingOptions so;
+  so.ruiz_iterations = ruiz_iterations;
+  so.pock_chambolle = pock_chambolle != 0;
+  const anukulan::ScalingReport rep = anukulan::scale_lp(&lp, so);
+  for (Int k = 0; k < lp.k.nnz(); ++k) k_value[k] = lp.k.value()[static_cast<std::size_t>(k)];
+  for (std::size_t j = 0; j < lp.c.size(); ++j) {
+    c[j] = lp.c[j];
+    lower[j] = lp.lower[j];
+    upper[j] = lp.upper[j];
+    col_scale[j] = rep.scaling.col_scale[j];
+  }
+  for (std::size_t i = 0; i < lp.q.size(); ++i) {
+    q[i] = lp.q[i];
+    row_scale[i] = rep.scaling.row_scale[i];
+  }
+  spreads[0] = rep.row_spread_before;
+  spreads[1] = rep.row_spread_after;
+  spreads[2] = rep.col_spread_before;
+  spreads[3] = rep.col_spread_after;
+  return 0;
+}
+
+// The reference dual simplex (src/anukulan/simplex.hpp:452) through solve_lp,
+// which falls back to the primal when the start cannot be made dual feasible.
+// Returns the SimplexStatus as an int; x (n) and y (m) receive the solution.
+int ref_simplex_solve(const anu_lp* lp_in, double time_limit, double* x, double* y,
+                      double* objective, int* iterations) {
+  const anukulan::StandardLp lp = to_lp(*lp_in);
+  anukulan::SimplexOptions so;
+  so.time_limit_seconds = time_limit;
+  const anukulan::SimplexResult r = anukulan::solve_lp(lp, so);
+  for (std::size_t j = 0; j < r.x.size() && j < static_cast<std::size_t>(lp_in->k.cols); ++j)
+    x[j] = r.x[j];
+  for (std::size_t i = 0; i < r.y.size() && i < static_cast<std::size_t>(lp_in->k.rows); ++i)
+    y[i] = r.y[i];
+  *objective = r.objective;
+  *iterations = r.iterations;
+  return static_cast<int>(r.status);
+}
+
+int ref_default_thread_count(void) { return anukulan::default_thread_count(); }
+
+}  // extern "C"
