@@ -59,6 +59,7 @@ class anu_pdhg_options(C.Structure):
         ("stop", C.POINTER(i32)),
         ("precision", i32), ("refinement_rounds", i32),
         ("refinement_inner_tolerance", f64), ("device", i32), ("use_graphs", i32),
+        ("profile", i32),
     ]
 
 
@@ -84,6 +85,7 @@ class anu_pdhg_result(C.Structure):
         ("row_spread_before", f64), ("row_spread_after", f64),
         ("col_spread_before", f64), ("col_spread_after", f64),
         ("refinement_rounds", i32), ("kernel_launches", i32),
+        ("device_iteration_seconds", f64), ("device_iterations", C.c_int64),
         ("message", C.c_char * 160),
     ]
 
@@ -103,7 +105,7 @@ DEFAULTS = dict(
     detect_infeasibility=1, infeasibility_tolerance=1e-8, termination=0,
     known_matrix_norm=0.0, initial_step_size=0.0, initial_primal_weight=0.0,
     verbose=0, log_frequency=5000, precision=0, refinement_rounds=0,
-    refinement_inner_tolerance=0.0, device=0, use_graphs=1,
+    refinement_inner_tolerance=0.0, device=0, use_graphs=1, profile=0,
 )
 
 
@@ -197,6 +199,8 @@ class PdhgResult:
     spreads: tuple
     refinement_rounds: int
     kernel_launches: int
+    device_iteration_seconds: float
+    device_iterations: int
     message: str
 
     @property
@@ -213,8 +217,8 @@ class PdhgResult:
             Residual.from_c(r.residual),
             (r.row_spread_before, r.row_spread_after, r.col_spread_before,
              r.col_spread_after),
-            r.refinement_rounds, r.kernel_launches,
-            r.message.decode(errors="replace"))
+            r.refinement_rounds, r.kernel_launches, r.device_iteration_seconds,
+            r.device_iterations, r.message.decode(errors="replace"))
 
 
 def _ptr(a: np.ndarray, ctype):

@@ -1,0 +1,1836 @@
+// The PDHG engine: device problem setup, the lockstep case-stack solver and
+// the single-LP / case-stack entry points of the C ABI.
+//
+// The control flow of run_cases restates solve_pdhg
+// (src/anukulan/pdhg.cpp:377-1285) once per case: the same step-size and
+// primal-weight initialisation, Halpern epochs with reflection, the
+// fixed-point (or KKT) restart test with cuPDLP's three conditions, the PID
+// primal weight, feasibility polishing with its geometric schedule and exit
+// polish, the Farkas infeasibility test, the time limit and the stop flag.
+// What changes is where the work runs: the iteration is two fused kernels
+// (K'y + primal step, K x_bar + dual step) launched as CUDA-graph chunks of
+// one check period, and every check is a handful of device reductions whose
+// results (18 doubles per case) are the only thing that crosses the bus.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <utility>
+
+#include "engine.hpp"
+
+namespace anu {
+
+// ------------------------------------------------------------- errors
+
+namespace {
+thread_local std::string g_error;
+thread_local int g_error_code = ANU_OK;
+}  // namespace
+
+void set_last_error(int code, const std::string& message) {
+  g_error_code = code;
+  g_error = message;
+}
+void clear_last_error() {
+  g_error_code = ANU_OK;
+  g_error.clear();
+}
+int copy_last_error(char* buf, int32_t size) {
+  if (buf != nullptr && size > 0) std::snprintf(buf, static_cast<size_t>(size), "%s", g_error.c_str());
+  return g_error_code;
+}
+
+void cuda_check(cudaError_t status, const char* what) {
+  if (status != cudaSuccess) {
+    const int code = (status == cudaErrorNoDevice || status == cudaErrorInsufficientDriver)
+                         ? ANU_ERR_NO_DEVICE
+                         : (status == cudaErrorMemoryAllocation ? ANU_ERR_MEMORY : ANU_ERR_CUDA);
+    throw Error(code, std::string(what) + ": " + cudaGetErrorString(status));
+  }
+}
+
+// ------------------------------------------------------------ matrices
+
+void DevCsr::upload(const HostCsr& a, bool with_fp32, cudaStream_t s) {
+  rows = a.rows;
+  cols = a.cols;
+  nnz = a.nnz();
+  start.alloc(static_cast<size_t>(rows) + 1);
+  index.alloc(std::max<size_t>(nnz, 1));
+  v64.alloc(std::max<size_t>(nnz, 1));
+  ANU_CUDA(cudaMemcpyAsync(start.p, a.start.data(), sizeof(int32_t) * (rows + 1),
+                           cudaMemcpyHostToDevice, s));
+  std::vector<float> f;
+  if (nnz > 0) {
+    ANU_CUDA(cudaMemcpyAsync(index.p, a.index.data(), sizeof(int32_t) * nnz,
+                             cudaMemcpyHostToDevice, s));
+    ANU_CUDA(cudaMemcpyAsync(v64.p, a.value.data(), sizeof(double) * nnz,
+                             cudaMemcpyHostToDevice, s));
+  }
+  if (with_fp32) {
+    v32.alloc(std::max<size_t>(nnz, 1));
+    f.resize(nnz);
+    for (int32_t k = 0; k < nnz; ++k) f[k] = static_cast<float>(a.value[k]);
+    if (nnz > 0)
+      ANU_CUDA(cudaMemcpyAsync(v32.p, f.data(), sizeof(float) * nnz, cudaMemcpyHostToDevice, s));
+  }
+  const std::vector<RowBlock> b = row_blocks(a, kBlockNnz, kBlockRows);
+  num_blocks = static_cast<int32_t>(b.size());
+  blocks.alloc(std::max<size_t>(b.size(), 1));
+  std::vector<RowBlockDev> bd(b.size());
+  for (size_t i = 0; i < b.size(); ++i) bd[i] = {b[i].row_begin, b[i].row_end};
+  if (!bd.empty())
+    ANU_CUDA(cudaMemcpyAsync(blocks.p, bd.data(), sizeof(RowBlockDev) * bd.size(),
+                             cudaMemcpyHostToDevice, s));
+  ANU_CUDA(cudaStreamSynchronize(s));
+}
+
+template <>
+CsrView<double> DevCsr::view<double>() const {
+  return {rows, cols, start.p, index.p, v64.p, blocks.p, num_blocks};
+}
+template <>
+CsrView<float> DevCsr::view<float>() const {
+  return {rows, cols, start.p, index.p, v32.p, blocks.p, num_blocks};
+}
+
+Problem::~Problem() {
+  if (owns_stream && stream) cudaStreamDestroy(stream);
+}
+
+// ------------------------------------------------------------- launches
+
+namespace {
+
+template <class T>
+__global__ void accumulate_kernel(int64_t n, double weight, const T* __restrict__ v,
+                                  T* __restrict__ sum) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    sum[i] = add(sum[i], mul(static_cast<T>(weight), v[i]));
+}
+
+// Sum of squares over one vector per case (power iteration, step terms).
+template <class T>
+struct SquareTerms {
+  static constexpr int NT = 1;
+  int32_t K;
+  const T* __restrict__ v;
+  __device__ static void init(double* a) { a[0] = 0.0; }
+  __device__ static double identity(int) { return 0.0; }
+  __device__ static double combine(int, double a, double b) { return anu::add(a, b); }
+  __device__ void add(double* a, int32_t i, int32_t k) const {
+    const double x = static_cast<double>(v[(size_t)i * K + k]);
+    a[0] = anu::add(a[0], mul(x, x));
+  }
+};
+
+// dy . k_dx and |dy|^2 (rows), for the adaptive step size.
+template <class T>
+struct StepRowTerms {
+  static constexpr int NT = 2;
+  const T* __restrict__ dy;
+  const T* __restrict__ kdx;
+  __device__ static void init(double* a) { a[0] = a[1] = 0.0; }
+  __device__ static double identity(int) { return 0.0; }
+  __device__ static double combine(int, double a, double b) { return anu::add(a, b); }
+  __device__ void add(double* a, int32_t i, int32_t) const {
+    const double d = static_cast<double>(dy[i]);
+    a[0] = anu::add(a[0], mul(d, static_cast<double>(kdx[i])));
+    a[1] = anu::add(a[1], mul(d, d));
+  }
+};
+
+__global__ void normalize_kernel(int32_t n, const double* __restrict__ in,
+                                 const double* __restrict__ sumsq, double* __restrict__ out,
+                                 double* __restrict__ estimates, int32_t slot) {
+  const double next = sqrt(sumsq[0]);
+  for (int32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
+    out[j] = next != 0.0 ? in[j] / next : 0.0;
+  if (blockIdx.x == 0 && threadIdx.x == 0) estimates[slot] = next;
+}
+
+}  // namespace
+
+// ------------------------------------------------------ ||K|| estimate
+
+double device_matrix_norm(Problem& p, int iterations, double tolerance) {
+  const int32_t n = p.n, m = p.m;
+  if (n == 0 || m == 0 || p.dk.nnz == 0) return 0.0;
+  // Deterministic non-uniform start, normalised on the host exactly as the
+  // reference does (pdhg.cpp:233-238).
+  std::vector<double> v(n);
+  for (int32_t j = 0; j < n; ++j) v[j] = 1.0 + 0.1 * static_cast<double>(j % 7);
+  double ss = 0.0;
+  for (double a : v) ss += a * a;
+  const double norm = std::sqrt(ss);
+  if (norm == 0.0) return 0.0;
+  for (double& a : v) a /= norm;
+  DevBuf<double> dv(n), dkv(m), dktkv(n), partial, sumsq(1), est(std::max(iterations, 1));
+  ANU_CUDA(cudaMemcpyAsync(dv.p, v.data(), sizeof(double) * n, cudaMemcpyHostToDevice, p.stream));
+  std::vector<double> h_est(std::max(iterations, 1));
+  // Chunks of iterations between host looks; the convergence test reads the
+  // estimates in order, so running past convergence changes nothing.
+  const int chunk = 16;
+  double sigma = 0.0;
+  for (int base = 0; base < iterations; base += chunk) {
+    const int count = std::min(chunk, iterations - base);
+    for (int it = 0; it < count; ++it) {
+      product<double, double, double>(p, p.dk, dv.p, 1, StoreEpi<double>{1, dkv.p});
+      product<double, double, double>(p, p.dkt, dkv.p, 1, StoreEpi<double>{1, dktkv.p});
+      reduce_terms(p, n, 1, SquareTerms<double>{1, dktkv.p}, partial, sumsq.p, 1, 0);
+      normalize_kernel<<<grid_for(n, 256, 296), 256, 0, p.stream>>>(n, dktkv.p, sumsq.p, dv.p,
+                                                                     est.p, base + it);
+      ANU_CUDA(cudaGetLastError());
+      ++p.launches;
+    }
+    ANU_CUDA(cudaMemcpyAsync(h_est.data() + base, est.p + base, sizeof(double) * count,
+                             cudaMemcpyDeviceToHost, p.stream));
+    ANU_CUDA(cudaStreamSynchronize(p.stream));
+    for (int it = base; it < base + count; ++it) {
+      const double next = h_est[it];
+      if (next == 0.0) return 0.0;
+      const double estimate = std::sqrt(next);
+      if (it > 0 && std::fabs(estimate - sigma) <= tolerance * estimate) return estimate;
+      sigma = estimate;
+    }
+  }
+  return sigma;
+}
+
+// ---------------------------------------------------------- validation
+
+std::string validate_lp(const anu_lp& lp) {
+  const std::string e = validate_csr(lp.k.rows, lp.k.cols, lp.k.nnz, lp.k.start, lp.k.index);
+  if (!e.empty()) return e;
+  if (lp.k.nnz > 0 && lp.k.value == nullptr) return "null matrix values";
+  if (lp.k.cols > 0 && (lp.c == nullptr || lp.lower == nullptr || lp.upper == nullptr))
+    return "null column vectors";
+  if (lp.k.rows > 0 && lp.q == nullptr) return "null right-hand side";
+  if (lp.num_equalities < 0 || lp.num_equalities > lp.k.rows) return "num_equalities out of range";
+  for (int32_t j = 0; j < lp.k.cols; ++j)
+    if (lp.lower[j] > lp.upper[j]) return "empty bound interval at column " + std::to_string(j);
+  for (int32_t i = 0; i < lp.k.rows; ++i)
+    if (!std::isfinite(lp.q[i])) return "rhs is not finite";
+  return "";
+}
+
+void validate_options(const anu_pdhg_options& o) {
+  if (o.termination_check_frequency < 1) throw Error(ANU_ERR_INVALID, "termination_check_frequency < 1");
+  if (o.max_iterations < 0) throw Error(ANU_ERR_INVALID, "max_iterations < 0");
+  if (o.precision != ANU_PRECISION_FP64 && o.precision != ANU_PRECISION_FP32)
+    throw Error(ANU_ERR_INVALID, "unknown precision");
+  if (o.ruiz_iterations < 0) throw Error(ANU_ERR_INVALID, "ruiz_iterations < 0");
+  if (o.termination < 0 || o.termination > 2) throw Error(ANU_ERR_INVALID, "unknown termination");
+}
+
+// -------------------------------------------------------------- setup
+
+std::unique_ptr<Problem> make_problem(const anu_lp& lp, const anu_pdhg_options& o,
+                                      double* scaling_seconds, double* norm_seconds) {
+  int count = 0;
+  const cudaError_t ce = cudaGetDeviceCount(&count);
+  if (ce != cudaSuccess || count == 0)
+    throw Error(ANU_ERR_NO_DEVICE, "no CUDA device is available; this engine has no CPU fallback");
+  if (o.device < 0 || o.device >= count) throw Error(ANU_ERR_INVALID, "device ordinal out of range");
+  ANU_CUDA(cudaSetDevice(o.device));
+  auto p = std::make_unique<Problem>();
+  p->device = o.device;
+  ANU_CUDA(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
+  p->owns_stream = true;
+  p->m = lp.k.rows;
+  p->n = lp.k.cols;
+  p->num_eq = lp.num_equalities;
+  p->precision = o.precision;
+  double t0 = now_seconds();
+  p->k = copy_csr(lp.k.rows, lp.k.cols, lp.k.nnz, lp.k.start, lp.k.index, lp.k.value);
+  p->scaling = scale_matrix_sweeps(&p->k, o.ruiz_iterations, o.pock_chambolle != 0, &p->sweeps);
+  p->kt = transpose(p->k);
+  if (scaling_seconds) *scaling_seconds = now_seconds() - t0;
+  const bool fp32 = o.precision == ANU_PRECISION_FP32;
+  p->dk.upload(p->k, fp32, p->stream);
+  p->dkt.upload(p->kt, fp32, p->stream);
+  p->row_scale.alloc(std::max(p->m, 1));
+  p->col_scale.alloc(std::max(p->n, 1));
+  if (p->m > 0)
+    ANU_CUDA(cudaMemcpyAsync(p->row_scale.p, p->scaling.row_scale.data(), sizeof(double) * p->m,
+                             cudaMemcpyHostToDevice, p->stream));
+  if (p->n > 0)
+    ANU_CUDA(cudaMemcpyAsync(p->col_scale.p, p->scaling.col_scale.data(), sizeof(double) * p->n,
+                             cudaMemcpyHostToDevice, p->stream));
+  ANU_CUDA(cudaStreamSynchronize(p->stream));
+  t0 = now_seconds();
+  p->matrix_norm = o.known_matrix_norm > 0.0 ? o.known_matrix_norm
+                                              : device_matrix_norm(*p, 200, 1e-8);
+  if (norm_seconds) *norm_seconds = now_seconds() - t0;
+  return p;
+}
+
+CaseData make_case(const Problem& p, const double* c, const double* q, const double* lower,
+                   const double* upper, double objective_scale, double objective_offset) {
+  CaseData d;
+  d.c.assign(c, c + p.n);
+  d.q.assign(q, q + p.m);
+  d.lower.assign(lower, lower + p.n);
+  d.upper.assign(upper, upper + p.n);
+  d.cs = d.c;
+  d.qs = d.q;
+  d.ls = d.lower;
+  d.us = d.upper;
+  if (!p.unit_scaling)
+    scale_vectors(p.sweeps, p.m, p.n, d.cs.data(), d.qs.data(), d.ls.data(), d.us.data());
+  d.objective_scale = objective_scale;
+  d.objective_offset = objective_offset;
+  return d;
+}
+
+// ------------------------------------------------------------- solver
+
+namespace {
+
+double host_norm2(const std::vector<double>& v) {
+  double s = 0.0;
+  for (double a : v) s += a * a;
+  return std::sqrt(s);
+}
+double host_norminf(const std::vector<double>& v) {
+  double m = 0.0;
+  for (double a : v) m = std::fmax(m, std::fabs(a));
+  return m;
+}
+
+struct ResidualScales {
+  double q_two, c_two, q_inf, c_inf;
+};
+
+// residual_from_terms (pdhg.cpp:70-87) from the row and column check terms.
+anu_pdhg_residual residual_from_terms(const double* row, const double* col,
+                                      const ResidualScales& s) {
+  anu_pdhg_residual r{};
+  r.primal_residual = std::sqrt(row[0]);
+  r.primal_residual_inf = row[1];
+  r.dual_residual = std::sqrt(col[0]);
+  r.dual_residual_inf = col[1];
+  r.primal_objective = col[3];
+  r.dual_objective = row[2] + col[2];
+  r.absolute_gap = std::fabs(r.primal_objective - r.dual_objective);
+  r.relative_primal = r.primal_residual / (1.0 + s.q_two);
+  r.relative_dual = r.dual_residual / (1.0 + s.c_two);
+  r.relative_primal_inf = r.primal_residual_inf / (1.0 + s.q_inf);
+  r.relative_dual_inf = r.dual_residual_inf / (1.0 + s.c_inf);
+  r.relative_gap =
+      r.absolute_gap / (1.0 + std::fabs(r.primal_objective) + std::fabs(r.dual_objective));
+  return r;
+}
+
+bool primal_ok(const anu_pdhg_residual& r, double tol, double abs_tol, bool inf) {
+  bool ok = r.relative_primal <= tol;
+  if (inf) ok = ok && r.relative_primal_inf <= tol;
+  if (abs_tol > 0.0) ok = ok && r.primal_residual_inf <= abs_tol;
+  return ok;
+}
+bool dual_ok(const anu_pdhg_residual& r, double tol, double abs_tol, bool inf) {
+  bool ok = r.relative_dual <= tol;
+  if (inf) ok = ok && r.relative_dual_inf <= tol;
+  if (abs_tol > 0.0) ok = ok && r.dual_residual_inf <= abs_tol;
+  return ok;
+}
+bool converged(const anu_pdhg_residual& r, double tol, double abs_tol, bool inf, double gap_tol) {
+  return primal_ok(r, tol, abs_tol, inf) && dual_ok(r, tol, abs_tol, inf) &&
+         r.relative_gap <= (gap_tol > 0.0 ? gap_tol : tol);
+}
+
+void set_message(anu_pdhg_result* r, const std::string& m) {
+  std::snprintf(r->message, sizeof(r->message), "%s", m.c_str());
+}
+
+constexpr int kRowTerms = RowCheckTerms<double, double>::NT;  // 9
+constexpr int kColTerms = ColCheckTerms<double>::NT;          // 9
+constexpr int kCheckTerms = kRowTerms + kColTerms;            // 18
+constexpr int kKktTerms = 5;  // primal_sq, q_dot_y, dual_sq, bound_term, c_dot_x
+
+// Pinned host staging that lives as long as a run.
+template <class T>
+struct Pinned {
+  T* p = nullptr;
+  size_t n = 0;
+  explicit Pinned(size_t count) : n(count) {
+    if (count) ANU_CUDA(cudaMallocHost(reinterpret_cast<void**>(&p), sizeof(T) * count));
+  }
+  ~Pinned() {
+    if (p) cudaFreeHost(p);
+  }
+  Pinned(const Pinned&) = delete;
+  Pinned& operator=(const Pinned&) = delete;
+};
+
+// Evaluates the FP64 check terms of scaled points (x~, y~) of K cases: fresh
+// products, then the row and column terms; returns terms[case][18] on host.
+void eval_points_terms(Problem& p, bool unit, int K, const std::vector<const CaseData*>& cases,
+                       const std::vector<std::vector<double>>& xs,
+                       const std::vector<std::vector<double>>& ys, std::vector<double>* terms) {
+  const int32_t n = p.n, m = p.m;
+  std::vector<double> hx(static_cast<size_t>(n) * K), hy(static_cast<size_t>(m) * K);
+  std::vector<double> hc(hx.size()), hl(hx.size()), hu(hx.size()), hq(hy.size());
+  for (int k = 0; k < K; ++k) {
+    for (int32_t j = 0; j < n; ++j) {
+      const size_t e = static_cast<size_t>(j) * K + k;
+      hx[e] = xs[k][j];
+      hc[e] = cases[k]->c[j];
+      hl[e] = cases[k]->lower[j];
+      hu[e] = cases[k]->upper[j];
+    }
+    for (int32_t i = 0; i < m; ++i) {
+      const size_t e = static_cast<size_t>(i) * K + k;
+      hy[e] = ys[k][i];
+      hq[e] = cases[k]->q[i];
+    }
+  }
+  DevBuf<double> dx(std::max<size_t>(hx.size(), 1)), dy(std::max<size_t>(hy.size(), 1)),
+      dc(dx.n), dl(dx.n), du(dx.n), dq(dy.n), kx(dy.n), kty(dx.n), out(kCheckTerms * K), part;
+  auto up = [&](DevBuf<double>& d, const std::vector<double>& h) {
+    if (!h.empty())
+      ANU_CUDA(cudaMemcpyAsync(d.p, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice,
+                               p.stream));
+  };
+  up(dx, hx);
+  up(dy, hy);
+  up(dc, hc);
+  up(dl, hl);
+  up(du, hu);
+  up(dq, hq);
+  product<double, double, double>(p, p.dk, dx.p, K, StoreEpi<double>{K, kx.p});
+  product<double, double, double>(p, p.dkt, dy.p, K, StoreEpi<double>{K, kty.p});
+  RowCheckTerms<double, double> rt{K, p.num_eq, kx.p, dy.p, dy.p, nullptr, nullptr, dq.p,
+                                   nullptr, unit ? nullptr : p.row_scale.p};
+  ColCheckTerms<double> ct{K, kty.p, dx.p, dx.p, nullptr, nullptr, dc.p, dl.p, du.p,
+                           unit ? nullptr : p.col_scale.p, nullptr, nullptr, nullptr};
+  reduce_terms(p, m, K, rt, part, out.p, kCheckTerms, 0);
+  reduce_terms(p, n, K, ct, part, out.p, kCheckTerms, kRowTerms);
+  terms->resize(static_cast<size_t>(kCheckTerms) * K);
+  ANU_CUDA(cudaMemcpyAsync(terms->data(), out.p, sizeof(double) * terms->size(),
+                           cudaMemcpyDeviceToHost, p.stream));
+  ANU_CUDA(cudaStreamSynchronize(p.stream));
+}
+
+// Per-case host state: the locals of solve_pdhg's loop (pdhg.cpp:466-757).
+struct CaseState {
+  double eta = 0.0, omega = 1.0;
+  bool anchor_needs_reset = true;
+  int32_t halpern_k = 0;
+  double movement = 0.0, epoch_start_movement = 0.0;
+  bool have_previous_restart = false;
+  double kkt_at_restart = 0.0;
+  double last_candidate_kkt = INFINITY;
+  double residual_at_restart = INFINITY;
+  double last_residual = INFINITY;
+  double weight_error_sum = 0.0, weight_error_previous = 0.0;
+  int32_t iterations_since_restart = 0;
+  int32_t next_polish_iteration = 0;
+  double sum_weight = 0.0;
+  bool active = true;
+  int32_t status = ANU_PDHG_ITERATION_LIMIT;
+  int32_t final_iteration = 0;
+  bool use_average = false;
+  bool have_polished = false;
+  std::vector<double> polished_x, polished_y;
+  anu_pdhg_residual polished_residual{};
+  ResidualScales scales{};
+};
+
+int32_t polish_budget(const anu_pdhg_options& o, int32_t at_iteration) {
+  int32_t budget = static_cast<int32_t>(o.polish_iteration_factor * static_cast<double>(at_iteration + 1));
+  budget = std::max(budget, o.polish_minimum_iterations);
+  budget = std::min(budget, o.polish_maximum_iterations);
+  return budget;
+}
+
+double kkt_value(const double* t, double omega) {
+  // t: primal_sq, q_dot_y, dual_sq, bound_term, c_dot_x (pdhg.cpp:336-339)
+  const double gap = t[4] - (t[1] + t[3]);
+  const double value = omega * omega * t[0] + t[2] / (omega * omega) + gap * gap;
+  return std::sqrt(value);
+}
+
+template <class T>
+struct Workspace {
+  int K = 0;
+  int32_t m = 0, n = 0;
+  // iteration vectors (case-interleaved)
+  DevBuf<T> x, x_bar, anchor_x, dx, c, lo, hi, x_next, sum_x, avg_x, x_restart, x_prev;
+  DevBuf<T> y, kx, anchor_y, anchor_kx, dy, q, k_dx, y_next, k_next, sum_y, avg_y, y_restart,
+      y_prev, ylo;
+  // FP64 island
+  DevBuf<double> kty64, ktdy64, kx64, c0, lo0, hi0, q0, los, his, qs;
+  DevBuf<StepParams> params;
+  DevBuf<double> w_table;
+  DevBuf<int32_t> mask;
+  DevBuf<double> partial, terms, kkt, weights;
+  std::map<std::pair<int, int>, cudaGraphExec_t> graphs;
+  ~Workspace() {
+    for (auto& g : graphs) cudaGraphExecDestroy(g.second);
+  }
+};
+
+template <class T>
+void upload_interleaved(cudaStream_t s, DevBuf<T>& dst, int32_t len, int K,
+                        const std::vector<const std::vector<double>*>& src) {
+  std::vector<T> h(static_cast<size_t>(len) * K);
+  for (int k = 0; k < K; ++k)
+    for (int32_t i = 0; i < len; ++i) h[static_cast<size_t>(i) * K + k] = static_cast<T>((*src[k])[i]);
+  dst.alloc(std::max<size_t>(h.size(), 1));
+  if (!h.empty())
+    ANU_CUDA(cudaMemcpyAsync(dst.p, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice, s));
+  ANU_CUDA(cudaStreamSynchronize(s));
+}
+
+template <class T>
+void download_case(cudaStream_t s, const DevBuf<T>& src, int32_t len, int K, int k,
+                   std::vector<double>* out, std::vector<T>* staging) {
+  staging->resize(static_cast<size_t>(len) * K);
+  if (!staging->empty())
+    ANU_CUDA(cudaMemcpyAsync(staging->data(), src.p, sizeof(T) * staging->size(),
+                             cudaMemcpyDeviceToHost, s));
+  ANU_CUDA(cudaStreamSynchronize(s));
+  out->resize(len);
+  for (int32_t i = 0; i < len; ++i) (*out)[i] = static_cast<double>((*staging)[static_cast<size_t>(i) * K + k]);
+}
+
+template <class T>
+void download_all(cudaStream_t s, const DevBuf<T>& src, int32_t len, int K,
+                  std::vector<std::vector<double>>* out) {
+  std::vector<T> staging(static_cast<size_t>(len) * K);
+  if (!staging.empty())
+    ANU_CUDA(cudaMemcpyAsync(staging.data(), src.p, sizeof(T) * staging.size(),
+                             cudaMemcpyDeviceToHost, s));
+  ANU_CUDA(cudaStreamSynchronize(s));
+  out->assign(K, std::vector<double>(len));
+  for (int k = 0; k < K; ++k)
+    for (int32_t i = 0; i < len; ++i)
+      (*out)[k][i] = static_cast<double>(staging[static_cast<size_t>(i) * K + k]);
+}
+
+template <class T>
+void run_cases_t(Problem& p, const std::vector<const CaseData*>& cases,
+                 const anu_pdhg_options& o, const std::vector<const std::vector<double>*>& warm_x,
+                 const std::vector<const std::vector<double>*>& warm_y,
+                 std::vector<CaseResult>* results, double start_time, bool unit);
+
+// Feasibility polishing of a set of cases (pdhg.cpp:666-751): a primal
+// sub-stack (c = 0) warm started from the seeds' x, then a dual sub-stack
+// (q = 0, finite bounds = 0) from the seeds' y, both on the same device
+// matrix with unit scaling and the parent's ||K~||, step and weight.
+template <class T>
+void run_polish(Problem& p, bool unit, const std::vector<const CaseData*>& parent,
+                const std::vector<int>& which, const std::vector<std::vector<double>>& seed_x,
+                const std::vector<std::vector<double>>& seed_y, int32_t budget,
+                const std::vector<CaseState>& states, const anu_pdhg_options& o,
+                double start_time, std::vector<std::vector<double>>* out_xs,
+                std::vector<std::vector<double>>* out_ys,
+                std::vector<std::vector<double>>* out_x, std::vector<std::vector<double>>* out_y,
+                std::vector<anu_pdhg_residual>* out_r, std::vector<int32_t>* spent) {
+  const size_t W = which.size();
+  std::vector<CaseData> primal(W), dual(W);
+  for (size_t w = 0; w < W; ++w) {
+    const CaseData& src = *parent[which[w]];
+    CaseData& a = primal[w];
+    a.c.assign(p.n, 0.0);
+    a.q = src.qs;
+    a.lower = src.ls;
+    a.upper = src.us;
+    a.objective_scale = src.objective_scale;
+    a.objective_offset = 0.0;
+    a.cs = a.c;
+    a.qs = a.q;
+    a.ls = a.lower;
+    a.us = a.upper;
+    CaseData& b = dual[w];
+    b.c = src.cs;
+    b.q.assign(p.m, 0.0);
+    b.lower = src.ls;
+    b.upper = src.us;
+    for (int32_t j = 0; j < p.n; ++j) {
+      if (b.lower[j] > -kInf) b.lower[j] = 0.0;
+      if (b.upper[j] < kInf) b.upper[j] = 0.0;
+    }
+    b.objective_scale = src.objective_scale;
+    b.objective_offset = 0.0;
+    b.cs = b.c;
+    b.qs = b.q;
+    b.ls = b.lower;
+    b.us = b.upper;
+  }
+  anu_pdhg_options sub = o;
+  sub.polish_feasibility = 0;
+  sub.polish_on_exit = 0;
+  sub.detect_infeasibility = 0;
+  sub.verbose = 0;
+  sub.known_matrix_norm = p.matrix_norm;
+  sub.ruiz_iterations = 0;
+  sub.pock_chambolle = 0;
+  sub.max_iterations = budget;
+  sub.termination_check_frequency =
+      std::max<int32_t>(10, std::min(o.termination_check_frequency, budget / 4));
+  sub.time_limit_seconds = std::fmax(0.0, o.time_limit_seconds - (now_seconds() - start_time));
+  // The sub-stacks get the parent's step size and weight per case.
+  std::vector<const CaseData*> pp(W), dd(W);
+  std::vector<std::vector<double>> zx(W, std::vector<double>(p.n, 0.0)),
+      zy(W, std::vector<double>(p.m, 0.0));
+  std::vector<const std::vector<double>*> wx(W), wy(W), wx2(W), wy2(W);
+  for (size_t w = 0; w < W; ++w) {
+    pp[w] = &primal[w];
+    dd[w] = &dual[w];
+    wx[w] = &seed_x[w];
+    wy[w] = &zy[w];
+    wx2[w] = &zx[w];
+    wy2[w] = &seed_y[w];
+  }
+  // Step size and primal weight differ per case, so each case runs as its own
+  // sub-stack when they differ; cases with equal values share one.
+  std::vector<CaseResult> pres(W), dres(W);
+  std::vector<bool> done(W, false);
+  for (size_t w0 = 0; w0 < W; ++w0) {
+    if (done[w0]) continue;
+    std::vector<size_t> group;
+    for (size_t w = w0; w < W; ++w)
+      if (!done[w] && states[which[w]].eta == states[which[w0]].eta &&
+          states[which[w]].omega == states[which[w0]].omega)
+        group.push_back(w);
+    anu_pdhg_options g = sub;
+    g.initial_step_size = states[which[w0]].eta;
+    g.initial_primal_weight = states[which[w0]].omega;
+    std::vector<const CaseData*> gp, gd;
+    std::vector<const std::vector<double>*> gwx, gwy, gwx2, gwy2;
+    for (size_t w : group) {
+      gp.push_back(pp[w]);
+      gd.push_back(dd[w]);
+      gwx.push_back(wx[w]);
+      gwy.push_back(wy[w]);
+      gwx2.push_back(wx2[w]);
+      gwy2.push_back(wy2[w]);
+      done[w] = true;
+    }
+    std::vector<CaseResult> rp, rd;
+    g.termination = ANU_TERMINATION_PRIMAL_FEASIBILITY;
+    run_cases_t<T>(p, gp, g, gwx, gwy, &rp, now_seconds(), true);
+    g.termination = ANU_TERMINATION_DUAL_FEASIBILITY;
+    run_cases_t<T>(p, gd, g, gwx2, gwy2, &rd, now_seconds(), true);
+    for (size_t i = 0; i < group.size(); ++i) {
+      pres[group[i]] = std::move(rp[i]);
+      dres[group[i]] = std::move(rd[i]);
+    }
+  }
+  out_xs->assign(W, {});
+  out_ys->assign(W, {});
+  out_x->assign(W, {});
+  out_y->assign(W, {});
+  spent->assign(W, 0);
+  std::vector<const CaseData*> evc(W);
+  for (size_t w = 0; w < W; ++w) {
+    (*spent)[w] = pres[w].r.iterations + dres[w].r.iterations;
+    (*out_xs)[w] = pres[w].x;  // unit-scaled sub-solve: its x is the scaled iterate
+    (*out_ys)[w] = dres[w].y;
+    (*out_x)[w].resize(p.n);
+    (*out_y)[w].resize(p.m);
+    for (int32_t j = 0; j < p.n; ++j)
+      (*out_x)[w][j] = unit ? pres[w].x[j] : p.scaling.col_scale[j] * pres[w].x[j];
+    for (int32_t i = 0; i < p.m; ++i)
+      (*out_y)[w][i] = unit ? dres[w].y[i] : p.scaling.row_scale[i] * dres[w].y[i];
+    evc[w] = parent[which[w]];
+  }
+  std::vector<double> terms;
+  eval_points_terms(p, unit, static_cast<int>(W), evc, *out_xs, *out_ys, &terms);
+  out_r->resize(W);
+  for (size_t w = 0; w < W; ++w)
+    (*out_r)[w] = residual_from_terms(&terms[w * kCheckTerms], &terms[w * kCheckTerms + kRowTerms],
+                                      states[which[w]].scales);
+}
+
+template <class T>
+void run_cases_t(Problem& p, const std::vector<const CaseData*>& cases,
+                 const anu_pdhg_options& o, const std::vector<const std::vector<double>*>& warm_x,
+                 const std::vector<const std::vector<double>*>& warm_y,
+                 std::vector<CaseResult>* results, double start_time, bool unit) {
+  const int K = static_cast<int>(cases.size());
+  const int32_t n = p.n, m = p.m;
+  results->assign(K, CaseResult{});
+  if (K == 0) return;
+  if (K > kMaxCasesPerRun) throw Error(ANU_ERR_INVALID, "a case stack holds at most 64 cases per run");
+  double phase_mark = now_seconds();
+  auto phase_end = [&phase_mark]() {
+    const double now = now_seconds();
+    const double s = now - phase_mark;
+    phase_mark = now;
+    return s;
+  };
+  const int64_t launches0 = p.launches;
+  std::vector<CaseState> S(K);
+  for (int k = 0; k < K; ++k) {
+    S[k].scales = {host_norm2(cases[k]->q), host_norm2(cases[k]->c), host_norminf(cases[k]->q),
+                   host_norminf(cases[k]->c)};
+    S[k].next_polish_iteration = o.polish_first_iteration;
+  }
+  const double tolerance = o.tolerance;
+  const double gap_tolerance = o.gap_tolerance > 0.0 ? o.gap_tolerance : tolerance;
+  const bool inf_norm = o.require_inf_norm_termination != 0;
+  auto passes = [&](const anu_pdhg_residual& r) {
+    switch (o.termination) {
+      case ANU_TERMINATION_PRIMAL_FEASIBILITY:
+        return primal_ok(r, tolerance, o.absolute_tolerance, inf_norm);
+      case ANU_TERMINATION_DUAL_FEASIBILITY:
+        return dual_ok(r, tolerance, o.absolute_tolerance, inf_norm);
+      default:
+        return converged(r, tolerance, o.absolute_tolerance, inf_norm, gap_tolerance);
+    }
+  };
+
+  // No constraint matrix content (pdhg.cpp:428-457): componentwise answer.
+  if (p.matrix_norm <= 0.0) {
+    std::vector<std::vector<double>> xs(K), ys(K);
+    for (int k = 0; k < K; ++k) {
+      const CaseData& cd = *cases[k];
+      xs[k].assign(n, 0.0);
+      ys[k].assign(m, 0.0);
+      for (int32_t j = 0; j < n; ++j) {
+        const double lo = cd.lower[j], hi = cd.upper[j], cj = cd.c[j];
+        double v = 0.0;
+        if (cj > 0.0) v = lo;
+        else if (cj < 0.0) v = hi;
+        else v = std::isfinite(lo) ? lo : (std::isfinite(hi) ? hi : 0.0);
+        xs[k][j] = std::isfinite(v) ? v : 0.0;
+      }
+    }
+    std::vector<std::vector<double>> sx = xs;
+    if (!unit)
+      for (int k = 0; k < K; ++k)
+        for (int32_t j = 0; j < n; ++j) sx[k][j] = xs[k][j] / p.scaling.col_scale[j];
+    std::vector<double> terms;
+    eval_points_terms(p, unit, K, cases, sx, ys, &terms);
+    for (int k = 0; k < K; ++k) {
+      CaseResult& R = (*results)[k];
+      R.r.residual = residual_from_terms(&terms[k * kCheckTerms], &terms[k * kCheckTerms + kRowTerms],
+                                         S[k].scales);
+      R.x = xs[k];
+      R.y = ys[k];
+      R.xs = sx[k];
+      R.ys = ys[k];
+      double cx = 0.0;
+      for (int32_t j = 0; j < n; ++j) cx += cases[k]->c[j] * xs[k][j];
+      R.r.objective = cases[k]->objective_scale * cx + cases[k]->objective_offset;
+      R.r.status = converged(R.r.residual, tolerance, o.absolute_tolerance, inf_norm, 0.0)
+                       ? ANU_PDHG_OPTIMAL
+                       : ANU_PDHG_NUMERICAL_ERROR;
+      set_message(&R.r, "no constraint matrix content");
+      R.r.matrix_norm_estimate = p.matrix_norm;
+      R.r.solve_seconds = now_seconds() - start_time;
+      R.r.kernel_launches = static_cast<int32_t>(p.launches - launches0);
+    }
+    return;
+  }
+
+  const bool halpern = o.halpern && o.restarts;
+  const double reflection = halpern ? o.reflection : 0.0;
+  const bool adaptive = o.adaptive_step_size && !o.constant_step_size;
+  const bool slow = adaptive || o.halpern_restart;
+  const bool averaging = o.restarts && !halpern;
+  const bool need_kkt_any = (o.restarts && !halpern) || (o.restarts && !o.restart_on_fixed_point) ||
+                            o.verbose;
+  const bool fp64 = std::is_same<T, double>::value;
+  if (slow && K != 1)
+    throw Error(ANU_ERR_INVALID,
+                "adaptive step sizes and the Halpern restart test need a single case");
+
+  // Step size and primal weight (pdhg.cpp:460-479), per case.
+  for (int k = 0; k < K; ++k) {
+    double eta = 0.9 / p.matrix_norm;
+    if (o.constant_step_size) eta = o.constant_step_scale / p.matrix_norm;
+    double omega = 1.0;
+    if (o.primal_weight_updates) {
+      const double cn = host_norm2(cases[k]->cs);
+      const double qn = host_norm2(cases[k]->qs);
+      if (cn > 1e-12 && qn > 1e-12) omega = cn / qn;
+    }
+    if (o.initial_step_size > 0.0) eta = o.initial_step_size;
+    if (o.initial_primal_weight > 0.0) omega = o.initial_primal_weight;
+    S[k].eta = eta;
+    S[k].omega = omega;
+  }
+
+  // Starting points (pdhg.cpp:481-503).
+  std::vector<std::vector<double>> x0(K), y0(K);
+  for (int k = 0; k < K; ++k) {
+    const CaseData& cd = *cases[k];
+    const bool warm = k < static_cast<int>(warm_x.size()) && warm_x[k] != nullptr &&
+                      warm_y[k] != nullptr && warm_x[k]->size() == static_cast<size_t>(n) &&
+                      warm_y[k]->size() == static_cast<size_t>(m);
+    x0[k].assign(n, 0.0);
+    y0[k].assign(m, 0.0);
+    if (warm) {
+      x0[k] = *warm_x[k];
+      y0[k] = *warm_y[k];
+      for (int32_t i = p.num_eq; i < m; ++i)
+        if (!(y0[k][i] > 0.0)) y0[k][i] = 0.0;
+    }
+    for (int32_t j = 0; j < n; ++j) {
+      const double lo = cd.ls[j], hi = cd.us[j];
+      double v = warm ? x0[k][j] : 0.0;
+      if (!std::isfinite(v)) v = 0.0;
+      if (v < lo) v = std::isfinite(lo) ? lo : 0.0;
+      if (v > hi) v = std::isfinite(hi) ? hi : 0.0;
+      x0[k][j] = v;
+    }
+  }
+
+  // Device working set.
+  Workspace<T> w;
+  w.K = K;
+  w.m = m;
+  w.n = n;
+  const cudaStream_t st = p.stream;
+  std::vector<const std::vector<double>*> vx(K), vy(K), vc(K), vl(K), vu(K), vq(K), oc(K),
+      ol(K), ou(K), oq(K), ylo(K);
+  bool any_ylo = false;
+  for (int k = 0; k < K; ++k) {
+    vx[k] = &x0[k];
+    vy[k] = &y0[k];
+    vc[k] = &cases[k]->cs;
+    vl[k] = &cases[k]->ls;
+    vu[k] = &cases[k]->us;
+    vq[k] = &cases[k]->qs;
+    oc[k] = &cases[k]->c;
+    ol[k] = &cases[k]->lower;
+    ou[k] = &cases[k]->upper;
+    oq[k] = &cases[k]->q;
+    if (!cases[k]->ylo.empty()) any_ylo = true;
+  }
+  const size_t NK = static_cast<size_t>(std::max(n, 1)) * K;
+  const size_t MK = static_cast<size_t>(std::max(m, 1)) * K;
+  upload_interleaved(st, w.x, n, K, vx);
+  upload_interleaved(st, w.y, m, K, vy);
+  upload_interleaved(st, w.c, n, K, vc);
+  upload_interleaved(st, w.lo, n, K, vl);
+  upload_interleaved(st, w.hi, n, K, vu);
+  upload_interleaved(st, w.q, m, K, vq);
+  upload_interleaved(st, w.c0, n, K, oc);
+  upload_interleaved(st, w.lo0, n, K, ol);
+  upload_interleaved(st, w.hi0, n, K, ou);
+  upload_interleaved(st, w.q0, m, K, oq);
+  if (o.detect_infeasibility) {
+    upload_interleaved(st, w.los, n, K, vl);
+    upload_interleaved(st, w.his, n, K, vu);
+    upload_interleaved(st, w.qs, m, K, vq);
+    w.ktdy64.alloc(NK);
+  }
+  if (any_ylo) {
+    std::vector<std::vector<double>> zeros(K);
+    for (int k = 0; k < K; ++k) {
+      if (cases[k]->ylo.empty()) {
+        zeros[k].assign(m, 0.0);
+        ylo[k] = &zeros[k];
+      } else {
+        ylo[k] = &cases[k]->ylo;
+      }
+    }
+    upload_interleaved(st, w.ylo, m, K, ylo);
+  }
+  w.x_bar.alloc(NK);
+  w.anchor_x.alloc(NK);
+  w.dx.alloc(NK);
+  w.kx.alloc(MK);
+  w.anchor_y.alloc(MK);
+  w.anchor_kx.alloc(MK);
+  w.dy.alloc(MK);
+  ANU_CUDA(cudaMemsetAsync(w.dx.p, 0, sizeof(T) * NK, st));
+  ANU_CUDA(cudaMemsetAsync(w.dy.p, 0, sizeof(T) * MK, st));
+  ANU_CUDA(cudaMemsetAsync(w.anchor_x.p, 0, sizeof(T) * NK, st));
+  ANU_CUDA(cudaMemsetAsync(w.anchor_y.p, 0, sizeof(T) * MK, st));
+  ANU_CUDA(cudaMemsetAsync(w.anchor_kx.p, 0, sizeof(T) * MK, st));
+  w.x_restart.alloc(NK);
+  w.y_restart.alloc(MK);
+  ANU_CUDA(cudaMemcpyAsync(w.x_restart.p, w.x.p, sizeof(T) * NK, cudaMemcpyDeviceToDevice, st));
+  ANU_CUDA(cudaMemcpyAsync(w.y_restart.p, w.y.p, sizeof(T) * MK, cudaMemcpyDeviceToDevice, st));
+  if (!o.pid_primal_weight) {
+    w.x_prev.alloc(NK);
+    w.y_prev.alloc(MK);
+    ANU_CUDA(cudaMemcpyAsync(w.x_prev.p, w.x.p, sizeof(T) * NK, cudaMemcpyDeviceToDevice, st));
+    ANU_CUDA(cudaMemcpyAsync(w.y_prev.p, w.y.p, sizeof(T) * MK, cudaMemcpyDeviceToDevice, st));
+  }
+  if (slow) {
+    w.x_next.alloc(NK);
+    w.y_next.alloc(MK);
+    w.k_next.alloc(MK);
+    w.k_dx.alloc(MK);
+    ANU_CUDA(cudaMemsetAsync(w.k_dx.p, 0, sizeof(T) * MK, st));
+  }
+  if (averaging) {
+    w.sum_x.alloc(NK);
+    w.sum_y.alloc(MK);
+    w.avg_x.alloc(NK);
+    w.avg_y.alloc(MK);
+    ANU_CUDA(cudaMemsetAsync(w.sum_x.p, 0, sizeof(T) * NK, st));
+    ANU_CUDA(cudaMemsetAsync(w.sum_y.p, 0, sizeof(T) * MK, st));
+  }
+  w.kty64.alloc(NK);
+  w.kx64.alloc(MK);
+  w.params.alloc(K);
+  w.mask.alloc(K);
+  w.terms.alloc(static_cast<size_t>(kCheckTerms) * K * 2);
+  w.kkt.alloc(static_cast<size_t>(kKktTerms) * K * 2);
+  w.weights.alloc(K);
+  const int F = o.termination_check_frequency;
+  w.w_table.alloc(static_cast<size_t>(std::max(F, 1)) * K);
+  Pinned<StepParams> h_params(K);
+  Pinned<double> h_w(static_cast<size_t>(std::max(F, 1)) * K);
+  Pinned<double> h_terms(static_cast<size_t>(kCheckTerms) * K * 2);
+  Pinned<double> h_kkt(static_cast<size_t>(kKktTerms) * K * 2);
+  Pinned<int32_t> h_mask(K);
+  Pinned<double> h_weights(K);
+
+  const RowCheckTerms<T, T>* dummy = nullptr;
+  (void)dummy;
+
+  // k_x = K~ x0 in FP64, rounded to T (pdhg.cpp:593).
+  product<double, T, double>(p, p.dk, w.x.p, K, StoreEpi<double>{K, w.kx64.p});
+  masked_copy<T, double>(p, m, K, nullptr, w.kx64.p, w.kx.p);
+
+  // Weighted KKT terms of (x, y) on the scaled problem, for every case.
+  auto kkt_terms = [&](const T* xv, const T* yv, double* out_dev) {
+    product<double, T, double>(p, p.dk, xv, K, StoreEpi<double>{K, w.kx64.p});
+    product<double, T, double>(p, p.dkt, yv, K, StoreEpi<double>{K, w.kty64.p});
+    // The KKT error is measured on the scaled problem: scaled q, c, bounds.
+    DevBuf<double>* qsc = &w.qs;
+    DevBuf<double> tmpq, tmpc, tmpl, tmph;
+    if (!o.detect_infeasibility) {
+      upload_interleaved(st, tmpq, m, K, vq);
+      upload_interleaved(st, tmpl, n, K, vl);
+      upload_interleaved(st, tmph, n, K, vu);
+      qsc = &tmpq;
+    }
+    upload_interleaved(st, tmpc, n, K, vc);
+    RowKktTerms<T> rt{K, p.num_eq, w.kx64.p, yv, qsc->p};
+    ColKktTerms<T> ct{K, w.kty64.p, xv, tmpc.p, o.detect_infeasibility ? w.los.p : tmpl.p,
+                      o.detect_infeasibility ? w.his.p : tmph.p};
+    reduce_terms(p, m, K, rt, w.partial, out_dev, kKktTerms, 0);
+    reduce_terms(p, n, K, ct, w.partial, out_dev, kKktTerms, 2);
+    ANU_CUDA(cudaStreamSynchronize(st));
+  };
+
+  if (o.restarts && !o.restart_on_fixed_point) {
+    // pdhg.cpp:604 - the KKT error at the starting point.
+    kkt_terms(w.x.p, w.y.p, w.kkt.p);
+    ANU_CUDA(cudaMemcpy(h_kkt.p, w.kkt.p, sizeof(double) * kKktTerms * K, cudaMemcpyDeviceToHost));
+    for (int k = 0; k < K; ++k) S[k].kkt_at_restart = kkt_value(&h_kkt.p[k * kKktTerms], S[k].omega);
+  }
+
+  // Per-chunk parameter upload.
+  auto upload_params = [&](int len) {
+    for (int k = 0; k < K; ++k) {
+      StepParams& P = h_params.p[k];
+      P.tau = S[k].eta / S[k].omega;
+      P.sigma = S[k].eta * S[k].omega;
+      P.gamma = reflection;
+      P.eta = S[k].eta;
+      P.active = S[k].active ? 1 : 0;
+      P.halpern = halpern ? 1 : 0;
+      P.reset_pending = (halpern && S[k].anchor_needs_reset) ? 1 : 0;
+      P.pad = 0;
+      for (int it = 0; it < len; ++it) {
+        double wv = 1.0;
+        if (halpern) {
+          const int32_t kk = P.reset_pending ? it - 1 : S[k].halpern_k + it;
+          if (!(P.reset_pending && it == 0))
+            wv = static_cast<double>(kk + 1) / static_cast<double>(kk + 2);
+        }
+        h_w.p[static_cast<size_t>(it) * K + k] = wv;
+      }
+    }
+    ANU_CUDA(cudaMemcpyAsync(w.params.p, h_params.p, sizeof(StepParams) * K, cudaMemcpyHostToDevice, st));
+    ANU_CUDA(cudaMemcpyAsync(w.w_table.p, h_w.p, sizeof(double) * len * K, cudaMemcpyHostToDevice, st));
+  };
+
+  const T* ylo_ptr = any_ylo ? w.ylo.p : nullptr;
+  // One fast-path iteration (in place).
+  auto launch_iteration = [&](int it, uint32_t flags) {
+    PrimalEpi<T> pe{K, it, flags, w.params.p, w.w_table.p, w.x.p, w.x.p, w.c.p, w.lo.p, w.hi.p,
+                    w.x_bar.p, w.anchor_x.p, w.dx.p, w.sum_x.p};
+    product<T, T, T>(p, p.dkt, w.y.p, K, pe);
+    DualEpi<T> de{K, it, flags, p.num_eq, w.params.p, w.w_table.p, w.y.p, w.y.p, w.q.p, w.kx.p,
+                  w.kx.p, w.anchor_y.p, w.anchor_kx.p, w.dy.p, nullptr, w.sum_y.p, ylo_ptr};
+    product<T, T, T>(p, p.dk, w.x_bar.p, K, de);
+  };
+
+  auto run_chunk_body = [&](int len, bool check_at_end) {
+    const uint32_t base_flags = averaging ? kAccumulate : 0u;
+    if (o.use_graphs) {
+      const auto key = std::make_pair(len, check_at_end ? 1 : 0);
+      auto found = w.graphs.find(key);
+      if (found == w.graphs.end()) {
+        cudaGraph_t graph = nullptr;
+        const int64_t before = p.launches;
+        ANU_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        for (int it = 0; it < len; ++it)
+          launch_iteration(it, base_flags | ((check_at_end && it == len - 1) ? kWriteDelta : 0u));
+        ANU_CUDA(cudaStreamEndCapture(st, &graph));
+        cudaGraphExec_t exec = nullptr;
+        ANU_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+        cudaGraphDestroy(graph);
+        p.launches = before;  // counted when launched
+        found = w.graphs.emplace(key, exec).first;
+      }
+      ANU_CUDA(cudaGraphLaunch(found->second, st));
+      p.launches += 2 * len;
+    } else {
+      for (int it = 0; it < len; ++it)
+        launch_iteration(it, base_flags | ((check_at_end && it == len - 1) ? kWriteDelta : 0u));
+    }
+  };
+  cudaEvent_t ev_begin = nullptr, ev_end = nullptr;
+  double device_iter_s = 0.0;
+  int64_t device_iters = 0;
+  if (o.profile) {
+    ANU_CUDA(cudaEventCreate(&ev_begin));
+    ANU_CUDA(cudaEventCreate(&ev_end));
+  }
+  struct EventGuard {
+    cudaEvent_t a, b;
+    ~EventGuard() {
+      if (a) cudaEventDestroy(a);
+      if (b) cudaEventDestroy(b);
+    }
+  } event_guard{ev_begin, ev_end};
+  auto run_chunk = [&](int len, bool check_at_end) {
+    if (o.profile) ANU_CUDA(cudaEventRecord(ev_begin, st));
+    run_chunk_body(len, check_at_end);
+    if (o.profile) {
+      ANU_CUDA(cudaEventRecord(ev_end, st));
+      ANU_CUDA(cudaEventSynchronize(ev_end));
+      float ms = 0.0f;
+      ANU_CUDA(cudaEventElapsedTime(&ms, ev_begin, ev_end));
+      device_iter_s += 1e-3 * ms;
+      device_iters += len;
+    }
+  };
+
+  // Check reductions for every case at once. `xv`, `yv` is the point judged
+  // (the iterate or its average); kx_maint the maintained K x when it may be
+  // reused. Writes terms[case][18] at `out_dev`.
+  auto check_terms = [&](const T* xv, const T* yv, const T* kx_maint, bool fresh_kx,
+                         double* out_dev) {
+    const double* kxp = nullptr;
+    if (fresh_kx) {
+      product<double, T, double>(p, p.dk, xv, K, StoreEpi<double>{K, w.kx64.p});
+      kxp = w.kx64.p;
+    }
+    product<double, T, double>(p, p.dkt, yv, K, StoreEpi<double>{K, w.kty64.p});
+    if (o.detect_infeasibility)
+      product<double, T, double>(p, p.dkt, w.dy.p, K, StoreEpi<double>{K, w.ktdy64.p});
+    const double* rs = unit ? nullptr : p.row_scale.p;
+    const double* cs = unit ? nullptr : p.col_scale.p;
+    if (fresh_kx) {
+      RowCheckTerms<T, double> rt{K, p.num_eq, kxp, yv, w.dy.p, w.y_restart.p,
+                                  o.pid_primal_weight ? nullptr : w.y_prev.p, w.q0.p,
+                                  o.detect_infeasibility ? w.qs.p : nullptr, rs};
+      reduce_terms(p, m, K, rt, w.partial, out_dev, kCheckTerms, 0);
+    } else {
+      RowCheckTerms<T, T> rt{K, p.num_eq, kx_maint, yv, w.dy.p, w.y_restart.p,
+                             o.pid_primal_weight ? nullptr : w.y_prev.p, w.q0.p,
+                             o.detect_infeasibility ? w.qs.p : nullptr, rs};
+      reduce_terms(p, m, K, rt, w.partial, out_dev, kCheckTerms, 0);
+    }
+    ColCheckTerms<T> ct{K, w.kty64.p, xv, w.dx.p, w.x_restart.p,
+                        o.pid_primal_weight ? nullptr : w.x_prev.p, w.c0.p, w.lo0.p, w.hi0.p, cs,
+                        o.detect_infeasibility ? w.ktdy64.p : nullptr,
+                        o.detect_infeasibility ? w.los.p : nullptr,
+                        o.detect_infeasibility ? w.his.p : nullptr};
+    reduce_terms(p, n, K, ct, w.partial, out_dev, kCheckTerms, kRowTerms);
+  };
+
+  auto set_mask = [&](const std::vector<int32_t>& mk) {
+    for (int k = 0; k < K; ++k) h_mask.p[k] = mk[k];
+    ANU_CUDA(cudaMemcpyAsync(w.mask.p, h_mask.p, sizeof(int32_t) * K, cudaMemcpyHostToDevice, st));
+  };
+
+  // Adopting the averaged candidate moves it on the device (pdhg.cpp:981-987).
+  auto adopt = [&](const std::vector<int32_t>& mk) {
+    bool any = false;
+    for (int k = 0; k < K; ++k) any = any || mk[k];
+    if (!any) return;
+    set_mask(mk);
+    masked_copy<T, T>(p, n, K, w.mask.p, w.avg_x.p, w.x.p);
+    masked_copy<T, T>(p, m, K, w.mask.p, w.avg_y.p, w.y.p);
+    ANU_CUDA(cudaStreamSynchronize(st));
+  };
+
+  int32_t iteration = 0;
+  std::vector<CaseResult>& R = *results;
+  for (int k = 0; k < K; ++k) {
+    R[k].r.matrix_norm_estimate = p.matrix_norm;
+  }
+  double t_setup = phase_end();
+  double t_iter = 0.0, t_checks = 0.0, t_polish = 0.0;
+
+  auto any_active = [&]() {
+    for (int k = 0; k < K; ++k)
+      if (S[k].active) return true;
+    return false;
+  };
+
+  while (iteration < o.max_iterations && any_active()) {
+    int32_t last;
+    bool is_check;
+    int len;
+    if (!slow) {
+      const int32_t next_check = (iteration / F + 1) * F - 1;
+      last = std::min(next_check, o.max_iterations - 1);
+      is_check = (last == next_check);
+      len = last - iteration + 1;
+      upload_params(len);
+      run_chunk(len, is_check);
+      for (int k = 0; k < K; ++k) {
+        CaseState& c = S[k];
+        if (!c.active) continue;
+        c.iterations_since_restart += len;
+        if (halpern) {
+          if (c.anchor_needs_reset) {
+            c.anchor_needs_reset = false;
+            c.halpern_k = len - 1;
+          } else {
+            c.halpern_k += len;
+          }
+        }
+        if (averaging)
+          for (int i = 0; i < len; ++i) c.sum_weight += c.eta;
+      }
+    } else {
+      // One iteration at a time, host-driven, as the reference does when the
+      // step size adapts (pdhg.cpp:759-897). Single case.
+      CaseState& c = S[0];
+      last = iteration;
+      len = 1;
+      is_check = ((iteration + 1) % F == 0);
+      const bool blend = halpern && !c.anchor_needs_reset;
+      const double hw = blend ? static_cast<double>(c.halpern_k + 1) / static_cast<double>(c.halpern_k + 2) : 1.0;
+      const bool need_movement = adaptive || o.halpern_restart || is_check;
+      for (int attempt = 0;; ++attempt) {
+        StepParams& P = h_params.p[0];
+        P.tau = c.eta / c.omega;
+        P.sigma = c.eta * c.omega;
+        P.gamma = reflection;
+        P.eta = c.eta;
+        P.active = 1;
+        P.halpern = blend ? 1 : 0;
+        P.reset_pending = 0;
+        h_w.p[0] = hw;
+        ANU_CUDA(cudaMemcpyAsync(w.params.p, h_params.p, sizeof(StepParams), cudaMemcpyHostToDevice, st));
+        ANU_CUDA(cudaMemcpyAsync(w.w_table.p, h_w.p, sizeof(double), cudaMemcpyHostToDevice, st));
+        PrimalEpi<T> pe{1, 0, kWriteDelta, w.params.p, w.w_table.p, w.x.p, w.x_next.p, w.c.p,
+                        w.lo.p, w.hi.p, w.x_bar.p, w.anchor_x.p, w.dx.p, nullptr};
+        product<T, T, T>(p, p.dkt, w.y.p, 1, pe);
+        DualEpi<T> de{1, 0, kWriteDelta, p.num_eq, w.params.p, w.w_table.p, w.y.p, w.y_next.p,
+                      w.q.p, w.kx.p, w.k_next.p, w.anchor_y.p, w.anchor_kx.p, w.dy.p, w.k_dx.p,
+                      nullptr, ylo_ptr};
+        product<T, T, T>(p, p.dk, w.x_bar.p, 1, de);
+        double interaction = 0.0;
+        if (!adaptive) {
+          if (need_movement) {
+            reduce_terms(p, n, 1, SquareTerms<T>{1, w.dx.p}, w.partial, w.kkt.p, 1, 0);
+            reduce_terms(p, m, 1, SquareTerms<T>{1, w.dy.p}, w.partial, w.kkt.p + 1, 1, 0);
+            ANU_CUDA(cudaMemcpyAsync(h_kkt.p, w.kkt.p, sizeof(double) * 2, cudaMemcpyDeviceToHost, st));
+            ANU_CUDA(cudaStreamSynchronize(st));
+            c.movement = c.omega * h_kkt.p[0] + h_kkt.p[1] / c.omega;
+          }
+          break;
+        }
+        reduce_terms(p, n, 1, SquareTerms<T>{1, w.dx.p}, w.partial, w.kkt.p, 1, 0);
+        reduce_terms(p, m, 1, StepRowTerms<T>{w.dy.p, w.k_dx.p}, w.partial, w.kkt.p + 1, 2, 0);
+        ANU_CUDA(cudaMemcpyAsync(h_kkt.p, w.kkt.p, sizeof(double) * 3, cudaMemcpyDeviceToHost, st));
+        ANU_CUDA(cudaStreamSynchronize(st));
+        interaction = std::fabs(h_kkt.p[1]);
+        c.movement = c.omega * h_kkt.p[0] + h_kkt.p[2] / c.omega;
+        double eta_bar = INFINITY;
+        if (interaction > 0.0) eta_bar = c.movement / (2.0 * interaction);
+        const double k1 = static_cast<double>(iteration + 1);
+        double eta_next = c.eta;
+        if (std::isfinite(eta_bar))
+          eta_next = std::fmin((1.0 - std::pow(k1, -0.3)) * eta_bar, (1.0 + std::pow(k1, -0.6)) * c.eta);
+        else
+          eta_next = (1.0 + std::pow(k1, -0.6)) * c.eta;
+        if (!(eta_next > 0.0) || !std::isfinite(eta_next)) eta_next = c.eta;
+        const bool accept = (c.eta <= eta_bar);
+        c.eta = eta_next;
+        if (accept) break;
+        if (attempt > 60) break;
+      }
+      std::swap(w.x, w.x_next);
+      std::swap(w.y, w.y_next);
+      std::swap(w.kx, w.k_next);
+      ++c.iterations_since_restart;
+      if (halpern) {
+        if (c.anchor_needs_reset) {
+          ANU_CUDA(cudaMemcpyAsync(w.anchor_x.p, w.x.p, sizeof(T) * n, cudaMemcpyDeviceToDevice, st));
+          ANU_CUDA(cudaMemcpyAsync(w.anchor_y.p, w.y.p, sizeof(T) * m, cudaMemcpyDeviceToDevice, st));
+          ANU_CUDA(cudaMemcpyAsync(w.anchor_kx.p, w.kx.p, sizeof(T) * m, cudaMemcpyDeviceToDevice, st));
+          c.anchor_needs_reset = false;
+          c.halpern_k = 0;
+          c.epoch_start_movement = c.movement;
+        } else {
+          ++c.halpern_k;
+        }
+      }
+      if (averaging) {
+        accumulate_kernel<T><<<grid_for(n, 256, 296), 256, 0, st>>>(n, c.eta, w.x.p, w.sum_x.p);
+        accumulate_kernel<T><<<grid_for(m, 256, 296), 256, 0, st>>>(m, c.eta, w.y.p, w.sum_y.p);
+        ANU_CUDA(cudaGetLastError());
+        p.launches += 2;
+        c.sum_weight += c.eta;
+      }
+      if (halpern && o.halpern_restart && !c.anchor_needs_reset && c.epoch_start_movement > 0.0 &&
+          c.halpern_k >= o.halpern_minimum_epoch) {
+        if (c.movement <= c.epoch_start_movement / 7.389056098930650) {
+          c.anchor_needs_reset = true;
+          ++R[0].r.restarts;
+        }
+      }
+    }
+    iteration = last + 1;
+    if (!is_check) continue;
+    ANU_CUDA(cudaStreamSynchronize(st));
+    t_iter += phase_end();
+
+    // ------------------------------------------------------------- check
+    const int32_t it_idx = last;
+    bool any_avg = false;
+    for (int k = 0; k < K; ++k) any_avg = any_avg || (S[k].active && averaging && S[k].sum_weight > 0.0);
+    const bool fresh_kx = !fp64 || !o.reuse_products;
+    check_terms(w.x.p, w.y.p, w.kx.p, fresh_kx, w.terms.p);
+    const bool need_kkt = need_kkt_any;
+    if (need_kkt) kkt_terms(w.x.p, w.y.p, w.kkt.p);
+    if (any_avg) {
+      for (int k = 0; k < K; ++k) h_weights.p[k] = S[k].sum_weight > 0.0 ? S[k].sum_weight : 1.0;
+      ANU_CUDA(cudaMemcpyAsync(w.weights.p, h_weights.p, sizeof(double) * K, cudaMemcpyHostToDevice, st));
+      average_kernel<T><<<grid_for(static_cast<int64_t>(n) * K, 256, 1184), 256, 0, st>>>(
+          static_cast<int64_t>(n) * K, K, w.weights.p, w.sum_x.p, w.avg_x.p);
+      average_kernel<T><<<grid_for(static_cast<int64_t>(m) * K, 256, 1184), 256, 0, st>>>(
+          static_cast<int64_t>(m) * K, K, w.weights.p, w.sum_y.p, w.avg_y.p);
+      ANU_CUDA(cudaGetLastError());
+      p.launches += 2;
+      kkt_terms(w.avg_x.p, w.avg_y.p, w.kkt.p + static_cast<size_t>(kKktTerms) * K);
+      check_terms(w.avg_x.p, w.avg_y.p, nullptr, true, w.terms.p + static_cast<size_t>(kCheckTerms) * K);
+    }
+    ANU_CUDA(cudaMemcpyAsync(h_terms.p, w.terms.p, sizeof(double) * kCheckTerms * K * (any_avg ? 2 : 1),
+                             cudaMemcpyDeviceToHost, st));
+    if (need_kkt || any_avg)
+      ANU_CUDA(cudaMemcpyAsync(h_kkt.p, w.kkt.p, sizeof(double) * kKktTerms * K * (any_avg ? 2 : 1),
+                               cudaMemcpyDeviceToHost, st));
+    ANU_CUDA(cudaStreamSynchronize(st));
+
+    std::vector<int32_t> adopt_mask(K, 0);
+    std::vector<anu_pdhg_residual> rr(K);
+    std::vector<double> candidate_kkt(K, 0.0);
+    std::vector<int> polish_cases;
+    for (int k = 0; k < K; ++k) {
+      CaseState& c = S[k];
+      if (!c.active) continue;
+      const double* tc = &h_terms.p[static_cast<size_t>(k) * kCheckTerms];
+      c.movement = c.omega * tc[kRowTerms + 4] + tc[3] / c.omega;
+      if (o.detect_infeasibility) {
+        const double scale = tc[6];
+        const bool bad = tc[7] > 0.0 || tc[kRowTerms + 8] > 0.0 || !(scale > 0.0);
+        if (!bad && (tc[8] - tc[kRowTerms + 7]) / scale > o.infeasibility_tolerance) {
+          c.status = ANU_PDHG_PRIMAL_INFEASIBLE;
+          set_message(&R[k].r, "Farkas certificate found in the dual iterate difference");
+          c.final_iteration = it_idx + 1;
+          c.active = false;
+          continue;
+        }
+      }
+      const bool need_average = averaging && c.sum_weight > 0.0;
+      const double current_kkt = need_kkt ? kkt_value(&h_kkt.p[static_cast<size_t>(k) * kKktTerms], c.omega) : 0.0;
+      c.use_average = false;
+      candidate_kkt[k] = current_kkt;
+      if (need_average) {
+        const double average_kkt =
+            kkt_value(&h_kkt.p[static_cast<size_t>(K + k) * kKktTerms], c.omega);
+        if (average_kkt < current_kkt) {
+          c.use_average = true;
+          candidate_kkt[k] = average_kkt;
+        }
+      }
+      const double* t = c.use_average ? &h_terms.p[static_cast<size_t>(K + k) * kCheckTerms] : tc;
+      const anu_pdhg_residual r = residual_from_terms(t, t + kRowTerms, c.scales);
+      rr[k] = r;
+      if (!std::isfinite(r.primal_residual) || !std::isfinite(r.dual_residual)) {
+        c.status = ANU_PDHG_NUMERICAL_ERROR;
+        set_message(&R[k].r, "iterates stopped being finite");
+        c.final_iteration = it_idx + 1;
+        adopt_mask[k] = c.use_average;
+        c.active = false;
+        continue;
+      }
+      if (passes(r)) {
+        c.status = ANU_PDHG_OPTIMAL;
+        c.final_iteration = it_idx + 1;
+        adopt_mask[k] = c.use_average;
+        c.active = false;
+        continue;
+      }
+      if (o.polish_feasibility && o.termination == ANU_TERMINATION_FULL &&
+          it_idx + 1 >= c.next_polish_iteration) {
+        while (c.next_polish_iteration <= it_idx + 1) c.next_polish_iteration *= 2;
+        const int32_t budget = polish_budget(o, it_idx);
+        if (r.relative_gap <= gap_tolerance && budget > 0) polish_cases.push_back(k);
+      }
+    }
+    adopt(adopt_mask);
+    if (!polish_cases.empty()) {
+      t_checks += phase_end();
+      std::vector<std::vector<double>> cur_x, cur_y, avg_x, avg_y;
+      download_all(st, w.x, n, K, &cur_x);
+      download_all(st, w.y, m, K, &cur_y);
+      if (any_avg) {
+        download_all(st, w.avg_x, n, K, &avg_x);
+        download_all(st, w.avg_y, m, K, &avg_y);
+      }
+      std::vector<std::vector<double>> sx, sy;
+      for (int k : polish_cases) {
+        sx.push_back(S[k].use_average ? avg_x[k] : cur_x[k]);
+        sy.push_back(S[k].use_average ? avg_y[k] : cur_y[k]);
+      }
+      std::vector<std::vector<double>> pxs, pys, px, py;
+      std::vector<anu_pdhg_residual> pr;
+      std::vector<int32_t> spent;
+      run_polish<T>(p, unit, cases, polish_cases, sx, sy, polish_budget(o, it_idx), S, o,
+                    start_time, &pxs, &pys, &px, &py, &pr, &spent);
+      t_polish += phase_end();
+      for (size_t i = 0; i < polish_cases.size(); ++i) {
+        const int k = polish_cases[i];
+        CaseState& c = S[k];
+        ++R[k].r.polish_attempts;
+        R[k].r.polish_iterations += spent[i];
+        if (converged(pr[i], tolerance, o.absolute_tolerance, inf_norm, gap_tolerance)) {
+          c.polished_x = px[i];
+          c.polished_y = py[i];
+          R[k].xs = pxs[i];
+          R[k].ys = pys[i];
+          c.polished_residual = pr[i];
+          c.have_polished = true;
+          R[k].r.polished = 1;
+          c.status = ANU_PDHG_OPTIMAL;
+          set_message(&R[k].r, "converged after feasibility polishing");
+          c.final_iteration = it_idx + 1;
+          c.active = false;
+        }
+      }
+    }
+    for (int k = 0; k < K; ++k) {
+      if (!S[k].active || !o.verbose || o.log_frequency <= 0) continue;
+      if ((it_idx + 1) % o.log_frequency == 0)
+        std::printf("  iter %7d  primal %.3e  dual %.3e  gap %.3e  kkt %.3e  eta %.3e  w %.3e\n",
+                    it_idx + 1, rr[k].relative_primal, rr[k].relative_dual, rr[k].relative_gap,
+                    candidate_kkt[k], S[k].eta, S[k].omega);
+    }
+    const bool out_of_time = now_seconds() - start_time > o.time_limit_seconds ||
+                             (o.stop != nullptr && *o.stop != 0);
+    std::fill(adopt_mask.begin(), adopt_mask.end(), 0);
+    if (out_of_time) {
+      for (int k = 0; k < K; ++k) {
+        if (!S[k].active) continue;
+        S[k].status = ANU_PDHG_TIME_LIMIT;
+        S[k].final_iteration = it_idx + 1;
+        adopt_mask[k] = S[k].use_average;
+        S[k].active = false;
+      }
+      adopt(adopt_mask);
+      t_checks += phase_end();
+      break;
+    }
+    if (!o.restarts) {
+      t_checks += phase_end();
+      continue;
+    }
+    std::vector<int32_t> restart_mask(K, 0);
+    bool any_restart = false;
+    for (int k = 0; k < K; ++k) {
+      CaseState& c = S[k];
+      if (!c.active) continue;
+      const double residual = std::sqrt(std::fmax(c.movement, 0.0));
+      const bool by_residual = o.restart_on_fixed_point != 0;
+      if (by_residual && !std::isfinite(c.residual_at_restart)) c.residual_at_restart = residual;
+      const double measure = by_residual ? residual : candidate_kkt[k];
+      const double at_restart = by_residual ? c.residual_at_restart : c.kkt_at_restart;
+      const double previous = by_residual ? c.last_residual : c.last_candidate_kkt;
+      const bool sufficient = measure <= 0.2 * at_restart;
+      const bool necessary = measure <= 0.8 * at_restart && measure > previous;
+      const bool too_long = static_cast<double>(c.iterations_since_restart) >=
+                            0.36 * static_cast<double>(it_idx + 1);
+      c.last_candidate_kkt = candidate_kkt[k];
+      c.last_residual = residual;
+      if (!(sufficient || necessary || too_long)) continue;
+      restart_mask[k] = 1;
+      adopt_mask[k] = c.use_average;
+      any_restart = true;
+    }
+    if (any_restart) {
+      adopt(adopt_mask);
+      // Fresh K x for the restarting cases (pdhg.cpp:1125).
+      product<double, T, double>(p, p.dk, w.x.p, K, StoreEpi<double>{K, w.kx64.p});
+      set_mask(restart_mask);
+      masked_copy<T, double>(p, m, K, w.mask.p, w.kx64.p, w.kx.p);
+      for (int k = 0; k < K; ++k) {
+        if (!restart_mask[k]) continue;
+        CaseState& c = S[k];
+        const double* t = c.use_average ? &h_terms.p[static_cast<size_t>(K + k) * kCheckTerms]
+                                        : &h_terms.p[static_cast<size_t>(k) * kCheckTerms];
+        if (o.primal_weight_updates && c.have_previous_restart) {
+          const double dxs = o.pid_primal_weight ? t[kRowTerms + 5] : t[kRowTerms + 6];
+          const double dys = o.pid_primal_weight ? t[4] : t[5];
+          const double delta_x = std::sqrt(dxs);
+          const double delta_y = std::sqrt(dys);
+          if (delta_x > 1e-12 && delta_y > 1e-12) {
+            double candidate = 0.0;
+            if (o.pid_primal_weight) {
+              const double e = std::log(c.omega * delta_x / delta_y);
+              c.weight_error_sum += e;
+              const double correction = o.primal_weight_kp * e + o.primal_weight_ki * c.weight_error_sum +
+                                        o.primal_weight_kd * (e - c.weight_error_previous);
+              c.weight_error_previous = e;
+              candidate = std::exp(std::log(c.omega) - correction);
+            } else {
+              candidate = std::exp(0.5 * std::log(delta_y / delta_x) + 0.5 * std::log(c.omega));
+            }
+            if (std::isfinite(candidate) && candidate > 1e-12 && candidate < 1e12) c.omega = candidate;
+          }
+        }
+        c.have_previous_restart = true;
+        c.sum_weight = 0.0;
+        c.anchor_needs_reset = true;
+        c.iterations_since_restart = 0;
+        c.last_candidate_kkt = INFINITY;
+        c.last_residual = INFINITY;
+        c.residual_at_restart = std::sqrt(std::fmax(c.movement, 0.0));
+        if (!o.restart_on_fixed_point) {
+          const double* kt = c.use_average ? &h_kkt.p[static_cast<size_t>(K + k) * kKktTerms]
+                                           : &h_kkt.p[static_cast<size_t>(k) * kKktTerms];
+          c.kkt_at_restart = kkt_value(kt, c.omega);
+        }
+        ++R[k].r.restarts;
+      }
+      if (!o.pid_primal_weight) {
+        masked_copy<T, T>(p, n, K, w.mask.p, w.x_restart.p, w.x_prev.p);
+        masked_copy<T, T>(p, m, K, w.mask.p, w.y_restart.p, w.y_prev.p);
+      }
+      masked_copy<T, T>(p, n, K, w.mask.p, w.x.p, w.x_restart.p);
+      masked_copy<T, T>(p, m, K, w.mask.p, w.y.p, w.y_restart.p);
+      if (averaging) {
+        masked_fill<T>(p, n, K, w.mask.p, static_cast<T>(0), w.sum_x.p);
+        masked_fill<T>(p, m, K, w.mask.p, static_cast<T>(0), w.sum_y.p);
+      }
+      ANU_CUDA(cudaStreamSynchronize(st));
+    }
+    t_checks += phase_end();
+  }
+  for (int k = 0; k < K; ++k)
+    if (S[k].active) {
+      S[k].final_iteration = iteration;
+      S[k].status = ANU_PDHG_ITERATION_LIMIT;
+    }
+
+  // Results (pdhg.cpp:1205-1285).
+  std::vector<std::vector<double>> fx, fy;
+  download_all(st, w.x, n, K, &fx);
+  download_all(st, w.y, m, K, &fy);
+  std::vector<double> fterms;
+  eval_points_terms(p, unit, K, cases, fx, fy, &fterms);
+  std::vector<int> exit_polish;
+  for (int k = 0; k < K; ++k) {
+    CaseState& c = S[k];
+    CaseResult& cr = R[k];
+    if (c.have_polished) {
+      cr.x = c.polished_x;
+      cr.y = c.polished_y;
+      cr.r.residual = c.polished_residual;
+      continue;
+    }
+    cr.xs = fx[k];
+    cr.ys = fy[k];
+    cr.x.resize(n);
+    cr.y.resize(m);
+    for (int32_t j = 0; j < n; ++j) cr.x[j] = unit ? fx[k][j] : p.scaling.col_scale[j] * fx[k][j];
+    for (int32_t i = 0; i < m; ++i) cr.y[i] = unit ? fy[k][i] : p.scaling.row_scale[i] * fy[k][i];
+    cr.r.residual = residual_from_terms(&fterms[static_cast<size_t>(k) * kCheckTerms],
+                                        &fterms[static_cast<size_t>(k) * kCheckTerms + kRowTerms],
+                                        c.scales);
+    const bool worth = o.polish_feasibility && o.polish_on_exit &&
+                       o.termination == ANU_TERMINATION_FULL && c.status != ANU_PDHG_OPTIMAL &&
+                       c.status != ANU_PDHG_PRIMAL_INFEASIBLE &&
+                       c.status != ANU_PDHG_NUMERICAL_ERROR &&
+                       std::isfinite(cr.r.residual.primal_residual) &&
+                       std::isfinite(cr.r.residual.dual_residual) &&
+                       now_seconds() - start_time < o.time_limit_seconds;
+    if (worth && polish_budget(o, c.final_iteration) > 0) exit_polish.push_back(k);
+  }
+  if (!exit_polish.empty()) {
+    // All cases that reach here stopped at the same iteration count.
+    std::vector<std::vector<double>> sx, sy;
+    for (int k : exit_polish) {
+      sx.push_back(fx[k]);
+      sy.push_back(fy[k]);
+    }
+    std::vector<std::vector<double>> pxs, pys, px, py;
+    std::vector<anu_pdhg_residual> pr;
+    std::vector<int32_t> spent;
+    run_polish<T>(p, unit, cases, exit_polish, sx, sy, polish_budget(o, S[exit_polish[0]].final_iteration),
+                  S, o, start_time, &pxs, &pys, &px, &py, &pr, &spent);
+    t_polish += phase_end();
+    for (size_t i = 0; i < exit_polish.size(); ++i) {
+      const int k = exit_polish[i];
+      CaseResult& cr = R[k];
+      ++cr.r.polish_attempts;
+      cr.r.polish_iterations += spent[i];
+      const anu_pdhg_residual& cur = cr.r.residual;
+      const anu_pdhg_residual& tr = pr[i];
+      const double gap_ceiling = std::fmax(gap_tolerance, cur.relative_gap);
+      const bool improved = tr.relative_primal <= cur.relative_primal &&
+                            tr.relative_dual <= cur.relative_dual &&
+                            (tr.relative_primal < cur.relative_primal ||
+                             tr.relative_dual < cur.relative_dual);
+      if (improved && tr.relative_gap <= gap_ceiling) {
+        cr.x = px[i];
+        cr.y = py[i];
+        cr.xs = pxs[i];
+        cr.ys = pys[i];
+        cr.r.residual = tr;
+        cr.r.polished = 1;
+        if (converged(tr, tolerance, o.absolute_tolerance, inf_norm, gap_tolerance)) {
+          S[k].status = ANU_PDHG_OPTIMAL;
+          set_message(&cr.r, "converged after feasibility polishing");
+        } else if (cr.r.message[0] == '\0') {
+          set_message(&cr.r, "feasibility polished");
+        } else {
+          set_message(&cr.r, std::string(cr.r.message) + ", feasibility polished");
+        }
+      }
+    }
+  }
+  t_checks += phase_end();
+  for (int k = 0; k < K; ++k) {
+    CaseResult& cr = R[k];
+    double cx = 0.0;
+    for (int32_t j = 0; j < n; ++j) cx += cases[k]->c[j] * cr.x[j];
+    cr.r.objective = cases[k]->objective_scale * cx + cases[k]->objective_offset;
+    cr.r.iterations = S[k].final_iteration;
+    cr.r.status = S[k].status;
+    cr.r.final_step_size = S[k].eta;
+    cr.r.final_primal_weight = S[k].omega;
+    cr.r.solve_seconds = now_seconds() - start_time;
+    cr.r.phases.setup = t_setup;
+    cr.r.phases.iterating = t_iter;
+    cr.r.phases.checks = t_checks;
+    cr.r.phases.polishing = t_polish;
+    cr.r.kernel_launches = static_cast<int32_t>(p.launches - launches0);
+    cr.r.device_iteration_seconds = device_iter_s;
+    cr.r.device_iterations = device_iters;
+  }
+}
+
+}  // namespace
+
+void evaluate_point(Problem& p, const CaseData& cd, const std::vector<double>& x,
+                    const std::vector<double>& y, anu_pdhg_residual* out) {
+  std::vector<std::vector<double>> xs(1, x), ys(1, y);
+  std::vector<double> terms;
+  eval_points_terms(p, true, 1, {&cd}, xs, ys, &terms);
+  const ResidualScales s{host_norm2(cd.q), host_norm2(cd.c), host_norminf(cd.q),
+                         host_norminf(cd.c)};
+  *out = residual_from_terms(terms.data(), terms.data() + kRowTerms, s);
+}
+
+void run_cases(Problem& problem, const std::vector<const CaseData*>& cases,
+               const anu_pdhg_options& options,
+               const std::vector<const std::vector<double>*>& warm_x,
+               const std::vector<const std::vector<double>*>& warm_y,
+               std::vector<CaseResult>* results, double start_time) {
+  ANU_CUDA(cudaSetDevice(problem.device));
+  if (problem.precision == ANU_PRECISION_FP32)
+    run_cases_t<float>(problem, cases, options, warm_x, warm_y, results, start_time,
+                       problem.unit_scaling);
+  else
+    run_cases_t<double>(problem, cases, options, warm_x, warm_y, results, start_time,
+                        problem.unit_scaling);
+}
+
+}  // namespace anu
+
+// =============================================================== C ABI
+
+using anu::Error;
+
+namespace {
+
+template <class F>
+int guarded(F&& body) {
+  try {
+    anu::clear_last_error();
+    body();
+    return ANU_OK;
+  } catch (const Error& e) {
+    anu::set_last_error(e.code, e.what());
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    anu::set_last_error(ANU_ERR_MEMORY, "host allocation failed");
+    return ANU_ERR_MEMORY;
+  } catch (const std::exception& e) {
+    anu::set_last_error(ANU_ERR_INTERNAL, e.what());
+    return ANU_ERR_INTERNAL;
+  }
+}
+
+void fill_result(const anu::Problem& p, const anu::CaseResult& cr, double scaling_s, double norm_s,
+                 anu_pdhg_result* out) {
+  *out = cr.r;
+  out->phases.scaling = scaling_s;
+  out->phases.matrix_norm = norm_s;
+  out->row_spread_before = p.scaling.row_spread_before;
+  out->row_spread_after = p.scaling.row_spread_after;
+  out->col_spread_before = p.scaling.col_spread_before;
+  out->col_spread_after = p.scaling.col_spread_after;
+  out->matrix_norm_estimate = p.matrix_norm;
+}
+
+}  // namespace
+
+struct anu_pdhg {
+  std::unique_ptr<anu::Problem> problem;
+  anu::CaseData data;
+  anu_pdhg_options options;
+  double scaling_seconds = 0.0;
+  double norm_seconds = 0.0;
+};
+
+struct anu_pdhg_batch {
+  std::unique_ptr<anu::Problem> problem;
+  std::vector<anu::CaseData> cases;
+  anu_pdhg_options options;
+  double scaling_seconds = 0.0;
+  double norm_seconds = 0.0;
+};
+
+extern "C" {
+
+const char* anu_pdhg_version(void) { return "anu-pdhg-b200 0.1.0 sm_100a"; }
+
+void anu_pdhg_default_options(anu_pdhg_options* o) {
+  if (o == nullptr) return;
+  std::memset(o, 0, sizeof(*o));
+  o->tolerance = 1e-6;
+  o->gap_tolerance = 0.0;
+  o->max_iterations = 200000;
+  o->time_limit_seconds = 300.0;
+  o->termination_check_frequency = 40;
+  o->absolute_tolerance = 0.0;
+  o->require_inf_norm_termination = 1;
+  o->adaptive_step_size = 1;
+  o->primal_weight_updates = 1;
+  o->restarts = 1;
+  o->halpern = 1;
+  o->halpern_restart = 0;
+  o->halpern_minimum_epoch = 16;
+  o->polish_feasibility = 1;
+  o->polish_first_iteration = 100;
+  o->polish_iteration_factor = 0.125;
+  o->polish_minimum_iterations = 40;
+  o->polish_maximum_iterations = 20000;
+  o->polish_on_exit = 1;
+  o->reflection = 1.0;
+  o->constant_step_size = 1;
+  o->constant_step_scale = 0.90;
+  o->restart_on_fixed_point = 1;
+  o->pid_primal_weight = 1;
+  o->primal_weight_kp = 0.5;
+  o->primal_weight_ki = 0.0;
+  o->primal_weight_kd = 0.3;
+  o->ruiz_iterations = 10;
+  o->pock_chambolle = 1;
+  o->reuse_products = 1;
+  o->detect_infeasibility = 1;
+  o->infeasibility_tolerance = 1e-8;
+  o->termination = ANU_TERMINATION_FULL;
+  o->known_matrix_norm = 0.0;
+  o->initial_step_size = 0.0;
+  o->initial_primal_weight = 0.0;
+  o->verbose = 0;
+  o->log_frequency = 5000;
+  o->stop = nullptr;
+  o->precision = ANU_PRECISION_FP64;
+  o->refinement_rounds = 0;
+  o->refinement_inner_tolerance = 0.0;
+  o->device = 0;
+  o->use_graphs = 1;
+  o->profile = 0;
+}
+
+int anu_last_error(char* buf, int32_t size) { return anu::copy_last_error(buf, size); }
+
+int32_t anu_device_count(void) {
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return count;
+}
+
+int anu_pdhg_create(const anu_lp* lp, const anu_pdhg_options* options, anu_pdhg** handle) {
+  return guarded([&] {
+    if (lp == nullptr || options == nullptr || handle == nullptr)
+      throw Error(ANU_ERR_INVALID, "null argument");
+    *handle = nullptr;
+    anu::validate_options(*options);
+    const std::string e = anu::validate_lp(*lp);
+    if (!e.empty()) throw Error(ANU_ERR_INVALID, "invalid LP: " + e);
+    auto h = std::make_unique<anu_pdhg>();
+    h->options = *options;
+    h->problem = anu::make_problem(*lp, *options, &h->scaling_seconds, &h->norm_seconds);
+    h->data = anu::make_case(*h->problem, lp->c, lp->q, lp->lower, lp->upper, lp->objective_scale,
+                             lp->objective_offset);
+    *handle = h.release();
+  });
+}
+
+int anu_pdhg_run(anu_pdhg* h, const double* warm_x, const double* warm_y, double* x, double* y,
+                 anu_pdhg_result* result) {
+  return guarded([&] {
+    if (h == nullptr || result == nullptr) throw Error(ANU_ERR_INVALID, "null argument");
+    const double start = anu::now_seconds();
+    std::vector<double> wx, wy;
+    std::vector<const std::vector<double>*> vwx(1, nullptr), vwy(1, nullptr);
+    if (warm_x != nullptr && warm_y != nullptr) {
+      wx.assign(warm_x, warm_x + h->problem->n);
+      wy.assign(warm_y, warm_y + h->problem->m);
+      vwx[0] = &wx;
+      vwy[0] = &wy;
+    }
+    std::vector<anu::CaseResult> res;
+    anu::run_cases(*h->problem, {&h->data}, h->options, vwx, vwy, &res, start);
+    fill_result(*h->problem, res[0], h->scaling_seconds, h->norm_seconds, result);
+    if (x) std::copy(res[0].x.begin(), res[0].x.end(), x);
+    if (y) std::copy(res[0].y.begin(), res[0].y.end(), y);
+  });
+}
+
+void anu_pdhg_destroy(anu_pdhg* h) { delete h; }
+
+int anu_pdhg_solve(const anu_lp* lp, const anu_pdhg_options* options, const double* warm_x,
+                   const double* warm_y, double* x, double* y, anu_pdhg_result* result) {
+  const double t0 = anu::now_seconds();
+  anu_pdhg* h = nullptr;
+  int rc = anu_pdhg_create(lp, options, &h);
+  if (rc != ANU_OK) return rc;
+  rc = anu_pdhg_run(h, warm_x, warm_y, x, y, result);
+  if (rc == ANU_OK) result->solve_seconds = anu::now_seconds() - t0;
+  anu_pdhg_destroy(h);
+  return rc;
+}
+
+int anu_estimate_matrix_norm(const anu_lp* lp, int32_t iterations, double tolerance,
+                             double* norm) {
+  return guarded([&] {
+    if (lp == nullptr || norm == nullptr) throw Error(ANU_ERR_INVALID, "null argument");
+    const std::string e = anu::validate_lp(*lp);
+    if (!e.empty()) throw Error(ANU_ERR_INVALID, "invalid LP: " + e);
+    anu_pdhg_options o;
+    anu_pdhg_default_options(&o);
+    o.ruiz_iterations = 0;
+    o.pock_chambolle = 0;
+    o.known_matrix_norm = 1.0;  // skip the default estimate; measured below
+    auto p = anu::make_problem(*lp, o, nullptr, nullptr);
+    *norm = anu::device_matrix_norm(*p, iterations, tolerance);
+  });
+}
+
+int anu_evaluate_residual(const anu_lp* lp, const double* x, const double* y,
+                          anu_pdhg_residual* out) {
+  return guarded([&] {
+    if (lp == nullptr || x == nullptr || y == nullptr || out == nullptr)
+      throw Error(ANU_ERR_INVALID, "null argument");
+    const std::string e = anu::validate_lp(*lp);
+    if (!e.empty()) throw Error(ANU_ERR_INVALID, "invalid LP: " + e);
+    anu_pdhg_options o;
+    anu_pdhg_default_options(&o);
+    o.ruiz_iterations = 0;
+    o.pock_chambolle = 0;
+    o.known_matrix_norm = 1.0;
+    auto p = anu::make_problem(*lp, o, nullptr, nullptr);
+    p->unit_scaling = true;
+    anu::CaseData cd = anu::make_case(*p, lp->c, lp->q, lp->lower, lp->upper,
+                                      lp->objective_scale, lp->objective_offset);
+    anu::evaluate_point(*p, cd, std::vector<double>(x, x + lp->k.cols),
+                        std::vector<double>(y, y + lp->k.rows), out);
+  });
+}
+
+int anu_pdhg_batch_create(const anu_lp* base, int32_t num_cases, const double* c,
+                          const double* q, const double* lower, const double* upper,
+                          const anu_pdhg_options* options, anu_pdhg_batch** handle) {
+  return guarded([&] {
+    if (base == nullptr || options == nullptr || handle == nullptr)
+      throw Error(ANU_ERR_INVALID, "null argument");
+    *handle = nullptr;
+    if (num_cases < 1) throw Error(ANU_ERR_INVALID, "num_cases < 1");
+    anu::validate_options(*options);
+    const std::string e = anu::validate_lp(*base);
+    if (!e.empty()) throw Error(ANU_ERR_INVALID, "invalid LP: " + e);
+    const int32_t n = base->k.cols, m = base->k.rows;
+    for (int32_t k = 0; k < num_cases; ++k) {
+      const double* lo = lower ? lower + static_cast<size_t>(k) * n : base->lower;
+      const double* hi = upper ? upper + static_cast<size_t>(k) * n : base->upper;
+      for (int32_t j = 0; j < n; ++j)
+        if (lo[j] > hi[j]) throw Error(ANU_ERR_INVALID, "empty bound interval in case " + std::to_string(k));
+      const double* qq = q ? q + static_cast<size_t>(k) * m : base->q;
+      for (int32_t i = 0; i < m; ++i)
+        if (!std::isfinite(qq[i])) throw Error(ANU_ERR_INVALID, "rhs is not finite in case " + std::to_string(k));
+    }
+    auto h = std::make_unique<anu_pdhg_batch>();
+    h->options = *options;
+    h->problem = anu::make_problem(*base, *options, &h->scaling_seconds, &h->norm_seconds);
+    h->cases.reserve(num_cases);
+    for (int32_t k = 0; k < num_cases; ++k) {
+      h->cases.push_back(anu::make_case(
+          *h->problem, c ? c + static_cast<size_t>(k) * n : base->c,
+          q ? q + static_cast<size_t>(k) * m : base->q,
+          lower ? lower + static_cast<size_t>(k) * n : base->lower,
+          upper ? upper + static_cast<size_t>(k) * n : base->upper, base->objective_scale,
+          base->objective_offset));
+    }
+    *handle = h.release();
+  });
+}
+
+int anu_pdhg_batch_solve(anu_pdhg_batch* h, double* x, double* y, anu_pdhg_result* results) {
+  return guarded([&] {
+    if (h == nullptr || results == nullptr) throw Error(ANU_ERR_INVALID, "null argument");
+    const int32_t n = h->problem->n, m = h->problem->m;
+    const int total = static_cast<int>(h->cases.size());
+    // Stacks larger than one run's capacity go through in slices.
+    for (int base = 0; base < total; base += anu::kMaxCasesPerRun) {
+      const int count = std::min(anu::kMaxCasesPerRun, total - base);
+      const double start = anu::now_seconds();
+      std::vector<const anu::CaseData*> cs(count);
+      for (int k = 0; k < count; ++k) cs[k] = &h->cases[base + k];
+      std::vector<const std::vector<double>*> none(count, nullptr);
+      std::vector<anu::CaseResult> res;
+      anu::run_cases(*h->problem, cs, h->options, none, none, &res, start);
+      for (int k = 0; k < count; ++k) {
+        fill_result(*h->problem, res[k], h->scaling_seconds, h->norm_seconds, &results[base + k]);
+        if (x) std::copy(res[k].x.begin(), res[k].x.end(), x + static_cast<size_t>(base + k) * n);
+        if (y) std::copy(res[k].y.begin(), res[k].y.end(), y + static_cast<size_t>(base + k) * m);
+      }
+    }
+  });
+}
+
+void anu_pdhg_batch_destroy(anu_pdhg_batch* h) { delete h; }
+
+}  // extern "C"

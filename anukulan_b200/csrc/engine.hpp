@@ -1,0 +1,150 @@
+// Internal declarations of the engine (not part of the C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/anu_pdhg.h"
+#include "kernels.cuh"
+#include "launch.cuh"
+#include "prep.hpp"
+
+namespace anu {
+
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+void cuda_check(cudaError_t status, const char* what);
+#define ANU_CUDA(call) ::anu::cuda_check((call), #call)
+
+void set_last_error(int code, const std::string& message);
+void clear_last_error();
+
+// Device memory owned by RAII.
+template <class T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  explicit DevBuf(size_t count) { alloc(count); }
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+  DevBuf& operator=(DevBuf&& o) noexcept {
+    if (this != &o) {
+      release();
+      p = o.p;
+      n = o.n;
+      o.p = nullptr;
+      o.n = 0;
+    }
+    return *this;
+  }
+  ~DevBuf() { release(); }
+  void alloc(size_t count) {
+    release();
+    n = count;
+    if (count == 0) return;
+    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&p), sizeof(T) * count);
+    if (e != cudaSuccess) {
+      p = nullptr;
+      throw Error(ANU_ERR_MEMORY, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    }
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  T* get() const { return p; }
+};
+
+// One sparse matrix on the device: structure, FP64 values, optional FP32
+// values, and the row-block schedule of the staged SpMV.
+struct DevCsr {
+  int32_t rows = 0, cols = 0, nnz = 0;
+  DevBuf<int32_t> start, index;
+  DevBuf<double> v64;
+  DevBuf<float> v32;
+  DevBuf<RowBlockDev> blocks;
+  int32_t num_blocks = 0;
+  void upload(const HostCsr& a, bool with_fp32, cudaStream_t s);
+  template <class V>
+  CsrView<V> view() const;
+};
+
+// Everything that depends on the matrix alone: the scaled matrix and its
+// transpose (host and device), the scaling, ||K~||, the stream.
+struct Problem : Exec {
+  int32_t m = 0, n = 0, num_eq = 0;
+  int precision = ANU_PRECISION_FP64;
+  HostCsr k;   // scaled K~
+  HostCsr kt;  // its transpose
+  Scaling scaling;
+  ScalingSweeps sweeps;
+  bool unit_scaling = false;  // sub-solves run on already-scaled data
+  DevCsr dk, dkt;
+  DevBuf<double> row_scale, col_scale;
+  double matrix_norm = 0.0;
+  bool owns_stream = false;
+  int device = 0;
+  ~Problem();
+};
+
+// One case: the unscaled data the convergence test judges, the scaled data
+// the iteration runs on.
+struct CaseData {
+  std::vector<double> c, q, lower, upper;      // original
+  std::vector<double> cs, qs, ls, us;          // scaled
+  std::vector<double> ylo;                     // dual floor (refinement), empty = 0
+  double objective_scale = 1.0;
+  double objective_offset = 0.0;
+};
+
+struct CaseResult {
+  anu_pdhg_result r{};
+  std::vector<double> x;  // unscaled
+  std::vector<double> y;
+  std::vector<double> xs;  // scaled iterate the result came from
+  std::vector<double> ys;
+};
+
+// Builds the problem from a validated LP: copies, scales, uploads, and
+// estimates ||K~|| unless known_matrix_norm is given.
+std::unique_ptr<Problem> make_problem(const anu_lp& lp, const anu_pdhg_options& o,
+                                      double* scaling_seconds, double* norm_seconds);
+CaseData make_case(const Problem& p, const double* c, const double* q, const double* lower,
+                   const double* upper, double objective_scale, double objective_offset);
+
+// Runs K cases sharing `problem` to termination (solve_pdhg semantics per
+// case). warm_x / warm_y: per case, scaled-space starts or empty.
+void run_cases(Problem& problem, const std::vector<const CaseData*>& cases,
+               const anu_pdhg_options& options,
+               const std::vector<const std::vector<double>*>& warm_x,
+               const std::vector<const std::vector<double>*>& warm_y,
+               std::vector<CaseResult>* results, double start_time);
+
+// ||K~|| by power iteration on the device, FP64 (pdhg.cpp:223-282).
+double device_matrix_norm(Problem& p, int iterations, double tolerance);
+
+// Cases one run of the case-stack kernels carries (lanes x cases per lane).
+constexpr int kMaxCasesPerRun = 64;
+
+// FP64 convergence measures of one point against an unscaled LP held by a
+// unit-scaled problem (evaluate_residual, pdhg.cpp:112-174).
+void evaluate_point(Problem& p, const CaseData& cd, const std::vector<double>& x,
+                    const std::vector<double>& y, anu_pdhg_residual* out);
+
+int copy_last_error(char* buf, int32_t size);
+
+std::string validate_lp(const anu_lp& lp);
+void validate_options(const anu_pdhg_options& o);
+
+}  // namespace anu

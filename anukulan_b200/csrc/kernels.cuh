@@ -1,0 +1,595 @@
+// sm_100a kernels of the PDHG engine.
+//
+// Two sparse-product shapes, both reading A through a CSR with int32 indices:
+//
+//  * rows_kernel - one LP. CSR-adaptive: each CTA takes one row block (a run
+//    of consecutive rows holding at most kBlockNnz nonzeros, or one longer
+//    row). The block's value*x products are streamed into shared memory with
+//    coalesced loads of the index and value arrays, summed per row (one
+//    thread per row while rows are short, a shuffle group when they are long,
+//    a CTA-wide tree for a row longer than the block), and the row sums feed
+//    an epilogue over the block's rows - contiguous, so the epilogue's vector
+//    traffic is coalesced too. The epilogue is where the PDHG step is fused:
+//    the primal step, bound projection, reflection and Halpern blend after
+//    K'y, the dual step, cone projection and K x bookkeeping after K x_bar.
+//
+//  * cases_kernel - a case stack of K LPs sharing A, vectors case-interleaved
+//    (element (row, case) at row*K + case). A group of L lanes takes a row;
+//    lane l owns cases l, l+L, ... Every nonzero of A is loaded once per row
+//    group and serves all K cases; the x loads of the K cases are one
+//    contiguous run. Each (row, case) sum is accumulated left to right.
+//
+// Sums are deterministic: the order depends only on the row-block schedule,
+// never on timing. FP64 arithmetic in the epilogues and sums is written with
+// explicit round-to-nearest intrinsics so nvcc does not contract it into
+// FMAs; that keeps the FP64 path on the reference's own arithmetic
+// (src/anukulan/backend.cpp:60-111 runs without contraction on x86-64).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace anu {
+
+constexpr int kThreads = 256;
+constexpr int kBlockNnz = 2048;
+constexpr int kBlockRows = 256;
+
+// ------------------------------------------------------------------ math
+
+__device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float mul(float a, float b) { return a * b; }
+__device__ __forceinline__ float add(float a, float b) { return a + b; }
+__device__ __forceinline__ float sub(float a, float b) { return a - b; }
+// acc + a*b: contracted to an FMA in FP32, two rounded operations in FP64.
+__device__ __forceinline__ double madd(double acc, double a, double b) { return add(acc, mul(a, b)); }
+__device__ __forceinline__ float madd(float acc, float a, float b) { return fmaf(a, b, acc); }
+
+template <class T> __device__ __forceinline__ T load(const T* p) { return __ldg(p); }
+
+// -------------------------------------------------------------- matrices
+
+struct RowBlockDev {
+  int32_t row_begin;
+  int32_t row_end;
+};
+
+template <class V>
+struct CsrView {
+  int32_t rows;
+  int32_t cols;
+  const int32_t* __restrict__ start;
+  const int32_t* __restrict__ index;
+  const V* __restrict__ value;
+  const RowBlockDev* __restrict__ blocks;
+  int32_t num_blocks;
+};
+
+// ------------------------------------------------------- per-case state
+
+// What one case's step needs, read by every thread of the iteration kernels.
+// Written by the host before each iteration chunk.
+struct StepParams {
+  double tau;
+  double sigma;
+  double gamma;        // reflection, 0 when off
+  double eta;          // step size, for the averaged scheme's running sums
+  int32_t active;      // 0: retired, its lanes do nothing
+  int32_t halpern;     // Halpern blending on for this case
+  int32_t reset_pending;  // the chunk's first step starts a new epoch
+  int32_t pad;
+};
+
+enum : uint32_t {
+  kWriteDelta = 1u,   // write dx / dy (and k_dx)
+  kAccumulate = 2u,   // running sums of the averaged scheme
+};
+
+// ------------------------------------------------------------ epilogues
+
+// out[row*K + case] = sum
+template <class Out>
+struct StoreEpi {
+  int32_t K;
+  Out* __restrict__ out;
+  template <class Acc>
+  __device__ __forceinline__ void operator()(int32_t r, int32_t k, Acc s) const {
+    out[(size_t)r * K + k] = static_cast<Out>(s);
+  }
+};
+
+// Two products over one matrix read: out1 = A x1 and out2 = A x2 handled by
+// running the kernel twice is simpler; kept single for clarity.
+
+// The primal side of one reflected Halpern PDHG step on column j of case k,
+// given kty = (K'y)_j (backend.hpp:89-93, backend.cpp:60-79):
+//   v = clamp(x - tau (c - kty), lower, upper); dx = v - x; x_bar = v + dx;
+//   next = v + gamma dx; next = w next + (1-w) anchor  (when blending)
+template <class T>
+struct PrimalEpi {
+  int32_t K;
+  int32_t it;
+  uint32_t flags;
+  const StepParams* __restrict__ p;
+  const double* __restrict__ w_table;  // Halpern weight per (it, case)
+  const T* x_in;
+  T* x_out;
+  const T* __restrict__ c;
+  const T* __restrict__ lo;
+  const T* __restrict__ hi;
+  T* __restrict__ x_bar;
+  T* anchor;
+  T* __restrict__ dx;
+  T* __restrict__ sum_x;
+
+  __device__ __forceinline__ void operator()(int32_t j, int32_t k, T kty) const {
+    const StepParams& P = p[k];
+    if (!P.active) return;
+    const size_t e = (size_t)j * K + k;
+    const T xj = x_in[e];
+    T v = sub(xj, mul(static_cast<T>(P.tau), sub(c[e], kty)));
+    const T l = lo[e];
+    const T u = hi[e];
+    if (v < l) v = l;
+    if (v > u) v = u;
+    const T d = sub(v, xj);
+    if (flags & kWriteDelta) dx[e] = d;
+    x_bar[e] = add(v, d);
+    T next = v;
+    if (P.gamma != 0.0) next = add(next, mul(static_cast<T>(P.gamma), d));
+    const bool reset_now = P.reset_pending && it == 0;
+    if (P.halpern && !reset_now) {
+      const double w = w_table[(size_t)it * K + k];
+      next = add(mul(static_cast<T>(w), next), mul(static_cast<T>(1.0 - w), anchor[e]));
+    }
+    x_out[e] = next;
+    if (P.halpern && reset_now) anchor[e] = next;
+    if (flags & kAccumulate) sum_x[e] = add(sum_x[e], mul(static_cast<T>(P.eta), next));
+  }
+};
+
+// The dual side on row i of case k, given bar = (K x_bar)_i
+// (backend.hpp:114-119, backend.cpp:81-111):
+//   v = y + sigma (q - bar), projected to v >= ylo on inequality rows
+//   dy = v - y; k_dx = (bar - kx)/2; next_y = v + gamma dy;
+//   next_k = (bar + kx)/2 + gamma k_dx; both blended with their anchors.
+// ylo is zero except in a refinement correction solve.
+template <class T>
+struct DualEpi {
+  int32_t K;
+  int32_t it;
+  uint32_t flags;
+  int32_t num_eq;
+  const StepParams* __restrict__ p;
+  const double* __restrict__ w_table;
+  const T* y_in;
+  T* y_out;
+  const T* __restrict__ q;
+  const T* kx_in;
+  T* kx_out;
+  T* anchor_y;
+  T* anchor_kx;
+  T* __restrict__ dy;
+  T* __restrict__ k_dx;
+  T* __restrict__ sum_y;
+  const T* __restrict__ ylo;  // may be null (zero)
+
+  __device__ __forceinline__ void operator()(int32_t i, int32_t k, T bar) const {
+    const StepParams& P = p[k];
+    if (!P.active) return;
+    const size_t e = (size_t)i * K + k;
+    const T yi = y_in[e];
+    const T kx = kx_in[e];
+    T v = add(yi, mul(static_cast<T>(P.sigma), sub(q[e], bar)));
+    if (i >= num_eq) {
+      const T floor_v = ylo ? ylo[e] : static_cast<T>(0);
+      if (v < floor_v) v = floor_v;
+    }
+    const T d = sub(v, yi);
+    const T kd = mul(static_cast<T>(0.5), sub(bar, kx));
+    if (flags & kWriteDelta) {
+      dy[e] = d;
+      if (k_dx) k_dx[e] = kd;
+    }
+    T next_y = v;
+    T next_k = mul(static_cast<T>(0.5), add(bar, kx));
+    if (P.gamma != 0.0) {
+      next_y = add(next_y, mul(static_cast<T>(P.gamma), d));
+      next_k = add(next_k, mul(static_cast<T>(P.gamma), kd));
+    }
+    const bool reset_now = P.reset_pending && it == 0;
+    if (P.halpern && !reset_now) {
+      const double w = w_table[(size_t)it * K + k];
+      const T wt = static_cast<T>(w);
+      const T wc = static_cast<T>(1.0 - w);
+      next_y = add(mul(wt, next_y), mul(wc, anchor_y[e]));
+      next_k = add(mul(wt, next_k), mul(wc, anchor_kx[e]));
+    }
+    y_out[e] = next_y;
+    kx_out[e] = next_k;
+    if (P.halpern && reset_now) {
+      anchor_y[e] = next_y;
+      anchor_kx[e] = next_k;
+    }
+    if (flags & kAccumulate) sum_y[e] = add(sum_y[e], mul(static_cast<T>(P.eta), next_y));
+  }
+};
+
+// ------------------------------------------------------- block reductions
+
+template <class Acc>
+__device__ __forceinline__ Acc block_sum(Acc v, Acc* scratch) {
+  // Deterministic tree over the CTA.
+  scratch[threadIdx.x] = v;
+  __syncthreads();
+  for (int s = kThreads / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) scratch[threadIdx.x] = add(scratch[threadIdx.x], scratch[threadIdx.x + s]);
+    __syncthreads();
+  }
+  const Acc r = scratch[0];
+  __syncthreads();
+  return r;
+}
+
+// ----------------------------------------------------------- rows_kernel
+
+template <class V, class X, class Acc, class Epi>
+__global__ void __launch_bounds__(kThreads) rows_kernel(CsrView<V> a, const X* __restrict__ x,
+                                                         Epi epi) {
+  __shared__ Acc prod[kBlockNnz];
+  __shared__ Acc rowsum[kBlockRows];
+  const RowBlockDev blk = a.blocks[blockIdx.x];
+  const int32_t r0 = blk.row_begin;
+  const int32_t nrows = blk.row_end - r0;
+  const int32_t nz0 = a.start[r0];
+  const int32_t nnz = a.start[blk.row_end] - nz0;
+  if (nnz > kBlockNnz) {
+    // One long row: strided partial sums, then a fixed-order tree.
+    Acc s = 0;
+    for (int32_t k = nz0 + threadIdx.x; k < nz0 + nnz; k += kThreads)
+      s = madd(s, static_cast<Acc>(a.value[k]), static_cast<Acc>(x[a.index[k]]));
+    s = block_sum(s, prod);
+    if (threadIdx.x == 0) epi(r0, 0, s);
+    return;
+  }
+  for (int32_t k = threadIdx.x; k < nnz; k += kThreads)
+    prod[k] = mul(static_cast<Acc>(a.value[nz0 + k]), static_cast<Acc>(x[a.index[nz0 + k]]));
+  __syncthreads();
+  // Lanes per row: one while rows average at most 32 nonzeros (a serial sum
+  // over shared memory, the reference's own order), else a shuffle group.
+  int g = 1;
+  if (nrows > 0 && nnz > 32 * nrows) {
+    g = 32;
+    while (g > 1 && g * nrows > kThreads) g >>= 1;
+  }
+  const int32_t row = threadIdx.x / g;
+  const int lane = threadIdx.x % g;
+  Acc s = 0;
+  if (row < nrows) {
+    const int32_t b = a.start[r0 + row] - nz0;
+    const int32_t e = a.start[r0 + row + 1] - nz0;
+    for (int32_t k = b + lane; k < e; k += g) s = add(s, prod[k]);
+  }
+  for (int off = g >> 1; off > 0; off >>= 1) s = add(s, __shfl_down_sync(0xffffffffu, s, off));
+  if (lane == 0 && row < nrows) rowsum[row] = s;
+  __syncthreads();
+  for (int32_t t = threadIdx.x; t < nrows; t += kThreads) epi(r0 + t, 0, rowsum[t]);
+}
+
+// ---------------------------------------------------------- cases_kernel
+
+// L lanes per row group (power of two, <= 32); CPL cases per lane.
+template <class V, class X, class Acc, class Epi, int L, int CPL>
+__global__ void __launch_bounds__(kThreads) cases_kernel(CsrView<V> a, const X* __restrict__ x,
+                                                          int32_t K, Epi epi) {
+  constexpr int kGroups = kThreads / L;
+  const int group = threadIdx.x / L;
+  const int lane = threadIdx.x % L;
+  for (int32_t row = blockIdx.x * kGroups + group; row < a.rows; row += gridDim.x * kGroups) {
+    Acc acc[CPL];
+#pragma unroll
+    for (int c = 0; c < CPL; ++c) acc[c] = 0;
+    const int32_t b = a.start[row];
+    const int32_t e = a.start[row + 1];
+    for (int32_t k = b; k < e; ++k) {
+      const int32_t col = a.index[k];
+      const Acc v = static_cast<Acc>(a.value[k]);
+      const X* xc = x + (size_t)col * K;
+#pragma unroll
+      for (int c = 0; c < CPL; ++c) {
+        const int32_t cs = lane + c * L;
+        if (cs < K) acc[c] = madd(acc[c], v, static_cast<Acc>(xc[cs]));
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < CPL; ++c) {
+      const int32_t cs = lane + c * L;
+      if (cs < K) epi(row, cs, acc[c]);
+    }
+  }
+}
+
+// ------------------------------------------------------- term reductions
+
+// Stage 1 of a per-case reduction over `len` rows (or columns): groups of L
+// lanes walk rows, lane l owns cases l, l+L, ...; each thread keeps NT
+// accumulators per owned case; the CTA combines its groups in a fixed tree
+// and writes partial[block][case][term].
+template <class Terms, int L, int CPL>
+__global__ void __launch_bounds__(kThreads) terms_stage1(int32_t len, int32_t K, Terms t,
+                                                          double* __restrict__ partial) {
+  constexpr int NT = Terms::NT;
+  constexpr int kGroups = kThreads / L;
+  constexpr int kSlots = L * CPL;
+  __shared__ double red[kGroups][kSlots][NT];
+  const int group = threadIdx.x / L;
+  const int lane = threadIdx.x % L;
+  double acc[CPL][NT];
+#pragma unroll
+  for (int c = 0; c < CPL; ++c) Terms::init(acc[c]);
+  for (int32_t r = blockIdx.x * kGroups + group; r < len; r += gridDim.x * kGroups) {
+#pragma unroll
+    for (int c = 0; c < CPL; ++c) {
+      const int32_t cs = lane + c * L;
+      if (cs < K) t.add(acc[c], r, cs);
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < CPL; ++c)
+#pragma unroll
+    for (int q = 0; q < NT; ++q) red[group][lane + c * L][q] = acc[c][q];
+  __syncthreads();
+  for (int s = kGroups / 2; s > 0; s >>= 1) {
+    for (int idx = threadIdx.x; idx < s * kSlots * NT; idx += kThreads) {
+      const int g = idx / (kSlots * NT);
+      const int rem = idx % (kSlots * NT);
+      const int slot = rem / NT;
+      const int q = rem % NT;
+      red[g][slot][q] = Terms::combine(q, red[g][slot][q], red[g + s][slot][q]);
+    }
+    __syncthreads();
+  }
+  for (int idx = threadIdx.x; idx < kSlots * NT; idx += kThreads) {
+    const int slot = idx / NT;
+    const int q = idx % NT;
+    // slot = lane + c*L -> case index is the slot itself.
+    if (slot < K) partial[((size_t)blockIdx.x * K + slot) * NT + q] = red[0][slot][q];
+  }
+}
+
+// Stage 2: out[case*stride + offset + term] = fixed-order combination of the
+// blocks' partials.
+template <class Terms>
+__global__ void terms_stage2(int32_t blocks, int32_t K, const double* __restrict__ partial,
+                             double* __restrict__ out, int32_t stride, int32_t offset) {
+  constexpr int NT = Terms::NT;
+  const int32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= K * NT) return;
+  const int32_t k = idx / NT;
+  const int q = idx % NT;
+  double acc = Terms::identity(q);
+  for (int32_t b = 0; b < blocks; ++b) acc = Terms::combine(q, acc, partial[((size_t)b * K + k) * NT + q]);
+  out[(size_t)k * stride + offset + q] = acc;
+}
+
+// ------------------------------------------------------------ check terms
+
+// Row side of a termination check, per case (backend.cpp:143-161 and the
+// row half of pdhg.cpp:191-221), plus the squared norms the step-size rule,
+// the restart test and the primal-weight update read.
+// Terms: 0 primal_sq, 1 primal_inf (max), 2 q_dot_y, 3 dy_sq, 4 dyr_sq
+// (|y - y_restart|^2), 5 dypr_sq (|y - y_prev_restart|^2), 6 inf_scale (max
+// |dy|), 7 inf_badcone (max of indicator), 8 inf_rhs (sum q~ dy).
+template <class T, class KX>
+struct RowCheckTerms {
+  static constexpr int NT = 9;
+  int32_t K;
+  int32_t num_eq;
+  const KX* __restrict__ kx;       // K~ x~ (scaled)
+  const T* __restrict__ y;
+  const T* __restrict__ dy;
+  const T* __restrict__ y_restart;
+  const T* __restrict__ y_prev;
+  const double* __restrict__ q;        // original, per case
+  const double* __restrict__ q_scaled; // for the Farkas test
+  const double* __restrict__ row_scale;  // shared, may be null (unit)
+  __device__ static void init(double* a) {
+#pragma unroll
+    for (int i = 0; i < NT; ++i) a[i] = 0.0;
+  }
+  __device__ static double identity(int) { return 0.0; }
+  __device__ static double combine(int q, double a, double b) {
+    return (q == 1 || q == 6 || q == 7) ? fmax(a, b) : anu::add(a, b);
+  }
+  __device__ void add(double* a, int32_t i, int32_t k) const {
+    const size_t e = (size_t)i * K + k;
+    const double scale = row_scale ? row_scale[i] : 1.0;
+    const double kxv = static_cast<double>(kx[e]);
+    const double row = scale != 0.0 ? kxv / scale : kxv;
+    const double qi = q[e];
+    const double slack = anu::sub(row, qi);
+    const double viol = (i < num_eq) ? slack : fmin(slack, 0.0);
+    a[0] = anu::add(a[0], mul(viol, viol));
+    a[1] = fmax(a[1], fabs(viol));
+    const double yi = static_cast<double>(y[e]);
+    a[2] = anu::add(a[2], mul(qi, mul(scale, yi)));
+    const double d = dy ? static_cast<double>(dy[e]) : 0.0;
+    a[3] = anu::add(a[3], mul(d, d));
+    if (y_restart) {
+      const double r = anu::sub(yi, static_cast<double>(y_restart[e]));
+      a[4] = anu::add(a[4], mul(r, r));
+    }
+    if (y_prev) {
+      const double r = anu::sub(yi, static_cast<double>(y_prev[e]));
+      a[5] = anu::add(a[5], mul(r, r));
+    }
+    a[6] = fmax(a[6], fabs(d));
+    if (i >= num_eq && d < 0.0) a[7] = 1.0;
+    if (q_scaled) a[8] = anu::add(a[8], mul(q_scaled[e], d));
+  }
+};
+
+// Column side (backend.cpp:163-198 and the column half of the Farkas test).
+// Terms: 0 dual_sq, 1 dual_inf (max), 2 bound_term, 3 c_dot_x, 4 dx_sq,
+// 5 dxr_sq, 6 dxpr_sq, 7 inf_support, 8 inf_unbounded (max of indicator).
+template <class T>
+struct ColCheckTerms {
+  static constexpr int NT = 9;
+  int32_t K;
+  const double* __restrict__ kty;   // K~' y~ (scaled)
+  const T* __restrict__ x;
+  const T* __restrict__ dx;
+  const T* __restrict__ x_restart;
+  const T* __restrict__ x_prev;
+  const double* __restrict__ c;      // original, per case
+  const double* __restrict__ lower;  // original
+  const double* __restrict__ upper;  // original
+  const double* __restrict__ col_scale;  // may be null
+  const double* __restrict__ kt_dy;      // K~' dy, may be null
+  const double* __restrict__ lower_scaled;
+  const double* __restrict__ upper_scaled;
+  __device__ static void init(double* a) {
+#pragma unroll
+    for (int i = 0; i < NT; ++i) a[i] = 0.0;
+  }
+  __device__ static double identity(int) { return 0.0; }
+  __device__ static double combine(int q, double a, double b) {
+    return (q == 1 || q == 8) ? fmax(a, b) : anu::add(a, b);
+  }
+  __device__ void add(double* a, int32_t j, int32_t k) const {
+    const size_t e = (size_t)j * K + k;
+    const double scale = col_scale ? col_scale[j] : 1.0;
+    const double p = kty[e];
+    const double product = scale != 0.0 ? p / scale : p;
+    const double cj = c[e];
+    const double lambda = anu::sub(cj, product);
+    const double lo = lower[e];
+    const double hi = upper[e];
+    const bool has_lo = lo > -INFINITY;
+    const bool has_hi = hi < INFINITY;
+    double leftover = 0.0;
+    if (has_lo && has_hi) leftover = 0.0;
+    else if (has_lo) leftover = fmin(lambda, 0.0);
+    else if (has_hi) leftover = fmax(lambda, 0.0);
+    else leftover = lambda;
+    a[0] = anu::add(a[0], mul(leftover, leftover));
+    a[1] = fmax(a[1], fabs(leftover));
+    const double absorbed = anu::sub(lambda, leftover);
+    if (absorbed > 0.0) a[2] = anu::add(a[2], mul(absorbed, lo));
+    else if (absorbed < 0.0) a[2] = anu::add(a[2], mul(absorbed, hi));
+    const double xj = static_cast<double>(x[e]);
+    a[3] = anu::add(a[3], mul(cj, mul(scale, xj)));
+    const double d = dx ? static_cast<double>(dx[e]) : 0.0;
+    a[4] = anu::add(a[4], mul(d, d));
+    if (x_restart) {
+      const double r = anu::sub(xj, static_cast<double>(x_restart[e]));
+      a[5] = anu::add(a[5], mul(r, r));
+    }
+    if (x_prev) {
+      const double r = anu::sub(xj, static_cast<double>(x_prev[e]));
+      a[6] = anu::add(a[6], mul(r, r));
+    }
+    if (kt_dy) {
+      const double lam = kt_dy[e];
+      if (lam > 0.0) {
+        const double u = upper_scaled[e];
+        if (u >= INFINITY) a[8] = 1.0;
+        else a[7] = anu::add(a[7], mul(lam, u));
+      } else if (lam < 0.0) {
+        const double l = lower_scaled[e];
+        if (l <= -INFINITY) a[8] = 1.0;
+        else a[7] = anu::add(a[7], mul(lam, l));
+      }
+    }
+  }
+};
+
+// Weighted KKT error terms on the scaled problem (pdhg.cpp:295-340):
+// row side 0 primal_sq, 1 q_dot_y; column side 0 dual_sq, 1 bound_term,
+// 2 c_dot_x.
+template <class T>
+struct RowKktTerms {
+  static constexpr int NT = 2;
+  int32_t K;
+  int32_t num_eq;
+  const double* __restrict__ kx;
+  const T* __restrict__ y;
+  const double* __restrict__ q;
+  __device__ static void init(double* a) { a[0] = a[1] = 0.0; }
+  __device__ static double identity(int) { return 0.0; }
+  __device__ static double combine(int, double a, double b) { return anu::add(a, b); }
+  __device__ void add(double* a, int32_t i, int32_t k) const {
+    const size_t e = (size_t)i * K + k;
+    const double s = anu::sub(kx[e], q[e]);
+    const double v = (i < num_eq) ? s : fmin(s, 0.0);
+    a[0] = anu::add(a[0], mul(v, v));
+    a[1] = anu::add(a[1], mul(q[e], static_cast<double>(y[e])));
+  }
+};
+
+template <class T>
+struct ColKktTerms {
+  static constexpr int NT = 3;
+  int32_t K;
+  const double* __restrict__ kty;
+  const T* __restrict__ x;
+  const double* __restrict__ c;
+  const double* __restrict__ lower;
+  const double* __restrict__ upper;
+  __device__ static void init(double* a) { a[0] = a[1] = a[2] = 0.0; }
+  __device__ static double identity(int) { return 0.0; }
+  __device__ static double combine(int, double a, double b) { return anu::add(a, b); }
+  __device__ void add(double* a, int32_t j, int32_t k) const {
+    const size_t e = (size_t)j * K + k;
+    const double lambda = anu::sub(c[e], kty[e]);
+    const double lo = lower[e], hi = upper[e];
+    const bool has_lo = lo > -INFINITY, has_hi = hi < INFINITY;
+    double leftover = 0.0;
+    if (has_lo && has_hi) leftover = 0.0;
+    else if (has_lo) leftover = fmin(lambda, 0.0);
+    else if (has_hi) leftover = fmax(lambda, 0.0);
+    else leftover = lambda;
+    a[0] = anu::add(a[0], mul(leftover, leftover));
+    const double absorbed = anu::sub(lambda, leftover);
+    if (absorbed > 0.0) a[1] = anu::add(a[1], mul(absorbed, lo));
+    else if (absorbed < 0.0) a[1] = anu::add(a[1], mul(absorbed, hi));
+    a[2] = anu::add(a[2], mul(c[e], static_cast<double>(x[e])));
+  }
+};
+
+// ------------------------------------------------------------ elementwise
+
+// dst[e] = src[e] for the elements of cases whose mask is set (mask null:
+// all). len is rows or columns; the arrays hold len*K elements.
+template <class D, class S>
+__global__ void masked_copy_kernel(int64_t total, int32_t K, const int32_t* __restrict__ mask,
+                                   const S* __restrict__ src, D* __restrict__ dst) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    if (mask == nullptr || mask[e % K]) dst[e] = static_cast<D>(src[e]);
+  }
+}
+
+template <class D>
+__global__ void masked_fill_kernel(int64_t total, int32_t K, const int32_t* __restrict__ mask,
+                                   D value, D* __restrict__ dst) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    if (mask == nullptr || mask[e % K]) dst[e] = value;
+  }
+}
+
+// out = sum / weight per case (the averaged iterate), weights per case.
+template <class T>
+__global__ void average_kernel(int64_t total, int32_t K, const double* __restrict__ weight,
+                               const T* __restrict__ sum, T* __restrict__ out) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const double w = weight[e % K];
+    out[e] = static_cast<T>(static_cast<double>(sum[e]) / w);
+  }
+}
+
+}  // namespace anu

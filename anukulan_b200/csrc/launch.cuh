@@ -1,0 +1,103 @@
+// Launch helpers shared by the solver and the backend seam: the sparse
+// product in its single-case and case-stack shapes, the two-stage per-case
+// reductions, and masked per-case copies.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "kernels.cuh"
+
+namespace anu {
+
+void cuda_check(cudaError_t status, const char* what);
+
+// A stream and a count of the kernels launched on it.
+struct Exec {
+  cudaStream_t stream = nullptr;
+  int64_t launches = 0;
+};
+
+
+inline int grid_for(int64_t items, int per_block, int cap) {
+  int64_t g = (items + per_block - 1) / per_block;
+  if (g < 1) g = 1;
+  if (g > cap) g = cap;
+  return static_cast<int>(g);
+}
+
+
+// y = A x (any epilogue) for K cases.
+template <class V, class X, class Acc, class Epi, class Mat>
+void product(Exec& p, const Mat& a, const X* x, int K, const Epi& epi) {
+  if (a.rows == 0) return;
+  cudaStream_t s = p.stream;
+  if (K == 1) {
+    rows_kernel<V, X, Acc, Epi><<<a.num_blocks, kThreads, 0, s>>>(a.template view<V>(), x, epi);
+  } else {
+#define ANU_CASES(L_, CPL_)                                                                  \
+  cases_kernel<V, X, Acc, Epi, L_, CPL_>                                                     \
+      <<<grid_for(a.rows, kThreads / L_, 148 * 16), kThreads, 0, s>>>(a.template view<V>(), x, K, epi)
+    if (K <= 4) ANU_CASES(4, 1);
+    else if (K <= 8) ANU_CASES(8, 1);
+    else if (K <= 16) ANU_CASES(16, 1);
+    else if (K <= 32) ANU_CASES(32, 1);
+    else ANU_CASES(32, 2);
+#undef ANU_CASES
+  }
+  cuda_check(cudaGetLastError(), "kernel launch");
+  ++p.launches;
+}
+
+// Two-stage per-case reduction of `t` over len rows; results land in
+// out[case*stride + offset + term] (device).
+template <class Terms, class Buf>
+void reduce_terms(Exec& p, int32_t len, int K, const Terms& t, Buf& partial,
+                  double* out, int stride, int offset) {
+  constexpr int NT = Terms::NT;
+  cudaStream_t s = p.stream;
+  int blocks = 0;
+#define ANU_TERMS(L_, CPL_)                                                           \
+  do {                                                                                \
+    blocks = grid_for(len, kThreads / L_, 296);                                       \
+    if (partial.n < static_cast<size_t>(blocks) * K * NT)                             \
+      partial.alloc(static_cast<size_t>(blocks) * K * NT);                            \
+    terms_stage1<Terms, L_, CPL_><<<blocks, kThreads, 0, s>>>(len, K, t, partial.p);  \
+  } while (0)
+  if (K == 1) ANU_TERMS(1, 1);
+  else if (K <= 4) ANU_TERMS(4, 1);
+  else if (K <= 8) ANU_TERMS(8, 1);
+  else if (K <= 16) ANU_TERMS(16, 1);
+  else if (K <= 32) ANU_TERMS(32, 1);
+  else ANU_TERMS(32, 2);
+#undef ANU_TERMS
+  cuda_check(cudaGetLastError(), "kernel launch");
+  terms_stage2<Terms><<<(K * NT + 127) / 128, 128, 0, s>>>(blocks, K, partial.p, out, stride,
+                                                            offset);
+  cuda_check(cudaGetLastError(), "kernel launch");
+  p.launches += 2;
+}
+
+template <class D, class S>
+void masked_copy(Exec& p, int64_t len, int K, const int32_t* mask, const S* src, D* dst) {
+  const int64_t total = len * K;
+  if (total == 0) return;
+  masked_copy_kernel<D, S><<<grid_for(total, 256, 148 * 8), 256, 0, p.stream>>>(total, K, mask,
+                                                                              src, dst);
+  cuda_check(cudaGetLastError(), "kernel launch");
+  ++p.launches;
+}
+
+template <class D>
+void masked_fill(Exec& p, int64_t len, int K, const int32_t* mask, D value, D* dst) {
+  const int64_t total = len * K;
+  if (total == 0) return;
+  masked_fill_kernel<D><<<grid_for(total, 256, 148 * 8), 256, 0, p.stream>>>(total, K, mask,
+                                                                           value, dst);
+  cuda_check(cudaGetLastError(), "kernel launch");
+  ++p.launches;
+}
+
+
+}  // namespace anu

@@ -1,0 +1,253 @@
+"""Host-side mirror of the reference's PDHG interface over the CUDA engine.
+
+``solve_pdhg(lp, options)`` is ``anukulan::solve_pdhg``
+(src/anukulan/pdhg.hpp:543): same options (``PdhgOptions`` field names, see
+:func:`anukulan_b200.abi.make_options`), same result fields, same status
+values. Every call goes through ``libanu_pdhg.so``; there is no CPU path, and
+a missing library or device raises instead of falling back.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional, Sequence
+
+import numpy as np
+
+from .abi import (CLp, PdhgResult, Residual, anu_csr, anu_lp, anu_pdhg_options,
+                  anu_pdhg_residual, anu_pdhg_result, f64_ptr, make_options)
+from .model import StandardLp
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libanu_pdhg.so")
+
+_P = C.POINTER
+_lib = None
+
+# Every function the C ABI declares (include/anu_pdhg.h).
+EXPORTS = (
+    "anu_pdhg_version", "anu_pdhg_default_options", "anu_last_error", "anu_device_count",
+    "anu_pdhg_solve", "anu_pdhg_create", "anu_pdhg_run", "anu_pdhg_destroy",
+    "anu_evaluate_residual", "anu_estimate_matrix_norm",
+    "anu_backend_allocate", "anu_backend_deallocate", "anu_backend_upload",
+    "anu_backend_download", "anu_backend_fill", "anu_backend_copy", "anu_backend_prepare",
+    "anu_backend_release", "anu_backend_multiply", "anu_backend_dot", "anu_backend_two_norm",
+    "anu_backend_inf_norm", "anu_backend_primal_update", "anu_backend_dual_update",
+    "anu_backend_accumulate", "anu_backend_scale_into", "anu_backend_weighted_norm_squared",
+    "anu_backend_step_size_terms", "anu_backend_convergence_terms",
+    "anu_pdhg_batch_create", "anu_pdhg_batch_solve", "anu_pdhg_batch_destroy",
+)
+
+
+class EngineError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"anu_pdhg error {code}: {message}")
+        self.code = code
+
+
+def lib():
+    """Loads libanu_pdhg.so (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise FileNotFoundError(
+            f"{LIB_PATH} is missing: build it with `python -m anukulan_b200.build`")
+    L = C.CDLL(LIB_PATH)
+
+    def d(name, res, args):
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+
+    d("anu_pdhg_version", C.c_char_p, [])
+    d("anu_pdhg_default_options", None, [_P(anu_pdhg_options)])
+    d("anu_last_error", C.c_int, [C.c_char_p, C.c_int32])
+    d("anu_device_count", C.c_int32, [])
+    d("anu_pdhg_solve", C.c_int, [_P(anu_lp), _P(anu_pdhg_options), _P(C.c_double),
+                                  _P(C.c_double), _P(C.c_double), _P(C.c_double),
+                                  _P(anu_pdhg_result)])
+    d("anu_pdhg_create", C.c_int, [_P(anu_lp), _P(anu_pdhg_options), _P(C.c_void_p)])
+    d("anu_pdhg_run", C.c_int, [C.c_void_p, _P(C.c_double), _P(C.c_double), _P(C.c_double),
+                                _P(C.c_double), _P(anu_pdhg_result)])
+    d("anu_pdhg_destroy", None, [C.c_void_p])
+    d("anu_evaluate_residual", C.c_int, [_P(anu_lp), _P(C.c_double), _P(C.c_double),
+                                         _P(anu_pdhg_residual)])
+    d("anu_estimate_matrix_norm", C.c_int, [_P(anu_lp), C.c_int32, C.c_double,
+                                            _P(C.c_double)])
+    d("anu_pdhg_batch_create", C.c_int, [_P(anu_lp), C.c_int32, _P(C.c_double),
+                                         _P(C.c_double), _P(C.c_double), _P(C.c_double),
+                                         _P(anu_pdhg_options), _P(C.c_void_p)])
+    d("anu_pdhg_batch_solve", C.c_int, [C.c_void_p, _P(C.c_double), _P(C.c_double),
+                                        _P(anu_pdhg_result)])
+    d("anu_pdhg_batch_destroy", None, [C.c_void_p])
+    vp = C.c_void_p
+    i64 = C.c_int64
+    dbl = C.c_double
+    d("anu_backend_allocate", C.c_int, [i64, _P(vp)])
+    d("anu_backend_deallocate", C.c_int, [vp])
+    d("anu_backend_upload", C.c_int, [_P(dbl), vp, i64])
+    d("anu_backend_download", C.c_int, [vp, _P(dbl), i64])
+    d("anu_backend_fill", C.c_int, [vp, i64, dbl])
+    d("anu_backend_copy", C.c_int, [vp, vp, i64])
+    d("anu_backend_prepare", C.c_int, [C.c_uint64, _P(anu_csr)])
+    d("anu_backend_release", C.c_int, [])
+    d("anu_backend_multiply", C.c_int, [C.c_uint64, vp, vp])
+    d("anu_backend_dot", C.c_int, [vp, vp, i64, _P(dbl)])
+    d("anu_backend_two_norm", C.c_int, [vp, i64, _P(dbl)])
+    d("anu_backend_inf_norm", C.c_int, [vp, i64, _P(dbl)])
+    d("anu_backend_primal_update", C.c_int, [i64, dbl, dbl, dbl] + [vp] * 9)
+    d("anu_backend_dual_update", C.c_int, [i64, i64, dbl, dbl, dbl] + [vp] * 10)
+    d("anu_backend_accumulate", C.c_int, [i64, dbl, vp, vp])
+    d("anu_backend_scale_into", C.c_int, [i64, dbl, vp, vp])
+    d("anu_backend_weighted_norm_squared", C.c_int, [i64, i64, vp, vp, dbl, _P(dbl)])
+    d("anu_backend_step_size_terms", C.c_int, [i64, i64, vp, vp, vp, dbl, _P(dbl), _P(dbl)])
+    d("anu_backend_convergence_terms", C.c_int, [i64, i64] + [vp] * 6 + [i64] + [vp] * 4
+      + [_P(dbl)])
+    _lib = L
+    return L
+
+
+def check(rc: int) -> None:
+    if rc != 0:
+        buf = C.create_string_buffer(512)
+        lib().anu_last_error(buf, 512)
+        raise EngineError(rc, buf.value.decode(errors="replace"))
+
+
+def version() -> str:
+    return lib().anu_pdhg_version().decode()
+
+
+def device_count() -> int:
+    return int(lib().anu_device_count())
+
+
+def default_options() -> anu_pdhg_options:
+    o = anu_pdhg_options()
+    lib().anu_pdhg_default_options(C.byref(o))
+    return o
+
+
+def _options(options: Optional[anu_pdhg_options], kw) -> anu_pdhg_options:
+    if options is None:
+        return make_options(**kw)
+    if kw:
+        o = anu_pdhg_options()
+        C.memmove(C.byref(o), C.byref(options), C.sizeof(o))
+        for k, v in kw.items():
+            setattr(o, k, int(v) if isinstance(v, bool) else v)
+        return o
+    return options
+
+
+def solve_pdhg(lp: StandardLp, options: Optional[anu_pdhg_options] = None,
+               warm_x=None, warm_y=None, **kw) -> PdhgResult:
+    """``solve_pdhg`` on the B200 engine (pdhg.hpp:543)."""
+    cl = CLp(lp)
+    o = _options(options, kw)
+    x = np.zeros(cl.n)
+    y = np.zeros(cl.m)
+    r = anu_pdhg_result()
+    wx = None if warm_x is None else np.ascontiguousarray(warm_x, np.float64)
+    wy = None if warm_y is None else np.ascontiguousarray(warm_y, np.float64)
+    check(lib().anu_pdhg_solve(cl.ref(), C.byref(o), f64_ptr(wx), f64_ptr(wy), f64_ptr(x),
+                               f64_ptr(y), C.byref(r)))
+    return PdhgResult.from_c(r, x, y)
+
+
+class PdhgHandle:
+    """A prepared LP (scaled, uploaded, ||K|| measured) that can be solved
+    repeatedly: ``anu_pdhg_create`` / ``anu_pdhg_run``."""
+
+    def __init__(self, lp: StandardLp, options: Optional[anu_pdhg_options] = None, **kw):
+        self._cl = CLp(lp)
+        self.options = _options(options, kw)
+        self._h = C.c_void_p()
+        check(lib().anu_pdhg_create(self._cl.ref(), C.byref(self.options), C.byref(self._h)))
+
+    def run(self, warm_x=None, warm_y=None, x=None, y=None) -> PdhgResult:
+        x = np.zeros(self._cl.n) if x is None else x
+        y = np.zeros(self._cl.m) if y is None else y
+        r = anu_pdhg_result()
+        wx = None if warm_x is None else np.ascontiguousarray(warm_x, np.float64)
+        wy = None if warm_y is None else np.ascontiguousarray(warm_y, np.float64)
+        check(lib().anu_pdhg_run(self._h, f64_ptr(wx), f64_ptr(wy), f64_ptr(x), f64_ptr(y),
+                                 C.byref(r)))
+        return PdhgResult.from_c(r, x, y)
+
+    def close(self):
+        if self._h:
+            lib().anu_pdhg_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def evaluate_residual(lp: StandardLp, x, y) -> Residual:
+    """``evaluate_residual`` (pdhg.hpp:548) computed on the device."""
+    cl = CLp(lp)
+    out = anu_pdhg_residual()
+    check(lib().anu_evaluate_residual(cl.ref(), f64_ptr(np.ascontiguousarray(x, np.float64)),
+                                      f64_ptr(np.ascontiguousarray(y, np.float64)),
+                                      C.byref(out)))
+    return Residual.from_c(out)
+
+
+def estimate_matrix_norm(lp: StandardLp, iterations: int = 200, tolerance: float = 1e-8) -> float:
+    """``estimate_matrix_norm`` (pdhg.hpp:580) on the device."""
+    out = C.c_double(0.0)
+    check(lib().anu_estimate_matrix_norm(CLp(lp).ref(), iterations, tolerance, C.byref(out)))
+    return out.value
+
+
+class CaseStackSolver:
+    """A case stack sharing one matrix (``anu_pdhg_batch_*``)."""
+
+    def __init__(self, base: StandardLp, c=None, q=None, lower=None, upper=None,
+                 options: Optional[anu_pdhg_options] = None, **kw):
+        arrays = [c, q, lower, upper]
+        counts = {np.asarray(a).shape[0] for a in arrays if a is not None}
+        if len(counts) != 1:
+            raise ValueError("case arrays must share their first dimension")
+        self.num_cases = counts.pop()
+        self._keep = [None if a is None else np.ascontiguousarray(a, np.float64) for a in arrays]
+        self._cl = CLp(base)
+        self.options = _options(options, kw)
+        self._h = C.c_void_p()
+        check(lib().anu_pdhg_batch_create(self._cl.ref(), self.num_cases,
+                                          *[f64_ptr(a) for a in self._keep],
+                                          C.byref(self.options), C.byref(self._h)))
+
+    def solve(self):
+        """Returns a list of PdhgResult, one per case."""
+        K, n, m = self.num_cases, self._cl.n, self._cl.m
+        x = np.zeros((K, n))
+        y = np.zeros((K, m))
+        res = (anu_pdhg_result * K)()
+        check(lib().anu_pdhg_batch_solve(self._h, f64_ptr(x), f64_ptr(y), res))
+        return [PdhgResult.from_c(res[k], x[k], y[k]) for k in range(K)]
+
+    def close(self):
+        if self._h:
+            lib().anu_pdhg_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def solve_case_stack(stack, options: Optional[anu_pdhg_options] = None, **kw):
+    """Solves an :class:`anukulan_b200.lpgen.CaseStack` on the engine."""
+    s = CaseStackSolver(stack.base, stack.c, stack.q, stack.lower, stack.upper, options, **kw)
+    try:
+        return s.solve()
+    finally:
+        s.close()

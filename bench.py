@@ -1,0 +1,340 @@
+"""Benchmark of the PDHG path: LP solves per second at relative KKT 1e-6.
+
+Workload (default): the 60-case refinery-shaped case stack - 24 period blocks
+of 115 rows x 160 columns (2,760 x 3,840, 43,412 nonzeros), every case
+sharing the matrix and differing from the base in one cost, supply bound,
+demand or capacity - solved by the engine as one batched FP32 run with FP64
+restart/termination checks, to relative KKT 1e-6. A step is one solve of the
+whole stack; `value` is cases solved per second with the stack's data already
+on the device; `e2e` is the same metric through the C ABI from host arrays
+(create + solve + download inside the timed region).
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+                    [--workload stack|large]
+
+Under torchrun every rank solves its own copy of the stack (weak scaling, no
+collective on the data path); rank 0 prints one JSON line. `--impl reference`
+times the reference's own CPU PDHG (oracle/_ref, compiled from the reference
+sources; the oracle port where that is absent) on the host cores, solving the
+same cases concurrently on all threads.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM = 6650.0
+TOL = 1e-6
+
+
+def hbm_peak():
+    try:
+        with open(PEAKS) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM, "fallback"
+
+
+# ----------------------------------------------------------------- clocks
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int = 0):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- workloads
+
+def stack_workload():
+    from anukulan_b200 import lpgen
+    st = lpgen.refinery_stack()
+    cfg = {"workload": "refinery_case_stack", "cases": st.num_cases,
+           "rows": st.base.num_rows, "cols": st.base.num_cols, "nnz": st.base.k.nnz,
+           "tolerance": TOL, "precision": "fp32 iterates, fp64 checks",
+           "l2": "flushed (256 MiB write) before every step"}
+    return st, cfg
+
+
+def algorithmic_bytes_per_iteration(nnz, m, n, cases, s_a, s_x):
+    """Minimum bytes one PDHG iteration moves (both fused kernels): A and A'
+    read once (value + int32 index) with their row starts, and per case x
+    read/written, c, l, u, anchor_x, x_bar written and read (8n) and y
+    read/written, q, Kx read/written, anchor_y, anchor_kx (7m)."""
+    return 2 * nnz * (s_a + 4) + 4 * (m + n + 2) + cases * s_x * (8 * n + 7 * m)
+
+
+def flush_l2(torch, buf):
+    buf.zero_()
+
+
+# -------------------------------------------------------------- our arm
+
+def run_engine(args, rank, world, local_rank):
+    import torch
+    from anukulan_b200 import pdhg
+    from anukulan_b200.abi import OPTIMAL, PRECISION_FP32, make_options
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600),
+                                device_id=torch.device("cuda", local_rank))
+    st, cfg = stack_workload()
+    opts = make_options(tolerance=TOL, precision=PRECISION_FP32, device=local_rank, profile=1)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    # value: data resident (handle created once), one solve per step
+    solver = pdhg.CaseStackSolver(st.base, st.c, st.q, st.lower, st.upper, opts)
+    for _ in range(args.warmup):
+        res = solver.solve()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    step_ms = []
+    dev_iter_s = 0.0
+    dev_iters = 0
+    launches = 0
+    solved = 0
+    total_iterations = 0
+    for _ in range(args.steps):
+        flush_l2(torch, flush)
+        barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        res = solver.solve()
+        e1.record()
+        torch.cuda.synchronize()
+        step_ms.append(e0.elapsed_time(e1))
+        solved += sum(1 for r in res if r.status == OPTIMAL)
+        dev_iter_s += res[0].device_iteration_seconds
+        dev_iters += res[0].device_iterations
+        launches += res[0].kernel_launches
+        total_iterations += max(r.iterations for r in res)
+    clk = clocks.stop()
+    solver.close()
+    # e2e: from host arrays through the C ABI, every step
+    e2e_ms = []
+    for i in range(args.warmup + args.steps):
+        flush_l2(torch, flush)
+        barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        s2 = pdhg.CaseStackSolver(st.base, st.c, st.q, st.lower, st.upper, opts)
+        r2 = s2.solve()
+        s2.close()
+        e1.record()
+        torch.cuda.synchronize()
+        if i >= args.warmup:
+            e2e_ms.append(e0.elapsed_time(e1))
+    total_ms = float(np.sum(step_ms))
+    total_e2e = float(np.sum(e2e_ms))
+    if dist is not None:
+        t = torch.tensor([total_ms, total_e2e], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms, total_e2e = float(t[0]), float(t[1])
+        s = torch.tensor([solved], device="cuda", dtype=torch.float64)
+        dist.all_reduce(s)
+        solved_all = int(s[0])
+    else:
+        solved_all = solved
+    cases_all = st.num_cases * args.steps * world
+    out = None
+    if rank == 0:
+        peak, peak_kind = hbm_peak()
+        nnz, m, n = st.base.k.nnz, st.base.num_rows, st.base.num_cols
+        bytes_it = algorithmic_bytes_per_iteration(nnz, m, n, st.num_cases, 4, 4)
+        per_launch_s = dev_iter_s / max(dev_iters, 1) / 2.0
+        achieved = (bytes_it / 2.0) / per_launch_s / 1e9 if dev_iters else None
+        h2d = (st.base.k.nnz * 12 + (st.base.num_rows + 1) * 4
+               + st.num_cases * 8 * (3 * n + m))
+        d2h = st.num_cases * 8 * (n + m)
+        out = {
+            "metric": "LP solves/s to relative KKT 1e-6 (batched FP32 PDHG, FP64 checks)",
+            "value": solved_all / (total_ms / 1e3),
+            "unit": "solves/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic (seeded generator, refinery-shaped 60-case stack)",
+            "config": dict(cfg, parallelism=f"case stacks replicated per GPU x{world}"),
+            "cases_optimal": solved_all,
+            "cases_attempted": cases_all,
+            "iterations_per_solve": total_iterations / args.steps,
+            "e2e": {"value": solved_all / (total_e2e / 1e3), "unit": "solves/s",
+                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": (achieved / peak) if achieved else None, "traffic": None,
+                         "peak_source": peak_kind,
+                         "kernel": "cases_kernel (fused SpMM + primal/dual step), mean per launch",
+                         "algorithmic_bytes_per_launch": bytes_it / 2.0,
+                         "launch_seconds": per_launch_s},
+            "clocks": clk,
+        }
+        if args.cpu_baseline:
+            out["cpu_baseline"] = cpu_baseline(st, seconds=args.cpu_seconds)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return out
+
+
+def cpu_baseline(st, seconds=15.0, threads=None, prefer_reference=True):
+    """The reference's CPU PDHG (or the oracle port) solving cases of the stack
+    concurrently, one case per host thread, for about `seconds`."""
+    import oracle
+    from concurrent.futures import ThreadPoolExecutor
+    from anukulan_b200.abi import OPTIMAL
+    threads = threads or os.cpu_count() or 1
+    use_ref = prefer_reference and oracle.have_reference()
+    solve = (lambda lp: oracle.ref_solve(lp, tolerance=TOL)) if use_ref else \
+        (lambda lp: oracle.oracle_solve(lp, tolerance=TOL))
+    done = 0
+    ok = 0
+    t0 = time.perf_counter()
+    k = 0
+    with ThreadPoolExecutor(max_workers=threads) as ex:
+        while time.perf_counter() - t0 < seconds or done == 0:
+            batch = [st.case((k + i) % st.num_cases) for i in range(threads)]
+            k += threads
+            for r in ex.map(solve, batch):
+                done += 1
+                ok += int(r.status == OPTIMAL)
+    dt = time.perf_counter() - t0
+    return {"value": ok / dt, "unit": "solves/s", "cores": threads,
+            "kind": "reference" if use_ref else "port",
+            "sample": f"{done} cases of the stack, {threads} concurrent single-thread solves "
+                      f"(cpu_backend), {dt:.1f} s"}
+
+
+# ---------------------------------------------------------- reference arm
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    try:
+        import oracle  # noqa: F401
+    except Exception as e:  # pragma: no cover
+        return {"impl": "reference", "unavailable": f"oracle package missing: {e}"}
+    st, cfg = stack_workload()
+    threads = os.cpu_count() or 1
+    per_step = []
+    solved = 0
+    for i in range(args.warmup + args.steps):
+        r = cpu_baseline(st, seconds=args.ref_seconds, threads=threads)
+        if i >= args.warmup:
+            per_step.append(r)
+            solved += 1
+    value = float(np.mean([r["value"] for r in per_step]))
+    return {
+        "impl": "reference",
+        "metric": "LP solves/s to relative KKT 1e-6 (batched FP32 PDHG, FP64 checks)",
+        "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": args.ref_seconds * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded generator, refinery-shaped 60-case stack)",
+        "config": cfg,
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": per_step[0]["cores"],
+                         "kind": per_step[0]["kind"], "sample": per_step[0]["sample"]},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--ref-seconds", type=float, default=10.0)
+    args = ap.parse_args(argv)
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        out = run_reference(args, rank, world)
+    else:
+        out = run_engine(args, rank, world, local_rank)
+    if rank == 0 and out is not None:
+        print(json.dumps(out), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

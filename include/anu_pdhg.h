@@ -154,6 +154,10 @@ typedef struct anu_pdhg_options {
   double refinement_inner_tolerance;
   int32_t device;               /* CUDA device ordinal, 0 */
   int32_t use_graphs;           /* capture iteration chunks in CUDA graphs, 1 */
+  /* Record CUDA events around every iteration chunk on the engine's stream
+   * and report their total in anu_pdhg_result::device_iteration_seconds.
+   * Events do not serialise the stream. 0 = off. */
+  int32_t profile;
 } anu_pdhg_options;
 
 /* PdhgResidual, src/anukulan/pdhg.hpp:429-496. */
@@ -206,6 +210,11 @@ typedef struct anu_pdhg_result {
   /* engine additions */
   int32_t refinement_rounds; /* outer refinement rounds actually run */
   int32_t kernel_launches;   /* kernels this solve launched (graph nodes included) */
+  /* With options.profile: device time of the iteration chunks (CUDA events
+   * on the engine stream) and the iterations they ran, summed over every
+   * case run this result shares (a case stack runs its cases together). */
+  double device_iteration_seconds;
+  int64_t device_iterations;
   char message[160];
 } anu_pdhg_result;
 

@@ -97,6 +97,13 @@ def ref_lib():
                  [C.c_void_p, C.c_double, _P(C.c_double), _P(C.c_double),
                   _P(C.c_double), _P(C.c_int)])
         _declare(lib, "ref_default_thread_count", C.c_int, [])
+        _declare(lib, "ref_default_options", None, [_P(anu_pdhg_options)])
+        _declare(lib, "ref_to_standard_form", C.c_int,
+                 [C.c_int32, C.c_int32, C.c_int32, _P(C.c_int32), _P(C.c_int32),
+                  _P(C.c_double)] + [_P(C.c_double)] * 5 + [C.c_int, C.c_double,
+                  _P(C.c_int32), _P(C.c_int32), _P(C.c_double), _P(C.c_double),
+                  _P(C.c_double), _P(C.c_int32), _P(C.c_double), _P(C.c_double),
+                  _P(C.c_int32)])
         _ref = lib
     return _ref
 
@@ -197,6 +204,47 @@ def ref_simplex(lp: StandardLp, time_limit: float = 300.0):
     st = ref_lib().ref_simplex_solve(cl.ref(), time_limit, f64_ptr(x), f64_ptr(y),
                                      C.byref(obj), C.byref(its))
     return st, obj.value, its.value, x, y
+
+
+def ref_default_options() -> anu_pdhg_options:
+    o = anu_pdhg_options()
+    ref_lib().ref_default_options(C.byref(o))
+    return o
+
+
+def ref_to_standard_form(model) -> Optional[StandardLp]:
+    """The reference's to_standard_form of a :class:`Model`."""
+    from anukulan_b200.model import Csr
+    a = model.constraints
+    m, n, nnz = a.rows, a.cols, a.nnz
+    i32 = lambda arr: np.ascontiguousarray(arr, np.int32)
+    f64 = lambda arr: np.ascontiguousarray(arr, np.float64)
+    keep = [i32(a.start), i32(a.index), f64(a.value), f64(model.objective),
+            f64(model.row_lower), f64(model.row_upper), f64(model.col_lower),
+            f64(model.col_upper)]
+    o_start = np.zeros(2 * m + 1, np.int32)
+    o_index = np.zeros(max(2 * nnz, 1), np.int32)
+    o_value = np.zeros(max(2 * nnz, 1))
+    o_c = np.zeros(max(n, 1))
+    o_q = np.zeros(max(2 * m, 1))
+    o_row = np.zeros(max(2 * m, 1), np.int32)
+    o_sign = np.zeros(max(2 * m, 1))
+    so = np.zeros(2)
+    sizes = np.zeros(2, np.int32)
+    ip = lambda arr: arr.ctypes.data_as(_P(C.c_int32))
+    rows = ref_lib().ref_to_standard_form(
+        m, n, nnz, ip(keep[0]), ip(keep[1]), f64_ptr(keep[2]), f64_ptr(keep[3]),
+        f64_ptr(keep[4]), f64_ptr(keep[5]), f64_ptr(keep[6]), f64_ptr(keep[7]),
+        int(model.maximize), float(model.objective_offset), ip(o_start), ip(o_index),
+        f64_ptr(o_value), f64_ptr(o_c), f64_ptr(o_q), ip(o_row), f64_ptr(o_sign), f64_ptr(so),
+        ip(sizes))
+    if rows < 0:
+        return None
+    k = Csr(rows, n, o_start[:rows + 1].copy(), o_index[:sizes[1]].copy(),
+            o_value[:sizes[1]].copy())
+    return StandardLp(k, o_c[:n].copy(), o_q[:rows].copy(), f64(model.col_lower).copy(),
+                      f64(model.col_upper).copy(), int(sizes[0]), float(so[0]), float(so[1]),
+                      o_row[:rows].copy(), o_sign[:rows].copy())
 
 
 def oracle_solve_many(lps, options=None, threads: int = 1, **kw):

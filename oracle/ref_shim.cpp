@@ -249,4 +249,93 @@ int ref_simplex_solve(const anu_lp* lp_in, double time_limit, double* x, double*
 
 int ref_default_thread_count(void) { return anukulan::default_thread_count(); }
 
+// PdhgOptions{} (src/anukulan/pdhg.hpp:19-415) written into the engine's
+// options struct, so the tests can check both carry the same defaults.
+void ref_default_options(anu_pdhg_options* o) {
+  const anukulan::PdhgOptions p;
+  std::memset(o, 0, sizeof(*o));
+  o->tolerance = p.tolerance;
+  o->gap_tolerance = p.gap_tolerance;
+  o->max_iterations = p.max_iterations;
+  o->time_limit_seconds = p.time_limit_seconds;
+  o->termination_check_frequency = p.termination_check_frequency;
+  o->absolute_tolerance = p.absolute_tolerance;
+  o->require_inf_norm_termination = p.require_inf_norm_termination;
+  o->adaptive_step_size = p.adaptive_step_size;
+  o->primal_weight_updates = p.primal_weight_updates;
+  o->restarts = p.restarts;
+  o->halpern = p.halpern;
+  o->halpern_restart = p.halpern_restart;
+  o->halpern_minimum_epoch = p.halpern_minimum_epoch;
+  o->polish_feasibility = p.polish_feasibility;
+  o->polish_first_iteration = p.polish_first_iteration;
+  o->polish_iteration_factor = p.polish_iteration_factor;
+  o->polish_minimum_iterations = p.polish_minimum_iterations;
+  o->polish_maximum_iterations = p.polish_maximum_iterations;
+  o->polish_on_exit = p.polish_on_exit;
+  o->reflection = p.reflection;
+  o->constant_step_size = p.constant_step_size;
+  o->constant_step_scale = p.constant_step_scale;
+  o->restart_on_fixed_point = p.restart_on_fixed_point;
+  o->pid_primal_weight = p.pid_primal_weight;
+  o->primal_weight_kp = p.primal_weight_kp;
+  o->primal_weight_ki = p.primal_weight_ki;
+  o->primal_weight_kd = p.primal_weight_kd;
+  o->ruiz_iterations = p.scaling.ruiz_iterations;
+  o->pock_chambolle = p.scaling.pock_chambolle;
+  o->reuse_products = p.reuse_products;
+  o->detect_infeasibility = p.detect_infeasibility;
+  o->infeasibility_tolerance = p.infeasibility_tolerance;
+  o->termination = static_cast<int32_t>(p.termination);
+  o->known_matrix_norm = p.known_matrix_norm;
+  o->initial_step_size = p.initial_step_size;
+  o->initial_primal_weight = p.initial_primal_weight;
+  o->verbose = p.verbose;
+  o->log_frequency = p.log_frequency;
+}
+
+// to_standard_form (src/anukulan/standard_form.cpp:72-165) of a model given
+// as CSR rows with row and column bounds. Output capacity: 2*rows rows and
+// 2*nnz nonzeros. Returns the standard-form row count, or -1 on failure;
+// sizes[0] = num_equalities, sizes[1] = nnz.
+int ref_to_standard_form(int32_t rows, int32_t cols, int32_t nnz, const int32_t* start,
+                         const int32_t* index, const double* value, const double* objective,
+                         const double* row_lower, const double* row_upper,
+                         const double* col_lower, const double* col_upper, int maximize,
+                         double offset, int32_t* out_start, int32_t* out_index,
+                         double* out_value, double* out_c, double* out_q,
+                         int32_t* out_origin_row, double* out_origin_sign,
+                         double* out_scale_offset, int32_t* sizes) {
+  anukulan::Model model;
+  anu_csr a{rows, cols, nnz, start, index, value};
+  model.constraints = csr_to_matrix(a);
+  model.objective.assign(objective, objective + cols);
+  model.row_lower.assign(row_lower, row_lower + rows);
+  model.row_upper.assign(row_upper, row_upper + rows);
+  model.col_lower.assign(col_lower, col_lower + cols);
+  model.col_upper.assign(col_upper, col_upper + cols);
+  model.col_type.assign(static_cast<std::size_t>(cols), anukulan::VarType::kContinuous);
+  model.sense = maximize ? anukulan::ObjSense::kMaximize : anukulan::ObjSense::kMinimize;
+  model.objective_offset = offset;
+  const anukulan::StandardFormResult sf = anukulan::to_standard_form(model);
+  if (!sf.ok) return -1;
+  const anukulan::StandardLp& lp = sf.lp;
+  for (Int i = 0; i <= lp.k.rows(); ++i) out_start[i] = lp.k.start()[static_cast<std::size_t>(i)];
+  for (Int k = 0; k < lp.k.nnz(); ++k) {
+    out_index[k] = lp.k.index()[static_cast<std::size_t>(k)];
+    out_value[k] = lp.k.value()[static_cast<std::size_t>(k)];
+  }
+  for (std::size_t j = 0; j < lp.c.size(); ++j) out_c[j] = lp.c[j];
+  for (std::size_t i = 0; i < lp.q.size(); ++i) {
+    out_q[i] = lp.q[i];
+    out_origin_row[i] = lp.row_origin[i].model_row;
+    out_origin_sign[i] = lp.row_origin[i].sign;
+  }
+  out_scale_offset[0] = lp.objective_scale;
+  out_scale_offset[1] = lp.objective_offset;
+  sizes[0] = lp.num_equalities;
+  sizes[1] = lp.k.nnz();
+  return lp.k.rows();
+}
+
 }  // extern "C"

@@ -1,0 +1,298 @@
+"""Parity of the sm_100a engine against the oracle (the restated reference
+PDHG path) and the reference's golden fixtures, through the C ABI.
+
+Tolerances (FP64 engine): the engine runs the reference's arithmetic without
+FMA contraction, but sums reductions as trees where the reference sums
+serially, so iterates agree to ~1e-12 relative and iteration counts agree
+exactly on these problems (allowed to differ by one check period where a
+restart test sits within rounding of its threshold). FP32 engine: every
+returned point is re-evaluated in FP64 by the oracle and must meet the
+requested relative KKT tolerance.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import lp_cases
+import oracle
+from anukulan_b200 import lpgen
+from anukulan_b200.abi import (ITERATION_LIMIT, OPTIMAL, PRECISION_FP32,
+                               PRIMAL_INFEASIBLE)
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "pdhg_golden.npz")
+FP64_ITERATE_RTOL = 1e-10
+
+
+def rel_err(a, b):
+    a = np.asarray(a)
+    b = np.asarray(b)
+    return float(np.max(np.abs(a - b)) / max(1.0, float(np.max(np.abs(b)))))
+
+
+@pytest.mark.parametrize("name", sorted(lp_cases.KNOWN))
+def test_known_optima_fp64(engine, name):
+    builder, objective, x = lp_cases.KNOWN[name]
+    lp = lp_cases.standard(builder())
+    r = engine.solve_pdhg(lp, tolerance=1e-8)
+    o = oracle.oracle_solve(lp, tolerance=1e-8)
+    assert r.status == OPTIMAL
+    assert abs(r.objective - objective) <= 1e-6 * max(1.0, abs(objective))
+    if x is not None:
+        np.testing.assert_allclose(r.x, x, atol=1e-5)
+    assert r.iterations == o.iterations
+    assert r.restarts == o.restarts
+    assert rel_err(r.x, o.x) < 1e-9 and rel_err(r.y, o.y) < 1e-9
+
+
+@pytest.mark.parametrize("name", sorted(lp_cases.KNOWN))
+def test_known_optima_fp32(engine, name):
+    builder, objective, _ = lp_cases.KNOWN[name]
+    lp = lp_cases.standard(builder())
+    r = engine.solve_pdhg(lp, tolerance=1e-6, precision=PRECISION_FP32)
+    assert r.status == OPTIMAL
+    res = oracle.oracle_residual(lp, r.x, r.y)
+    assert res.converged(1e-6), res
+    assert abs(r.objective - objective) <= 1e-4 * max(1.0, abs(objective))
+
+
+def test_iterates_after_n_iterations_fp64(engine):
+    lp, _ = lpgen.random_lp()
+    for n_it in (40, 200, 1000):
+        kw = dict(max_iterations=n_it, polish_on_exit=0, polish_feasibility=0)
+        r = engine.solve_pdhg(lp, **kw)
+        o = oracle.oracle_solve(lp, **kw)
+        assert r.status == o.status == ITERATION_LIMIT
+        assert r.iterations == o.iterations == n_it
+        assert r.restarts == o.restarts
+        assert rel_err(r.x, o.x) < FP64_ITERATE_RTOL, n_it
+        assert rel_err(r.y, o.y) < FP64_ITERATE_RTOL, n_it
+
+
+def test_random_lp_full_solve_fp64_matches_golden(engine):
+    g = np.load(GOLDEN)
+    lp, obj = lpgen.random_lp()
+    r = engine.solve_pdhg(lp, tolerance=1e-6)
+    assert r.status == OPTIMAL
+    assert abs(r.iterations - int(g["random_1000x1500/iterations"])) <= 40
+    assert abs(r.objective - float(g["random_1000x1500/objective"])) <= 1e-9 * abs(obj)
+    assert abs(r.objective - obj) <= 1e-5 * abs(obj)
+
+
+def test_random_lp_fp32_reaches_tolerance(engine):
+    lp, obj = lpgen.random_lp()
+    r = engine.solve_pdhg(lp, tolerance=1e-6, precision=PRECISION_FP32)
+    assert r.status == OPTIMAL, r.message
+    res = oracle.oracle_residual(lp, r.x, r.y)
+    assert res.converged(1e-6), res
+    assert abs(r.objective - obj) <= 1e-5 * abs(obj)
+
+
+def test_iteration_limit_exact(engine):
+    lp = lp_cases.standard(lp_cases.wyndor())
+    r = engine.solve_pdhg(lp, tolerance=1e-14, max_iterations=80,
+                          termination_check_frequency=40)
+    assert r.status == ITERATION_LIMIT and r.iterations == 80
+
+
+def test_infeasible_detected(engine):
+    r = engine.solve_pdhg(lp_cases.standard(lp_cases.infeasible()), tolerance=1e-8)
+    assert r.status == PRIMAL_INFEASIBLE
+
+
+def test_empty_matrix(engine):
+    r = engine.solve_pdhg(lp_cases.standard(lp_cases.empty_rows()), tolerance=1e-8)
+    np.testing.assert_allclose(r.x, [0.0, 5.0], atol=1e-6)
+    assert abs(r.objective + 5.0) <= 1e-6
+
+
+def test_deterministic(engine):
+    lp, _ = lpgen.random_lp(300, 450, 8, seed=4)
+    a = engine.solve_pdhg(lp)
+    b = engine.solve_pdhg(lp)
+    assert a.iterations == b.iterations and a.restarts == b.restarts
+    assert np.array_equal(a.x, b.x) and np.array_equal(a.y, b.y)
+
+
+def test_warm_start_is_used(engine):
+    lp = lp_cases.standard(lp_cases.wyndor())
+    cold = engine.solve_pdhg(lp, tolerance=1e-8)
+    warm = engine.solve_pdhg(lp, tolerance=1e-8, warm_x=cold.x, warm_y=cold.y,
+                             ruiz_iterations=0, pock_chambolle=0)
+    assert warm.status == OPTIMAL and warm.iterations < cold.iterations
+
+
+OPTION_SETS = [
+    dict(halpern=0),
+    dict(restart_on_fixed_point=0),
+    dict(pid_primal_weight=0),
+    dict(restarts=0, max_iterations=20000),
+    dict(tolerance=1e-8, gap_tolerance=1e-2),
+    dict(reuse_products=0),
+    dict(constant_step_size=0, max_iterations=2000),
+    dict(halpern_restart=1, max_iterations=2000),
+    dict(ruiz_iterations=0, pock_chambolle=0),
+    dict(use_graphs=0),
+]
+
+
+@pytest.mark.parametrize("opts", OPTION_SETS,
+                         ids=lambda d: ",".join(f"{k}={v}" for k, v in d.items()))
+def test_option_configurations_match_oracle(engine, opts):
+    lp, _ = lpgen.random_lp(300, 450, 8, seed=11)
+    r = engine.solve_pdhg(lp, **opts)
+    o = oracle.oracle_solve(lp, **opts)
+    assert r.status == o.status
+    assert abs(r.iterations - o.iterations) <= 40
+    if o.status == OPTIMAL:
+        assert abs(r.objective - o.objective) <= 1e-6 * max(1.0, abs(o.objective))
+
+
+def test_evaluate_residual_matches_oracle(engine):
+    lp, _ = lpgen.random_lp(300, 450, 8, seed=5)
+    rng = np.random.default_rng(3)
+    x = rng.uniform(0, 10, lp.num_cols)
+    y = rng.standard_normal(lp.num_rows)
+    a = engine.evaluate_residual(lp, x, y)
+    b = oracle.oracle_residual(lp, x, y)
+    for f in ("relative_primal", "relative_dual", "relative_gap", "primal_objective",
+              "dual_objective", "primal_residual_inf", "dual_residual_inf"):
+        assert abs(getattr(a, f) - getattr(b, f)) <= 1e-12 * max(1.0, abs(getattr(b, f))), f
+
+
+def test_matrix_norm_matches_oracle(engine):
+    lp = lp_cases.standard(lp_cases.norm_4())
+    assert abs(engine.estimate_matrix_norm(lp, 500, 1e-12) - 4.0) <= 1e-6
+    lp2, _ = lpgen.random_lp(300, 450, 8, seed=5)
+    a = engine.estimate_matrix_norm(lp2)
+    b = oracle.oracle_matrix_norm(lp2)
+    assert abs(a - b) <= 1e-12 * b
+
+
+def test_invalid_lp_rejected(engine):
+    lp = lp_cases.standard(lp_cases.wyndor())
+    bad = lp.with_vectors(lower=np.array([1.0, 0.0]), upper=np.array([0.0, 1.0]))
+    with pytest.raises(engine.EngineError) as e:
+        engine.solve_pdhg(bad)
+    assert e.value.code == 1
+
+
+# ---------------------------------------------------------------- case stack
+
+
+@pytest.fixture(scope="module")
+def stack():
+    return lpgen.refinery_stack()
+
+
+def test_case_stack_fp64_matches_golden(engine, stack):
+    g = np.load(GOLDEN)
+    res = engine.solve_case_stack(stack, tolerance=1e-6)
+    assert len(res) == 60
+    for k in (0, 33, 45, 55):
+        name = f"refinery_case{k}"
+        assert res[k].status == OPTIMAL
+        assert abs(res[k].iterations - int(g[f"{name}/iterations"])) <= 80, k
+        ref_obj = float(g[f"{name}/objective"])
+        assert abs(res[k].objective - ref_obj) <= 1e-7 * abs(ref_obj), k
+    for k, r in enumerate(res):
+        assert r.status == OPTIMAL, (k, r.message)
+
+
+def test_case_stack_fp32_reaches_tolerance(engine, stack):
+    res = engine.solve_case_stack(stack, tolerance=1e-6, precision=PRECISION_FP32)
+    g = np.load(GOLDEN)
+    for k, r in enumerate(res):
+        assert r.status == OPTIMAL, (k, r.message)
+        if k in (0, 33, 45, 55):
+            res_k = oracle.oracle_residual(stack.case(k), r.x, r.y)
+            assert res_k.converged(1e-6), (k, res_k)
+            ref_obj = float(g[f"refinery_case{k}/objective"])
+            assert abs(r.objective - ref_obj) <= 1e-5 * abs(ref_obj)
+
+
+def test_case_stack_equals_single_solves(engine, stack):
+    sub = lpgen.CaseStack(stack.base, stack.names[:5], stack.c[:5], stack.q[:5],
+                          stack.lower[:5], stack.upper[:5])
+    batch = engine.solve_case_stack(sub, tolerance=1e-6)
+    for k in range(5):
+        single = engine.solve_pdhg(stack.case(k), tolerance=1e-6)
+        assert batch[k].status == single.status
+        assert abs(batch[k].iterations - single.iterations) <= 40
+        assert abs(batch[k].objective - single.objective) <= 1e-8 * abs(single.objective)
+
+
+# ------------------------------------------------------------- backend seam
+
+
+def test_backend_seam_contract(engine):
+    import ctypes as C
+    L = engine.lib()
+    rng = np.random.default_rng(20260830)
+    n, m = 733, 501
+
+    def dev(v):
+        p = C.c_void_p()
+        engine.check(L.anu_backend_allocate(len(v), C.byref(p)))
+        a = np.ascontiguousarray(v, np.float64)
+        engine.check(L.anu_backend_upload(a.ctypes.data_as(C.POINTER(C.c_double)), p, len(v)))
+        return p
+
+    def host(p, count):
+        out = np.zeros(count)
+        engine.check(L.anu_backend_download(p, out.ctypes.data_as(C.POINTER(C.c_double)), count))
+        return out
+
+    x = rng.uniform(-1, 1, n)
+    c = rng.standard_normal(n)
+    kty = rng.standard_normal(n)
+    lo = np.full(n, -0.5)
+    hi = np.full(n, 0.5)
+    anchor = rng.standard_normal(n)
+    px, pc, pk, pl, ph, pa = map(dev, (x, c, kty, lo, hi, anchor))
+    xo, dxo, xbo = dev(np.zeros(n)), dev(np.zeros(n)), dev(np.zeros(n))
+    tau, gamma, w = 0.3, 1.0, 0.75
+    engine.check(L.anu_backend_primal_update(n, tau, gamma, w, px, pc, pk, pl, ph, pa, xo, dxo, xbo))
+    v = np.clip(x - tau * (c - kty), lo, hi)
+    d = v - x
+    nxt = w * (v + gamma * d) + (1 - w) * anchor
+    assert np.array_equal(host(dxo, n), d)
+    assert np.array_equal(host(xbo, n), v + d)
+    assert np.array_equal(host(xo, n), nxt)
+    # dot / norms
+    out = C.c_double()
+    engine.check(L.anu_backend_dot(px, pc, n, C.byref(out)))
+    assert abs(out.value - float(np.dot(x, c))) <= 1e-13 * np.abs(x * c).sum()
+    engine.check(L.anu_backend_inf_norm(pc, n, C.byref(out)))
+    assert out.value == float(np.max(np.abs(c)))
+    # sparse product, ragged rows, every 5th row empty
+    r, cc, vv = [], [], []
+    for i in range(m):
+        if i % 5 == 0:
+            continue
+        length = 2 + (i * 7) % 40 if i % 100 else 3000
+        cols = rng.choice(n, size=min(length, n), replace=False)
+        r += [i] * len(cols)
+        cc += list(cols)
+        vv += list(rng.standard_normal(len(cols)))
+    from anukulan_b200.model import Csr
+    from anukulan_b200.abi import anu_csr
+    a = Csr.from_triplets(m, n, r, cc, vv)
+    st = np.ascontiguousarray(a.start, np.int32)
+    ix = np.ascontiguousarray(a.index, np.int32)
+    va = np.ascontiguousarray(a.value, np.float64)
+    csr = anu_csr(m, n, a.nnz, st.ctypes.data_as(C.POINTER(C.c_int32)),
+                  ix.ctypes.data_as(C.POINTER(C.c_int32)),
+                  va.ctypes.data_as(C.POINTER(C.c_double)))
+    engine.check(L.anu_backend_prepare(12345, C.byref(csr)))
+    py = dev(np.zeros(m))
+    engine.check(L.anu_backend_multiply(12345, px, py))
+    want = np.array([sum(a.value[k] * x[a.index[k]] for k in range(a.start[i], a.start[i + 1]))
+                     for i in range(m)])
+    got = host(py, m)
+    assert np.max(np.abs(got - want)) <= 1e-13 * max(1.0, np.max(np.abs(want)))
+    engine.check(L.anu_backend_release())
+    for p in (px, pc, pk, pl, ph, pa, xo, dxo, xbo, py):
+        engine.check(L.anu_backend_deallocate(p))

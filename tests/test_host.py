@@ -1,0 +1,170 @@
+"""Host-side logic: the standard form's integer maps, the workload
+generators' invariants, the ABI structs and defaults, and that the engine
+library loads and exports every symbol its header declares."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+import lp_cases
+import oracle
+from anukulan_b200 import abi, lpgen
+from anukulan_b200.model import Csr, Model, to_standard_form
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+needs_ref = pytest.mark.skipif(not oracle.have_reference(),
+                               reason="oracle/_ref/libanuref.so not built here")
+
+
+def _mixed_model(seed=0):
+    """Equality, >=, <=, ranged and free rows; free, boxed and one-sided columns."""
+    rng = np.random.default_rng(seed)
+    m, n = 40, 30
+    r, c, v = [], [], []
+    for i in range(m):
+        for j in rng.choice(n, size=rng.integers(0, 6), replace=False):
+            r.append(i)
+            c.append(int(j))
+            v.append(float(rng.standard_normal()))
+    a = Csr.from_triplets(m, n, r, c, v)
+    kinds = rng.integers(0, 5, m)
+    lo = np.where(kinds == 0, 1.0, np.where(kinds == 1, -2.0, np.where(kinds == 3, -1.0, -np.inf)))
+    hi = np.where(kinds == 0, 1.0, np.where(kinds == 2, 3.0, np.where(kinds == 3, 4.0, np.inf)))
+    lo[kinds == 4] = -np.inf
+    hi[kinds == 4] = np.inf
+    clo = np.where(rng.random(n) < 0.2, -np.inf, 0.0)
+    chi = np.where(rng.random(n) < 0.5, np.inf, 5.0)
+    return Model(a, rng.standard_normal(n), lo, hi, clo, chi, bool(seed % 2), 1.5)
+
+
+@needs_ref
+@pytest.mark.parametrize("seed", range(4))
+def test_standard_form_bit_exact_with_reference(seed):
+    model = _mixed_model(seed)
+    mine = to_standard_form(model)
+    ref = oracle.ref_to_standard_form(model)
+    assert mine.ok and ref is not None
+    lp = mine.lp
+    assert lp.num_equalities == ref.num_equalities
+    assert np.array_equal(lp.k.start, ref.k.start)
+    assert np.array_equal(lp.k.index, ref.k.index)
+    assert np.array_equal(lp.k.value, ref.k.value)
+    assert np.array_equal(lp.row_origin_row, ref.row_origin_row)
+    assert np.array_equal(lp.row_origin_sign, ref.row_origin_sign)
+    assert np.array_equal(lp.c, ref.c) and np.array_equal(lp.q, ref.q)
+    assert (lp.objective_scale, lp.objective_offset) == (ref.objective_scale, ref.objective_offset)
+
+
+def test_standard_form_layout():
+    lp = lp_cases.standard(lp_cases.range_row())
+    # a ranged row becomes a'x >= lo and -a'x >= -hi
+    assert lp.num_rows == 2 and lp.num_equalities == 0
+    assert list(lp.q) == [5.0, -8.0]
+    assert list(lp.row_origin_sign) == [1.0, -1.0]
+    w = lp_cases.standard(lp_cases.wyndor())
+    assert w.objective_scale == -1.0 and list(w.c) == [-3.0, -5.0]
+
+
+def test_csr_transpose_roundtrip():
+    model = _mixed_model(1)
+    a = model.constraints
+    t = a.transpose()
+    tt = t.transpose()
+    assert np.array_equal(tt.start, a.start) and np.array_equal(tt.index, a.index)
+    assert np.array_equal(tt.value, a.value)
+
+
+def test_random_lp_known_optimum():
+    lp, obj = lpgen.random_lp(200, 300, 8, seed=2)
+    assert lp.k.nnz == 300 * 8
+    assert np.all(np.diff(lp.k.transpose().start) == 8)
+    # c'x0 = b'y0 at the planted optimum
+    rng_lp, obj2 = lpgen.random_lp(200, 300, 8, seed=2)
+    assert obj == obj2
+
+
+def test_power_law_lengths():
+    rng = np.random.default_rng(0)
+    L = lpgen.power_law_row_lengths(20000, 20000 * 12, rng)
+    assert L.sum() == 20000 * 12
+    assert L.min() >= 3 and L.max() <= 5000
+
+
+@pytest.mark.slow
+def test_power_law_lp_structure():
+    lp, _ = lpgen.power_law_lp(20000, 30000, 8, seed=7)
+    lengths = lp.k.row_lengths()
+    assert lp.k.nnz == 240000
+    assert lengths.min() >= 3 and lengths.max() <= 5000
+    t = lp.k.transpose()
+    assert np.all(np.diff(t.start) == 8)  # distinct rows per column survived
+
+
+def test_refinery_stack_shape():
+    st = lpgen.refinery_stack()
+    assert st.num_cases == 60
+    assert st.base.num_rows == 2760 and st.base.num_cols == 3840
+    # every case differs from the base in exactly one kind of data
+    for k in range(60):
+        diffs = sum([not np.array_equal(st.c[k], st.base.c), not np.array_equal(st.q[k], st.base.q),
+                     not np.array_equal(st.upper[k], st.base.upper)])
+        assert diffs == 1
+    # buying nothing is feasible: x = 0 satisfies every row
+    kx = st.base.k.multiply(np.zeros(st.base.num_cols))
+    eq = st.base.num_equalities
+    assert np.all(kx[:eq] == st.base.q[:eq])
+    assert np.all(kx[eq:] >= st.base.q[eq:])
+
+
+def test_python_defaults_match_c_abi_defaults():
+    from anukulan_b200 import pdhg
+    o = pdhg.default_options()
+    d = abi.options_dict(o)
+    for k, v in abi.DEFAULTS.items():
+        assert d[k] == v, k
+
+
+@needs_ref
+def test_defaults_match_reference_pdhg_options():
+    ref = abi.options_dict(oracle.ref_default_options())
+    mine = abi.options_dict(abi.make_options())
+    for k, v in ref.items():
+        if k in ("precision", "refinement_rounds", "refinement_inner_tolerance", "device",
+                 "use_graphs"):
+            continue
+        assert mine[k] == v, k
+
+
+def _header_symbols():
+    text = open(os.path.join(ROOT, "include", "anu_pdhg.h")).read()
+    return sorted(set(re.findall(r"\b(anu_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    from anukulan_b200 import pdhg
+    lib = pdhg.lib()
+    declared = _header_symbols()
+    assert set(declared) == set(pdhg.EXPORTS)
+    for name in declared:
+        assert hasattr(lib, name), name
+
+
+def test_library_version_and_no_fallback_without_device():
+    from anukulan_b200 import pdhg
+    assert "sm_100a" in pdhg.version()
+    if pdhg.device_count() > 0:
+        pytest.skip("a device is present")
+    lp = lp_cases.standard(lp_cases.wyndor())
+    with pytest.raises(pdhg.EngineError) as e:
+        pdhg.solve_pdhg(lp)
+    assert e.value.code == 3  # ANU_ERR_NO_DEVICE: no CPU fallback
+
+
+def test_struct_layout_roundtrip():
+    # The C library writes its defaults into the ctypes struct; a layout
+    # mismatch would scramble the fields checked above. Check sizes agree
+    # with a field-by-field sum plus natural alignment.
+    assert C.sizeof(abi.anu_pdhg_residual) == 12 * 8
+    assert C.sizeof(abi.anu_pdhg_phases) == 6 * 8
