@@ -104,8 +104,8 @@ DEFAULTS = dict(
     primal_weight_kd=0.3, ruiz_iterations=10, pock_chambolle=1, reuse_products=1,
     detect_infeasibility=1, infeasibility_tolerance=1e-8, termination=0,
     known_matrix_norm=0.0, initial_step_size=0.0, initial_primal_weight=0.0,
-    verbose=0, log_frequency=5000, precision=0, refinement_rounds=0,
-    refinement_inner_tolerance=0.0, device=0, use_graphs=1, profile=0,
+    verbose=0, log_frequency=5000, precision=0, refinement_rounds=8,
+    refinement_inner_tolerance=1e-3, device=0, use_graphs=1, profile=0,
 )
 
 

@@ -352,10 +352,11 @@ int anu_backend_convergence_terms(int64_t n, int64_t m, const double* c, const d
     anu::check_len(n);
     anu::check_len(m);
     if (s.out.n < 18) s.out.alloc(18);
-    anu::RowCheckTerms<double, double> rt{1, static_cast<int32_t>(num_equalities), k_x, y,
-                                          nullptr, nullptr, nullptr, q, nullptr, row_scale};
-    anu::ColCheckTerms<double> ct{1, kt_y, x, nullptr, nullptr, nullptr, c, lower, upper,
-                                  col_scale, nullptr, nullptr, nullptr};
+    anu::RowCheckTerms<double, double, double> rt{1, static_cast<int32_t>(num_equalities), k_x,
+                                                  y, nullptr, nullptr, nullptr, nullptr, q,
+                                                  nullptr, row_scale};
+    anu::ColCheckTerms<double, double> ct{1, kt_y, x, nullptr, nullptr, nullptr, nullptr, c,
+                                          lower, upper, col_scale, nullptr, nullptr, nullptr};
     anu::reduce_terms(s.exec, static_cast<int32_t>(m), 1, rt, s.partial, s.out.p, 18, 0);
     anu::reduce_terms(s.exec, static_cast<int32_t>(n), 1, ct, s.partial, s.out.p, 18, 9);
     double h[18];

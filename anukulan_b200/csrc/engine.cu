@@ -346,8 +346,8 @@ void set_message(anu_pdhg_result* r, const std::string& m) {
   std::snprintf(r->message, sizeof(r->message), "%s", m.c_str());
 }
 
-constexpr int kRowTerms = RowCheckTerms<double, double>::NT;  // 9
-constexpr int kColTerms = ColCheckTerms<double>::NT;          // 9
+constexpr int kRowTerms = RowCheckTerms<double, double, double>::NT;  // 9
+constexpr int kColTerms = ColCheckTerms<double, double>::NT;          // 9
 constexpr int kCheckTerms = kRowTerms + kColTerms;            // 18
 constexpr int kKktTerms = 5;  // primal_sq, q_dot_y, dual_sq, bound_term, c_dot_x
 
@@ -403,10 +403,10 @@ void eval_points_terms(Problem& p, bool unit, int K, const std::vector<const Cas
   up(dq, hq);
   product<double, double, double>(p, p.dk, dx.p, K, StoreEpi<double>{K, kx.p});
   product<double, double, double>(p, p.dkt, dy.p, K, StoreEpi<double>{K, kty.p});
-  RowCheckTerms<double, double> rt{K, p.num_eq, kx.p, dy.p, dy.p, nullptr, nullptr, dq.p,
-                                   nullptr, unit ? nullptr : p.row_scale.p};
-  ColCheckTerms<double> ct{K, kty.p, dx.p, dx.p, nullptr, nullptr, dc.p, dl.p, du.p,
-                           unit ? nullptr : p.col_scale.p, nullptr, nullptr, nullptr};
+  RowCheckTerms<double, double, double> rt{K, p.num_eq, kx.p, dy.p, nullptr, nullptr, nullptr,
+                                           nullptr, dq.p, nullptr, unit ? nullptr : p.row_scale.p};
+  ColCheckTerms<double, double> ct{K, kty.p, dx.p, nullptr, nullptr, nullptr, nullptr, dc.p, dl.p,
+                                   du.p, unit ? nullptr : p.col_scale.p, nullptr, nullptr, nullptr};
   reduce_terms(p, m, K, rt, part, out.p, kCheckTerms, 0);
   reduce_terms(p, n, K, ct, part, out.p, kCheckTerms, kRowTerms);
   terms->resize(static_cast<size_t>(kCheckTerms) * K);
@@ -438,7 +438,35 @@ struct CaseState {
   std::vector<double> polished_x, polished_y;
   anu_pdhg_residual polished_residual{};
   ResidualScales scales{};
+  // Iterative refinement (FP32): the round, the worst relative KKT error the
+  // round started from and the best one it has reached, the history of
+  // checks in the round, the iteration it started at, and its Delta.
+  int32_t round = 0;
+  double round_start_worst = 1.0;
+  double best_worst = INFINITY;
+  std::vector<double> history;
+  int32_t round_offset = 0;
+  double delta = 1.0;
+  bool final_from_best = false;
 };
+
+// Checks without a 10% improvement over the best before them after which a
+// refinement round ends.
+constexpr int kStallWindow = 100;
+
+double worst_relative(const anu_pdhg_residual& r, bool inf) {
+  double w = std::fmax(r.relative_primal, std::fmax(r.relative_dual, r.relative_gap));
+  if (inf) w = std::fmax(w, std::fmax(r.relative_primal_inf, r.relative_dual_inf));
+  return w;
+}
+
+bool stalled(const std::vector<double>& h) {
+  if (static_cast<int>(h.size()) <= kStallWindow) return false;
+  const auto split = h.end() - kStallWindow;
+  const double recent = *std::min_element(split, h.end());
+  const double before = *std::min_element(h.begin(), split);
+  return recent > 0.9 * before;
+}
 
 int32_t polish_budget(const anu_pdhg_options& o, int32_t at_iteration) {
   int32_t budget = static_cast<int32_t>(o.polish_iteration_factor * static_cast<double>(at_iteration + 1));
@@ -464,6 +492,10 @@ struct Workspace {
       y_prev, ylo;
   // FP64 island
   DevBuf<double> kty64, ktdy64, kx64, c0, lo0, hi0, q0, los, his, qs;
+  // refinement: base point, 1/Delta and Delta per case, the judged point,
+  // the round's best iterate, the scaled data the corrections are built from
+  DevBuf<double> xb, yb, inv_delta, delta, x_comb, y_comb, c0s, q0s, l0s, u0s;
+  DevBuf<T> x_best, y_best;
   DevBuf<StepParams> params;
   DevBuf<double> w_table;
   DevBuf<int32_t> mask;
@@ -738,6 +770,9 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& cases,
   const bool need_kkt_any = (o.restarts && !halpern) || (o.restarts && !o.restart_on_fixed_point) ||
                             o.verbose;
   const bool fp64 = std::is_same<T, double>::value;
+  const bool refine = !fp64 && o.refinement_rounds > 0;
+  const bool polish_on = o.polish_feasibility && !refine;
+  const double inner_tol = o.refinement_inner_tolerance > 0.0 ? o.refinement_inner_tolerance : 1e-3;
   if (slow && K != 1)
     throw Error(ANU_ERR_INVALID,
                 "adaptive step sizes and the Halpern restart test need a single case");
@@ -823,6 +858,7 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& cases,
     upload_interleaved(st, w.qs, m, K, vq);
     w.ktdy64.alloc(NK);
   }
+  if (refine) any_ylo = true;
   if (any_ylo) {
     std::vector<std::vector<double>> zeros(K);
     for (int k = 0; k < K; ++k) {
@@ -874,6 +910,27 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& cases,
   }
   w.kty64.alloc(NK);
   w.kx64.alloc(MK);
+  if (refine) {
+    w.xb.alloc(NK);
+    w.yb.alloc(MK);
+    ANU_CUDA(cudaMemsetAsync(w.xb.p, 0, sizeof(double) * NK, st));
+    ANU_CUDA(cudaMemsetAsync(w.yb.p, 0, sizeof(double) * MK, st));
+    std::vector<double> ones(K, 1.0);
+    w.inv_delta.alloc(K);
+    w.delta.alloc(K);
+    ANU_CUDA(cudaMemcpyAsync(w.inv_delta.p, ones.data(), sizeof(double) * K, cudaMemcpyHostToDevice, st));
+    ANU_CUDA(cudaMemcpyAsync(w.delta.p, ones.data(), sizeof(double) * K, cudaMemcpyHostToDevice, st));
+    w.x_comb.alloc(NK);
+    w.y_comb.alloc(MK);
+    w.x_best.alloc(NK);
+    w.y_best.alloc(MK);
+    ANU_CUDA(cudaMemcpyAsync(w.x_best.p, w.x.p, sizeof(T) * NK, cudaMemcpyDeviceToDevice, st));
+    ANU_CUDA(cudaMemcpyAsync(w.y_best.p, w.y.p, sizeof(T) * MK, cudaMemcpyDeviceToDevice, st));
+    upload_interleaved(st, w.c0s, n, K, vc);
+    upload_interleaved(st, w.q0s, m, K, vq);
+    upload_interleaved(st, w.l0s, n, K, vl);
+    upload_interleaved(st, w.u0s, n, K, vu);
+  }
   w.params.alloc(K);
   w.mask.alloc(K);
   w.terms.alloc(static_cast<size_t>(kCheckTerms) * K * 2);
@@ -888,8 +945,6 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& cases,
   Pinned<int32_t> h_mask(K);
   Pinned<double> h_weights(K);
 
-  const RowCheckTerms<T, T>* dummy = nullptr;
-  (void)dummy;
 
   // k_x = K~ x0 in FP64, rounded to T (pdhg.cpp:593).
   product<double, T, double>(p, p.dk, w.x.p, K, StoreEpi<double>{K, w.kx64.p});
@@ -1018,32 +1073,46 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& cases,
   // reused. Writes terms[case][18] at `out_dev`.
   auto check_terms = [&](const T* xv, const T* yv, const T* kx_maint, bool fresh_kx,
                          double* out_dev) {
-    const double* kxp = nullptr;
-    if (fresh_kx) {
-      product<double, T, double>(p, p.dk, xv, K, StoreEpi<double>{K, w.kx64.p});
-      kxp = w.kx64.p;
-    }
-    product<double, T, double>(p, p.dkt, yv, K, StoreEpi<double>{K, w.kty64.p});
-    if (o.detect_infeasibility)
-      product<double, T, double>(p, p.dkt, w.dy.p, K, StoreEpi<double>{K, w.ktdy64.p});
     const double* rs = unit ? nullptr : p.row_scale.p;
     const double* cs = unit ? nullptr : p.col_scale.p;
+    const T* yprev = o.pid_primal_weight ? nullptr : w.y_prev.p;
+    const T* xprev = o.pid_primal_weight ? nullptr : w.x_prev.p;
+    const double* qsc = o.detect_infeasibility ? w.qs.p : nullptr;
+    const double* ktdy = o.detect_infeasibility ? w.ktdy64.p : nullptr;
+    const double* los = o.detect_infeasibility ? w.los.p : nullptr;
+    const double* his = o.detect_infeasibility ? w.his.p : nullptr;
+    if (o.detect_infeasibility)
+      product<double, T, double>(p, p.dkt, w.dy.p, K, StoreEpi<double>{K, w.ktdy64.p});
+    if (refine) {
+      // The judged point is base + iterate / Delta, in FP64.
+      const int64_t tn = static_cast<int64_t>(n) * K, tm = static_cast<int64_t>(m) * K;
+      combine_kernel<T><<<grid_for(tn, 256, 1184), 256, 0, st>>>(tn, K, w.xb.p, xv, w.inv_delta.p, w.x_comb.p);
+      combine_kernel<T><<<grid_for(tm, 256, 1184), 256, 0, st>>>(tm, K, w.yb.p, yv, w.inv_delta.p, w.y_comb.p);
+      ANU_CUDA(cudaGetLastError());
+      p.launches += 2;
+      product<double, double, double>(p, p.dk, w.x_comb.p, K, StoreEpi<double>{K, w.kx64.p});
+      product<double, double, double>(p, p.dkt, w.y_comb.p, K, StoreEpi<double>{K, w.kty64.p});
+      RowCheckTerms<double, T, double> rt{K, p.num_eq, w.kx64.p, w.y_comb.p, yv, w.dy.p,
+                                          w.y_restart.p, yprev, w.q0.p, qsc, rs};
+      ColCheckTerms<double, T> ct{K, w.kty64.p, w.x_comb.p, xv, w.dx.p, w.x_restart.p, xprev,
+                                  w.c0.p, w.lo0.p, w.hi0.p, cs, ktdy, los, his};
+      reduce_terms(p, m, K, rt, w.partial, out_dev, kCheckTerms, 0);
+      reduce_terms(p, n, K, ct, w.partial, out_dev, kCheckTerms, kRowTerms);
+      return;
+    }
+    product<double, T, double>(p, p.dkt, yv, K, StoreEpi<double>{K, w.kty64.p});
     if (fresh_kx) {
-      RowCheckTerms<T, double> rt{K, p.num_eq, kxp, yv, w.dy.p, w.y_restart.p,
-                                  o.pid_primal_weight ? nullptr : w.y_prev.p, w.q0.p,
-                                  o.detect_infeasibility ? w.qs.p : nullptr, rs};
+      product<double, T, double>(p, p.dk, xv, K, StoreEpi<double>{K, w.kx64.p});
+      RowCheckTerms<T, T, double> rt{K, p.num_eq, w.kx64.p, yv, yv, w.dy.p, w.y_restart.p, yprev,
+                                     w.q0.p, qsc, rs};
       reduce_terms(p, m, K, rt, w.partial, out_dev, kCheckTerms, 0);
     } else {
-      RowCheckTerms<T, T> rt{K, p.num_eq, kx_maint, yv, w.dy.p, w.y_restart.p,
-                             o.pid_primal_weight ? nullptr : w.y_prev.p, w.q0.p,
-                             o.detect_infeasibility ? w.qs.p : nullptr, rs};
+      RowCheckTerms<T, T, T> rt{K, p.num_eq, kx_maint, yv, yv, w.dy.p, w.y_restart.p, yprev,
+                                w.q0.p, qsc, rs};
       reduce_terms(p, m, K, rt, w.partial, out_dev, kCheckTerms, 0);
     }
-    ColCheckTerms<T> ct{K, w.kty64.p, xv, w.dx.p, w.x_restart.p,
-                        o.pid_primal_weight ? nullptr : w.x_prev.p, w.c0.p, w.lo0.p, w.hi0.p, cs,
-                        o.detect_infeasibility ? w.ktdy64.p : nullptr,
-                        o.detect_infeasibility ? w.los.p : nullptr,
-                        o.detect_infeasibility ? w.his.p : nullptr};
+    ColCheckTerms<T, T> ct{K, w.kty64.p, xv, xv, w.dx.p, w.x_restart.p, xprev, w.c0.p, w.lo0.p,
+                           w.hi0.p, cs, ktdy, los, his};
     reduce_terms(p, n, K, ct, w.partial, out_dev, kCheckTerms, kRowTerms);
   };
 
@@ -1227,6 +1296,8 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& cases,
     ANU_CUDA(cudaStreamSynchronize(st));
 
     std::vector<int32_t> adopt_mask(K, 0);
+    std::vector<int32_t> best_mask(K, 0), refine_mask(K, 0);
+    bool any_best = false, any_refine = false;
     std::vector<anu_pdhg_residual> rr(K);
     std::vector<double> candidate_kkt(K, 0.0);
     std::vector<int> polish_cases;
@@ -1276,7 +1347,21 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& cases,
         c.active = false;
         continue;
       }
-      if (o.polish_feasibility && o.termination == ANU_TERMINATION_FULL &&
+      if (refine) {
+        const double worst = worst_relative(r, inf_norm);
+        if (worst < c.best_worst) {
+          c.best_worst = worst;
+          best_mask[k] = 1;
+          any_best = true;
+        }
+        c.history.push_back(worst);
+        const bool gained = worst <= inner_tol * c.round_start_worst;
+        if ((gained || stalled(c.history)) && c.round < o.refinement_rounds) {
+          refine_mask[k] = 1;
+          any_refine = true;
+        }
+      }
+      if (polish_on && o.termination == ANU_TERMINATION_FULL &&
           it_idx + 1 >= c.next_polish_iteration) {
         while (c.next_polish_iteration <= it_idx + 1) c.next_polish_iteration *= 2;
         const int32_t budget = polish_budget(o, it_idx);
@@ -1284,6 +1369,79 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& cases,
       }
     }
     adopt(adopt_mask);
+    if (any_best) {
+      // The round's best iterate so far, which its next round starts from.
+      set_mask(best_mask);
+      masked_copy<T, T>(p, n, K, w.mask.p, w.x.p, w.x_best.p);
+      masked_copy<T, T>(p, m, K, w.mask.p, w.y.p, w.y_best.p);
+    }
+    if (any_refine) {
+      // New rounds: the base moves to base + best / Delta, Delta becomes
+      // 1 / (worst relative KKT error there), and the correction LP -
+      // cost Delta (c~ - K~'y*), rhs Delta (q~ - K~ x*), bounds Delta (l~ - x*),
+      // Delta (u~ - x*), dual floor -Delta y* - replaces the case's data.
+      set_mask(refine_mask);
+      const int64_t tn = static_cast<int64_t>(n) * K, tm = static_cast<int64_t>(m) * K;
+      rebase_kernel<T><<<grid_for(tn, 256, 1184), 256, 0, st>>>(tn, K, w.mask.p, w.xb.p, w.x_best.p, w.inv_delta.p);
+      rebase_kernel<T><<<grid_for(tm, 256, 1184), 256, 0, st>>>(tm, K, w.mask.p, w.yb.p, w.y_best.p, w.inv_delta.p);
+      ANU_CUDA(cudaGetLastError());
+      p.launches += 2;
+      std::vector<double> hd(K), hinv(K);
+      for (int k = 0; k < K; ++k) {
+        if (refine_mask[k]) S[k].delta = std::fmin(1.0 / std::fmax(S[k].best_worst, 1e-14), 1e12);
+        hd[k] = S[k].delta;
+        hinv[k] = 1.0 / S[k].delta;
+      }
+      ANU_CUDA(cudaMemcpyAsync(w.delta.p, hd.data(), sizeof(double) * K, cudaMemcpyHostToDevice, st));
+      ANU_CUDA(cudaMemcpyAsync(w.inv_delta.p, hinv.data(), sizeof(double) * K, cudaMemcpyHostToDevice, st));
+      product<double, double, double>(p, p.dk, w.xb.p, K, StoreEpi<double>{K, w.kx64.p});
+      product<double, double, double>(p, p.dkt, w.yb.p, K, StoreEpi<double>{K, w.kty64.p});
+      refine_columns_kernel<T><<<grid_for(tn, 256, 1184), 256, 0, st>>>(
+          tn, K, w.mask.p, w.delta.p, w.c0s.p, w.l0s.p, w.u0s.p, w.xb.p, w.kty64.p, w.c.p, w.lo.p,
+          w.hi.p, o.detect_infeasibility ? w.los.p : nullptr,
+          o.detect_infeasibility ? w.his.p : nullptr, w.x.p);
+      refine_rows_kernel<T><<<grid_for(tm, 256, 1184), 256, 0, st>>>(
+          tm, K, p.num_eq, w.mask.p, w.delta.p, w.q0s.p, w.yb.p, w.kx64.p, w.q.p,
+          o.detect_infeasibility ? w.qs.p : nullptr, w.ylo.p, w.y.p);
+      ANU_CUDA(cudaGetLastError());
+      p.launches += 2;
+      product<double, T, double>(p, p.dk, w.x.p, K, StoreEpi<double>{K, w.kx64.p});
+      masked_copy<T, double>(p, m, K, w.mask.p, w.kx64.p, w.kx.p);
+      masked_copy<T, T>(p, n, K, w.mask.p, w.x.p, w.x_restart.p);
+      masked_copy<T, T>(p, m, K, w.mask.p, w.y.p, w.y_restart.p);
+      masked_copy<T, T>(p, n, K, w.mask.p, w.x.p, w.x_best.p);
+      masked_copy<T, T>(p, m, K, w.mask.p, w.y.p, w.y_best.p);
+      if (!o.pid_primal_weight) {
+        masked_copy<T, T>(p, n, K, w.mask.p, w.x.p, w.x_prev.p);
+        masked_copy<T, T>(p, m, K, w.mask.p, w.y.p, w.y_prev.p);
+      }
+      if (averaging) {
+        masked_fill<T>(p, n, K, w.mask.p, static_cast<T>(0), w.sum_x.p);
+        masked_fill<T>(p, m, K, w.mask.p, static_cast<T>(0), w.sum_y.p);
+      }
+      ANU_CUDA(cudaStreamSynchronize(st));
+      for (int k = 0; k < K; ++k) {
+        if (!refine_mask[k]) continue;
+        CaseState& c = S[k];
+        ++c.round;
+        c.round_start_worst = c.best_worst;
+        c.best_worst = INFINITY;
+        c.history.clear();
+        c.round_offset = it_idx + 1;
+        c.anchor_needs_reset = true;
+        c.halpern_k = 0;
+        c.iterations_since_restart = 0;
+        c.have_previous_restart = false;
+        c.residual_at_restart = INFINITY;
+        c.last_residual = INFINITY;
+        c.last_candidate_kkt = INFINITY;
+        c.kkt_at_restart = INFINITY;
+        c.weight_error_sum = 0.0;
+        c.weight_error_previous = 0.0;
+        c.sum_weight = 0.0;
+        ++R[k].r.refinement_rounds;
+      }
+    }
     if (!polish_cases.empty()) {
       t_checks += phase_end();
       std::vector<std::vector<double>> cur_x, cur_y, avg_x, avg_y;
@@ -1354,7 +1512,7 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& cases,
     bool any_restart = false;
     for (int k = 0; k < K; ++k) {
       CaseState& c = S[k];
-      if (!c.active) continue;
+      if (!c.active || refine_mask[k]) continue;
       const double residual = std::sqrt(std::fmax(c.movement, 0.0));
       const bool by_residual = o.restart_on_fixed_point != 0;
       if (by_residual && !std::isfinite(c.residual_at_restart)) c.residual_at_restart = residual;
@@ -1364,7 +1522,7 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& cases,
       const bool sufficient = measure <= 0.2 * at_restart;
       const bool necessary = measure <= 0.8 * at_restart && measure > previous;
       const bool too_long = static_cast<double>(c.iterations_since_restart) >=
-                            0.36 * static_cast<double>(it_idx + 1);
+                            0.36 * static_cast<double>(it_idx + 1 - c.round_offset);
       c.last_candidate_kkt = candidate_kkt[k];
       c.last_residual = residual;
       if (!(sufficient || necessary || too_long)) continue;
@@ -1441,6 +1599,21 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& cases,
   std::vector<std::vector<double>> fx, fy;
   download_all(st, w.x, n, K, &fx);
   download_all(st, w.y, m, K, &fy);
+  if (refine) {
+    // The answer is base + iterate / Delta: the passing iterate for a case
+    // that converged, the round's best iterate otherwise.
+    std::vector<std::vector<double>> bx, by, bestx, besty;
+    download_all(st, w.xb, n, K, &bx);
+    download_all(st, w.yb, m, K, &by);
+    download_all(st, w.x_best, n, K, &bestx);
+    download_all(st, w.y_best, m, K, &besty);
+    for (int k = 0; k < K; ++k) {
+      const bool use_best = S[k].status != ANU_PDHG_OPTIMAL;
+      const double inv = 1.0 / S[k].delta;
+      for (int32_t j = 0; j < n; ++j) fx[k][j] = bx[k][j] + (use_best ? bestx[k][j] : fx[k][j]) * inv;
+      for (int32_t i = 0; i < m; ++i) fy[k][i] = by[k][i] + (use_best ? besty[k][i] : fy[k][i]) * inv;
+    }
+  }
   std::vector<double> fterms;
   eval_points_terms(p, unit, K, cases, fx, fy, &fterms);
   std::vector<int> exit_polish;
@@ -1462,7 +1635,7 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& cases,
     cr.r.residual = residual_from_terms(&fterms[static_cast<size_t>(k) * kCheckTerms],
                                         &fterms[static_cast<size_t>(k) * kCheckTerms + kRowTerms],
                                         c.scales);
-    const bool worth = o.polish_feasibility && o.polish_on_exit &&
+    const bool worth = polish_on && o.polish_on_exit &&
                        o.termination == ANU_TERMINATION_FULL && c.status != ANU_PDHG_OPTIMAL &&
                        c.status != ANU_PDHG_PRIMAL_INFEASIBLE &&
                        c.status != ANU_PDHG_NUMERICAL_ERROR &&
@@ -1664,8 +1837,8 @@ void anu_pdhg_default_options(anu_pdhg_options* o) {
   o->log_frequency = 5000;
   o->stop = nullptr;
   o->precision = ANU_PRECISION_FP64;
-  o->refinement_rounds = 0;
-  o->refinement_inner_tolerance = 0.0;
+  o->refinement_rounds = 8;
+  o->refinement_inner_tolerance = 1e-3;
   o->device = 0;
   o->use_graphs = 1;
   o->profile = 0;

@@ -100,9 +100,6 @@ struct StoreEpi {
   }
 };
 
-// Two products over one matrix read: out1 = A x1 and out2 = A x2 handled by
-// running the kernel twice is simpler; kept single for clarity.
-
 // The primal side of one reflected Halpern PDHG step on column j of case k,
 // given kty = (K'y)_j (backend.hpp:89-93, backend.cpp:60-79):
 //   v = clamp(x - tau (c - kty), lower, upper); dx = v - x; x_bar = v + dx;
@@ -378,20 +375,23 @@ __global__ void terms_stage2(int32_t blocks, int32_t K, const double* __restrict
 
 // Row side of a termination check, per case (backend.cpp:143-161 and the
 // row half of pdhg.cpp:191-221), plus the squared norms the step-size rule,
-// the restart test and the primal-weight update read.
+// the restart test and the primal-weight update read. `y_pt` is the point
+// judged (FP64 when it combines a refinement base with the iterate), `y_it`
+// the iterate whose restart distances the primal weight reads.
 // Terms: 0 primal_sq, 1 primal_inf (max), 2 q_dot_y, 3 dy_sq, 4 dyr_sq
 // (|y - y_restart|^2), 5 dypr_sq (|y - y_prev_restart|^2), 6 inf_scale (max
 // |dy|), 7 inf_badcone (max of indicator), 8 inf_rhs (sum q~ dy).
-template <class T, class KX>
+template <class TP, class TI, class KX>
 struct RowCheckTerms {
   static constexpr int NT = 9;
   int32_t K;
   int32_t num_eq;
-  const KX* __restrict__ kx;       // K~ x~ (scaled)
-  const T* __restrict__ y;
-  const T* __restrict__ dy;
-  const T* __restrict__ y_restart;
-  const T* __restrict__ y_prev;
+  const KX* __restrict__ kx;       // K~ x~ (scaled) of the judged point
+  const TP* __restrict__ y_pt;
+  const TI* __restrict__ y_it;
+  const TI* __restrict__ dy;
+  const TI* __restrict__ y_restart;
+  const TI* __restrict__ y_prev;
   const double* __restrict__ q;        // original, per case
   const double* __restrict__ q_scaled; // for the Farkas test
   const double* __restrict__ row_scale;  // shared, may be null (unit)
@@ -413,16 +413,17 @@ struct RowCheckTerms {
     const double viol = (i < num_eq) ? slack : fmin(slack, 0.0);
     a[0] = anu::add(a[0], mul(viol, viol));
     a[1] = fmax(a[1], fabs(viol));
-    const double yi = static_cast<double>(y[e]);
+    const double yi = static_cast<double>(y_pt[e]);
     a[2] = anu::add(a[2], mul(qi, mul(scale, yi)));
     const double d = dy ? static_cast<double>(dy[e]) : 0.0;
     a[3] = anu::add(a[3], mul(d, d));
+    const double yit = y_it ? static_cast<double>(y_it[e]) : 0.0;
     if (y_restart) {
-      const double r = anu::sub(yi, static_cast<double>(y_restart[e]));
+      const double r = anu::sub(yit, static_cast<double>(y_restart[e]));
       a[4] = anu::add(a[4], mul(r, r));
     }
     if (y_prev) {
-      const double r = anu::sub(yi, static_cast<double>(y_prev[e]));
+      const double r = anu::sub(yit, static_cast<double>(y_prev[e]));
       a[5] = anu::add(a[5], mul(r, r));
     }
     a[6] = fmax(a[6], fabs(d));
@@ -434,15 +435,16 @@ struct RowCheckTerms {
 // Column side (backend.cpp:163-198 and the column half of the Farkas test).
 // Terms: 0 dual_sq, 1 dual_inf (max), 2 bound_term, 3 c_dot_x, 4 dx_sq,
 // 5 dxr_sq, 6 dxpr_sq, 7 inf_support, 8 inf_unbounded (max of indicator).
-template <class T>
+template <class TP, class TI>
 struct ColCheckTerms {
   static constexpr int NT = 9;
   int32_t K;
-  const double* __restrict__ kty;   // K~' y~ (scaled)
-  const T* __restrict__ x;
-  const T* __restrict__ dx;
-  const T* __restrict__ x_restart;
-  const T* __restrict__ x_prev;
+  const double* __restrict__ kty;   // K~' y~ (scaled) of the judged point
+  const TP* __restrict__ x_pt;
+  const TI* __restrict__ x_it;
+  const TI* __restrict__ dx;
+  const TI* __restrict__ x_restart;
+  const TI* __restrict__ x_prev;
   const double* __restrict__ c;      // original, per case
   const double* __restrict__ lower;  // original
   const double* __restrict__ upper;  // original
@@ -479,16 +481,17 @@ struct ColCheckTerms {
     const double absorbed = anu::sub(lambda, leftover);
     if (absorbed > 0.0) a[2] = anu::add(a[2], mul(absorbed, lo));
     else if (absorbed < 0.0) a[2] = anu::add(a[2], mul(absorbed, hi));
-    const double xj = static_cast<double>(x[e]);
+    const double xj = static_cast<double>(x_pt[e]);
     a[3] = anu::add(a[3], mul(cj, mul(scale, xj)));
     const double d = dx ? static_cast<double>(dx[e]) : 0.0;
     a[4] = anu::add(a[4], mul(d, d));
+    const double xit = x_it ? static_cast<double>(x_it[e]) : 0.0;
     if (x_restart) {
-      const double r = anu::sub(xj, static_cast<double>(x_restart[e]));
+      const double r = anu::sub(xit, static_cast<double>(x_restart[e]));
       a[5] = anu::add(a[5], mul(r, r));
     }
     if (x_prev) {
-      const double r = anu::sub(xj, static_cast<double>(x_prev[e]));
+      const double r = anu::sub(xit, static_cast<double>(x_prev[e]));
       a[6] = anu::add(a[6], mul(r, r));
     }
     if (kt_dy) {
@@ -589,6 +592,94 @@ __global__ void average_kernel(int64_t total, int32_t K, const double* __restric
        e += (int64_t)gridDim.x * blockDim.x) {
     const double w = weight[e % K];
     out[e] = static_cast<T>(static_cast<double>(sum[e]) / w);
+  }
+}
+
+// ------------------------------------------------------------ refinement
+
+// The judged point of a refinement round: base + iterate / Delta, per case
+// (FP64). In a case's first round the base is zero and 1/Delta is one, so
+// the point is the iterate itself, exactly.
+template <class T>
+__global__ void combine_kernel(int64_t total, int32_t K, const double* __restrict__ base,
+                               const T* __restrict__ it, const double* __restrict__ inv_delta,
+                               double* __restrict__ out) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    out[e] = add(base[e], mul(static_cast<double>(it[e]), inv_delta[e % K]));
+  }
+}
+
+// base += it / Delta for the masked cases: the new base point of a round.
+template <class T>
+__global__ void rebase_kernel(int64_t total, int32_t K, const int32_t* __restrict__ mask,
+                              double* __restrict__ base, const T* __restrict__ it,
+                              const double* __restrict__ inv_delta) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t k = static_cast<int32_t>(e % K);
+    if (mask[k]) base[e] = add(base[e], mul(static_cast<double>(it[e]), inv_delta[k]));
+  }
+}
+
+// A new refinement round for the masked cases, column side: the correction
+// LP's cost Delta (c~ - K~'y*), bounds Delta (l~ - x*), Delta (u~ - x*), and
+// its start: zero projected into those bounds.
+template <class T>
+__global__ void refine_columns_kernel(int64_t total, int32_t K, const int32_t* __restrict__ mask,
+                                      const double* __restrict__ delta,
+                                      const double* __restrict__ c0,
+                                      const double* __restrict__ l0,
+                                      const double* __restrict__ u0,
+                                      const double* __restrict__ xb,
+                                      const double* __restrict__ ktyb, T* __restrict__ c,
+                                      T* __restrict__ lo, T* __restrict__ hi,
+                                      double* __restrict__ lo64, double* __restrict__ hi64,
+                                      T* __restrict__ x) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t k = static_cast<int32_t>(e % K);
+    if (!mask[k]) continue;
+    const double d = delta[k];
+    const double cc = mul(d, sub(c0[e], ktyb[e]));
+    const double l = mul(d, sub(l0[e], xb[e]));
+    const double u = mul(d, sub(u0[e], xb[e]));
+    c[e] = static_cast<T>(cc);
+    lo[e] = static_cast<T>(l);
+    hi[e] = static_cast<T>(u);
+    if (lo64) lo64[e] = l;
+    if (hi64) hi64[e] = u;
+    double v = 0.0;
+    if (v < l) v = l;
+    if (v > u) v = u;
+    x[e] = static_cast<T>(v);
+  }
+}
+
+// Row side: right-hand side Delta (q~ - K~ x*), dual floor -Delta y* on the
+// inequality rows, and the start y = max(0, floor) there, 0 elsewhere.
+template <class T>
+__global__ void refine_rows_kernel(int64_t total, int32_t K, int32_t num_eq,
+                                   const int32_t* __restrict__ mask,
+                                   const double* __restrict__ delta,
+                                   const double* __restrict__ q0,
+                                   const double* __restrict__ yb,
+                                   const double* __restrict__ kxb, T* __restrict__ q,
+                                   double* __restrict__ q64, T* __restrict__ ylo,
+                                   T* __restrict__ y) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t k = static_cast<int32_t>(e % K);
+    if (!mask[k]) continue;
+    const int64_t i = e / K;
+    const double d = delta[k];
+    const double qq = mul(d, sub(q0[e], kxb[e]));
+    q[e] = static_cast<T>(qq);
+    if (q64) q64[e] = qq;
+    double floor_v = 0.0;
+    if (i >= num_eq) floor_v = -mul(d, yb[e]);
+    ylo[e] = static_cast<T>(floor_v);
+    y[e] = static_cast<T>(i >= num_eq ? fmax(0.0, floor_v) : 0.0);
   }
 }
 

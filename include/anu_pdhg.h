@@ -145,13 +145,15 @@ typedef struct anu_pdhg_options {
 
   /* --- engine additions, no counterpart in PdhgOptions --- */
   int32_t precision;            /* ANU_PRECISION_FP64 (default) or _FP32 */
-  /* Outer iterative-refinement rounds after the first solve (FP32 only).
-   * Each round re-solves a correction LP built from the FP64 residuals of the
-   * current point. 0 = none. */
-  int32_t refinement_rounds;    /* 0 */
-  /* Relative KKT tolerance of each inner solve when refining; 0 means
-   * max(tolerance, 1e-6). */
-  double refinement_inner_tolerance;
+  /* Iterative refinement, FP32 only. A refinement round ends when the
+   * worst relative KKT error (FP64) has fallen by refinement_inner_tolerance
+   * from the round's start, or has stopped improving; the next round
+   * re-centres the LP on the round's best point in FP64 and rescales it by
+   * 1/(that error), so the FP32 iterate carries only the correction. The
+   * termination test always judges the recombined FP64 point against the
+   * original LP. Feasibility polishing is off while refining. */
+  int32_t refinement_rounds;    /* 8; 0 = plain FP32 */
+  double refinement_inner_tolerance; /* 1e-3; 0 means 1e-3 */
   int32_t device;               /* CUDA device ordinal, 0 */
   int32_t use_graphs;           /* capture iteration chunks in CUDA graphs, 1 */
   /* Record CUDA events around every iteration chunk on the engine's stream
