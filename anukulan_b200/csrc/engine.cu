@@ -84,16 +84,29 @@ void DevCsr::upload(const HostCsr& a, bool with_fp32, cudaStream_t s) {
   if (!bd.empty())
     ANU_CUDA(cudaMemcpyAsync(blocks.p, bd.data(), sizeof(RowBlockDev) * bd.size(),
                              cudaMemcpyHostToDevice, s));
+  const SegmentSchedule sch = segment_schedule(a, kSegNnz, kSegPerCta, kSegRows);
+  num_ctas = static_cast<int32_t>(sch.cta_row.size()) - 1;
+  auto put = [&](DevBuf<int32_t>& d, const std::vector<int32_t>& h) {
+    d.alloc(std::max<size_t>(h.size(), 1));
+    if (!h.empty())
+      ANU_CUDA(cudaMemcpyAsync(d.p, h.data(), sizeof(int32_t) * h.size(), cudaMemcpyHostToDevice, s));
+  };
+  put(seg_begin, sch.seg_begin);
+  put(row_seg, sch.row_seg);
+  put(cta_row, sch.cta_row);
+  put(cta_seg, sch.cta_seg);
   ANU_CUDA(cudaStreamSynchronize(s));
 }
 
 template <>
 CsrView<double> DevCsr::view<double>() const {
-  return {rows, cols, start.p, index.p, v64.p, blocks.p, num_blocks};
+  return {rows, cols, start.p, index.p, v64.p, blocks.p, num_blocks,
+          seg_begin.p, row_seg.p, cta_row.p, cta_seg.p, num_ctas};
 }
 template <>
 CsrView<float> DevCsr::view<float>() const {
-  return {rows, cols, start.p, index.p, v32.p, blocks.p, num_blocks};
+  return {rows, cols, start.p, index.p, v32.p, blocks.p, num_blocks,
+          seg_begin.p, row_seg.p, cta_row.p, cta_seg.p, num_ctas};
 }
 
 Problem::~Problem() {

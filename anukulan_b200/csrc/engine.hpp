@@ -75,6 +75,8 @@ struct DevCsr {
   DevBuf<float> v32;
   DevBuf<RowBlockDev> blocks;
   int32_t num_blocks = 0;
+  DevBuf<int32_t> seg_begin, row_seg, cta_row, cta_seg;
+  int32_t num_ctas = 0;
   void upload(const HostCsr& a, bool with_fp32, cudaStream_t s);
   template <class V>
   CsrView<V> view() const;

@@ -34,6 +34,12 @@ namespace anu {
 constexpr int kThreads = 256;
 constexpr int kBlockNnz = 2048;
 constexpr int kBlockRows = 256;
+// Case-stack product: nonzeros per segment, segments per CTA, rows per CTA,
+// and the most cases one launch carries.
+constexpr int kSegNnz = 16;
+constexpr int kSegPerCta = 8;
+constexpr int kSegRows = 64;
+constexpr int kMaxCaseLanes = 64;
 
 // ------------------------------------------------------------------ math
 
@@ -65,6 +71,15 @@ struct CsrView {
   const V* __restrict__ value;
   const RowBlockDev* __restrict__ blocks;
   int32_t num_blocks;
+  // Segment schedule of the case-stack product: every row cut into
+  // segments of at most a few nonzeros (seg_begin, in nonzero order; the
+  // segments of row r are row_seg[r] .. row_seg[r+1]-1), and consecutive rows
+  // grouped so a CTA holds at most kSegPerCta segments (cta_row, cta_seg).
+  const int32_t* __restrict__ seg_begin;
+  const int32_t* __restrict__ row_seg;
+  const int32_t* __restrict__ cta_row;
+  const int32_t* __restrict__ cta_seg;
+  int32_t num_ctas;
 };
 
 // ------------------------------------------------------- per-case state
@@ -308,6 +323,79 @@ __global__ void __launch_bounds__(kThreads) cases_kernel(CsrView<V> a, const X* 
   }
 }
 
+// ------------------------------------------------------------ seg_kernel
+
+// The case-stack product in segments. A CTA owns a run of rows and their
+// segments; each group of L lanes takes one segment at a time: the group
+// loads the segment's indices and values once (one coalesced load), then
+// walks them by shuffle, so the x loads of successive nonzeros are
+// independent and overlap instead of waiting on an index load each. Lane l
+// accumulates cases l, l+L, ... The segment partial sums meet in shared
+// memory and are added per row in segment order (deterministic), and the
+// epilogue runs over (row, case) pairs of the CTA - case-contiguous, so its
+// vector traffic is coalesced.
+template <class V, class X, class Acc, class Epi, int L, int CPL>
+__global__ void __launch_bounds__(kThreads) seg_kernel(CsrView<V> a, const X* __restrict__ x,
+                                                        int32_t K, Epi epi) {
+  constexpr int kGroups = kThreads / L;
+  __shared__ Acc part[kSegPerCta][kMaxCaseLanes];
+  const int32_t cta = blockIdx.x;
+  const int32_t r0 = a.cta_row[cta];
+  const int32_t r1 = a.cta_row[cta + 1];
+  const int32_t s0 = a.cta_seg[cta];
+  const int32_t s1 = a.cta_seg[cta + 1];
+  const int group = threadIdx.x / L;
+  const int lane = threadIdx.x % L;
+  for (int32_t sb = s0; sb < s1; sb += kGroups) {
+    const int32_t sg = sb + group;
+    const bool active = sg < s1;
+    const int32_t b = active ? a.seg_begin[sg] : 0;
+    const int32_t e = active ? a.seg_begin[sg + 1] : 0;
+    Acc acc[CPL];
+#pragma unroll
+    for (int c = 0; c < CPL; ++c) acc[c] = 0;
+    // Every lane of the warp walks the warp's longest segment so the
+    // shuffles below see full participation.
+    const int32_t len = e - b;
+    const int32_t warp_len = __reduce_max_sync(0xffffffffu, static_cast<unsigned>(len));
+    for (int32_t base = 0; base < warp_len; base += L) {
+      int32_t idx = 0;
+      Acc val = 0;
+      if (base + lane < len) {
+        idx = a.index[b + base + lane];
+        val = static_cast<Acc>(a.value[b + base + lane]);
+      }
+      const int32_t cnt = min(L, warp_len - base);
+#pragma unroll 8
+      for (int t = 0; t < cnt; ++t) {
+        const int32_t col = __shfl_sync(0xffffffffu, idx, t, L);
+        const Acc v = __shfl_sync(0xffffffffu, val, t, L);
+        if (base + t < len) {
+          const X* xc = x + (size_t)col * K;
+#pragma unroll
+          for (int c = 0; c < CPL; ++c) {
+            const int32_t cs = lane + c * L;
+            if (cs < K) acc[c] = madd(acc[c], v, static_cast<Acc>(xc[cs]));
+          }
+        }
+      }
+    }
+    if (active) {
+#pragma unroll
+      for (int c = 0; c < CPL; ++c) part[sg - s0][lane + c * L] = acc[c];
+    }
+  }
+  __syncthreads();
+  const int32_t items = (r1 - r0) * K;
+  for (int32_t it = threadIdx.x; it < items; it += kThreads) {
+    const int32_t row = r0 + it / K;
+    const int32_t k = it % K;
+    Acc sum = 0;
+    for (int32_t sg = a.row_seg[row]; sg < a.row_seg[row + 1]; ++sg) sum = add(sum, part[sg - s0][k]);
+    epi(row, k, sum);
+  }
+}
+
 // ------------------------------------------------------- term reductions
 
 // Stage 1 of a per-case reduction over `len` rows (or columns): groups of L
@@ -356,19 +444,24 @@ __global__ void __launch_bounds__(kThreads) terms_stage1(int32_t len, int32_t K,
   }
 }
 
-// Stage 2: out[case*stride + offset + term] = fixed-order combination of the
-// blocks' partials.
+// Stage 2: out[case*stride + offset + term] = the blocks' partials combined
+// by one warp per (case, term): lane l folds blocks l, l+32, ... in order,
+// then a fixed shuffle tree - the same order on every run.
 template <class Terms>
 __global__ void terms_stage2(int32_t blocks, int32_t K, const double* __restrict__ partial,
                              double* __restrict__ out, int32_t stride, int32_t offset) {
   constexpr int NT = Terms::NT;
-  const int32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= K * NT) return;
-  const int32_t k = idx / NT;
-  const int q = idx % NT;
+  const int32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) / 32;
+  const int lane = threadIdx.x % 32;
+  if (warp >= K * NT) return;
+  const int32_t k = warp / NT;
+  const int q = warp % NT;
   double acc = Terms::identity(q);
-  for (int32_t b = 0; b < blocks; ++b) acc = Terms::combine(q, acc, partial[((size_t)b * K + k) * NT + q]);
-  out[(size_t)k * stride + offset + q] = acc;
+  for (int32_t b = lane; b < blocks; b += 32)
+    acc = Terms::combine(q, acc, partial[((size_t)b * K + k) * NT + q]);
+  for (int off = 16; off > 0; off >>= 1)
+    acc = Terms::combine(q, acc, __shfl_down_sync(0xffffffffu, acc, off));
+  if (lane == 0) out[(size_t)k * stride + offset + q] = acc;
 }
 
 // ------------------------------------------------------------ check terms

@@ -37,8 +37,8 @@ void product(Exec& p, const Mat& a, const X* x, int K, const Epi& epi) {
     rows_kernel<V, X, Acc, Epi><<<a.num_blocks, kThreads, 0, s>>>(a.template view<V>(), x, epi);
   } else {
 #define ANU_CASES(L_, CPL_)                                                                  \
-  cases_kernel<V, X, Acc, Epi, L_, CPL_>                                                     \
-      <<<grid_for(a.rows, kThreads / L_, 148 * 16), kThreads, 0, s>>>(a.template view<V>(), x, K, epi)
+  seg_kernel<V, X, Acc, Epi, L_, CPL_>                                                       \
+      <<<a.num_ctas, kThreads, 0, s>>>(a.template view<V>(), x, K, epi)
     if (K <= 4) ANU_CASES(4, 1);
     else if (K <= 8) ANU_CASES(8, 1);
     else if (K <= 16) ANU_CASES(16, 1);
@@ -73,8 +73,8 @@ void reduce_terms(Exec& p, int32_t len, int K, const Terms& t, Buf& partial,
   else ANU_TERMS(32, 2);
 #undef ANU_TERMS
   cuda_check(cudaGetLastError(), "kernel launch");
-  terms_stage2<Terms><<<(K * NT + 127) / 128, 128, 0, s>>>(blocks, K, partial.p, out, stride,
-                                                            offset);
+  terms_stage2<Terms><<<(K * NT * 32 + 255) / 256, 256, 0, s>>>(blocks, K, partial.p, out,
+                                                                 stride, offset);
   cuda_check(cudaGetLastError(), "kernel launch");
   p.launches += 2;
 }

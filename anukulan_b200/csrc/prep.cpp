@@ -185,4 +185,36 @@ std::vector<RowBlock> row_blocks(const HostCsr& a, int32_t block_nnz, int32_t bl
   return blocks;
 }
 
+SegmentSchedule segment_schedule(const HostCsr& a, int32_t seg_nnz, int32_t seg_per_cta,
+                                 int32_t row_max) {
+  SegmentSchedule s;
+  s.row_seg.assign(static_cast<size_t>(a.rows) + 1, 0);
+  for (int32_t r = 0; r < a.rows; ++r) {
+    const int32_t b = a.start[r], e = a.start[r + 1];
+    const int32_t len = e - b;
+    int32_t step = seg_nnz;
+    if (len > seg_nnz * seg_per_cta) step = (len + seg_per_cta - 1) / seg_per_cta;
+    s.row_seg[r] = static_cast<int32_t>(s.seg_begin.size());
+    for (int32_t k = b; k < e; k += step) s.seg_begin.push_back(k);
+  }
+  s.row_seg[a.rows] = static_cast<int32_t>(s.seg_begin.size());
+  s.seg_begin.push_back(a.nnz());
+  s.cta_row.push_back(0);
+  s.cta_seg.push_back(0);
+  int32_t r = 0;
+  while (r < a.rows) {
+    const int32_t r0 = r;
+    int32_t count = 0;
+    while (r < a.rows && r - r0 < row_max) {
+      const int32_t c = s.row_seg[r + 1] - s.row_seg[r];
+      if (count + c > seg_per_cta && r > r0) break;
+      count += c;
+      ++r;
+    }
+    s.cta_row.push_back(r);
+    s.cta_seg.push_back(s.row_seg[r]);
+  }
+  return s;
+}
+
 }  // namespace anu

@@ -68,6 +68,19 @@ struct RowBlock {
 };
 std::vector<RowBlock> row_blocks(const HostCsr& a, int32_t block_nnz, int32_t block_rows);
 
+// Segment schedule of the case-stack product (see seg_kernel): every row
+// cut into segments of at most seg_nnz nonzeros (a longer row into
+// seg_per_cta equal segments), and consecutive rows grouped into CTAs of at
+// most seg_per_cta segments and row_max rows.
+struct SegmentSchedule {
+  std::vector<int32_t> seg_begin;  // segments + 1
+  std::vector<int32_t> row_seg;    // rows + 1
+  std::vector<int32_t> cta_row;    // ctas + 1
+  std::vector<int32_t> cta_seg;    // ctas + 1
+};
+SegmentSchedule segment_schedule(const HostCsr& a, int32_t seg_nnz, int32_t seg_per_cta,
+                                 int32_t row_max);
+
 double now_seconds();
 
 }  // namespace anu
