@@ -57,8 +57,7 @@ class anu_pdhg_options(C.Structure):
         ("termination", i32), ("known_matrix_norm", f64), ("initial_step_size", f64),
         ("initial_primal_weight", f64), ("verbose", i32), ("log_frequency", i32),
         ("stop", C.POINTER(i32)),
-        ("precision", i32), ("refinement_rounds", i32),
-        ("refinement_inner_tolerance", f64), ("device", i32), ("use_graphs", i32),
+        ("precision", i32), ("refinement", i32), ("device", i32), ("use_graphs", i32),
         ("profile", i32),
     ]
 
@@ -104,8 +103,8 @@ DEFAULTS = dict(
     primal_weight_kd=0.3, ruiz_iterations=10, pock_chambolle=1, reuse_products=1,
     detect_infeasibility=1, infeasibility_tolerance=1e-8, termination=0,
     known_matrix_norm=0.0, initial_step_size=0.0, initial_primal_weight=0.0,
-    verbose=0, log_frequency=5000, precision=0, refinement_rounds=8,
-    refinement_inner_tolerance=1e-3, device=0, use_graphs=1, profile=0,
+    verbose=0, log_frequency=5000, precision=0, refinement=1,
+    device=0, use_graphs=1, profile=0,
 )
 
 

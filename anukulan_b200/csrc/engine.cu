@@ -451,34 +451,12 @@ struct CaseState {
   std::vector<double> polished_x, polished_y;
   anu_pdhg_residual polished_residual{};
   ResidualScales scales{};
-  // Iterative refinement (FP32): the round, the worst relative KKT error the
-  // round started from and the best one it has reached, the history of
-  // checks in the round, the iteration it started at, and its Delta.
-  int32_t round = 0;
-  double round_start_worst = 1.0;
-  double best_worst = INFINITY;
-  std::vector<double> history;
-  int32_t round_offset = 0;
-  double delta = 1.0;
-  bool final_from_best = false;
 };
-
-// Checks without a 10% improvement over the best before them after which a
-// refinement round ends.
-constexpr int kStallWindow = 100;
 
 double worst_relative(const anu_pdhg_residual& r, bool inf) {
   double w = std::fmax(r.relative_primal, std::fmax(r.relative_dual, r.relative_gap));
   if (inf) w = std::fmax(w, std::fmax(r.relative_primal_inf, r.relative_dual_inf));
   return w;
-}
-
-bool stalled(const std::vector<double>& h) {
-  if (static_cast<int>(h.size()) <= kStallWindow) return false;
-  const auto split = h.end() - kStallWindow;
-  const double recent = *std::min_element(split, h.end());
-  const double before = *std::min_element(h.begin(), split);
-  return recent > 0.9 * before;
 }
 
 int32_t polish_budget(const anu_pdhg_options& o, int32_t at_iteration) {
@@ -505,10 +483,10 @@ struct Workspace {
       y_prev, ylo;
   // FP64 island
   DevBuf<double> kty64, ktdy64, kx64, c0, lo0, hi0, q0, los, his, qs;
-  // refinement: base point, 1/Delta and Delta per case, the judged point,
-  // the round's best iterate, the scaled data the corrections are built from
-  DevBuf<double> xb, yb, inv_delta, delta, x_comb, y_comb, c0s, q0s, l0s, u0s;
-  DevBuf<T> x_best, y_best;
+  // refinement: the FP64 base point, the judged point (base + offset), the
+  // scaled data the correction LPs are formed from, K times a column shift,
+  // and the averaged scheme's running weight per case
+  DevBuf<double> xb, yb, x_comb, y_comb, c0s, q0s, l0s, u0s, kshift, sum_weight;
   DevBuf<StepParams> params;
   DevBuf<double> w_table;
   DevBuf<int32_t> mask;
@@ -783,9 +761,8 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& cases,
   const bool need_kkt_any = (o.restarts && !halpern) || (o.restarts && !o.restart_on_fixed_point) ||
                             o.verbose;
   const bool fp64 = std::is_same<T, double>::value;
-  const bool refine = !fp64 && o.refinement_rounds > 0;
-  const bool polish_on = o.polish_feasibility && !refine;
-  const double inner_tol = o.refinement_inner_tolerance > 0.0 ? o.refinement_inner_tolerance : 1e-3;
+  const bool refine = !fp64 && o.refinement != 0;
+  const bool polish_on = o.polish_feasibility != 0;
   if (slow && K != 1)
     throw Error(ANU_ERR_INVALID,
                 "adaptive step sizes and the Halpern restart test need a single case");
@@ -928,17 +905,10 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& cases,
     w.yb.alloc(MK);
     ANU_CUDA(cudaMemsetAsync(w.xb.p, 0, sizeof(double) * NK, st));
     ANU_CUDA(cudaMemsetAsync(w.yb.p, 0, sizeof(double) * MK, st));
-    std::vector<double> ones(K, 1.0);
-    w.inv_delta.alloc(K);
-    w.delta.alloc(K);
-    ANU_CUDA(cudaMemcpyAsync(w.inv_delta.p, ones.data(), sizeof(double) * K, cudaMemcpyHostToDevice, st));
-    ANU_CUDA(cudaMemcpyAsync(w.delta.p, ones.data(), sizeof(double) * K, cudaMemcpyHostToDevice, st));
     w.x_comb.alloc(NK);
     w.y_comb.alloc(MK);
-    w.x_best.alloc(NK);
-    w.y_best.alloc(MK);
-    ANU_CUDA(cudaMemcpyAsync(w.x_best.p, w.x.p, sizeof(T) * NK, cudaMemcpyDeviceToDevice, st));
-    ANU_CUDA(cudaMemcpyAsync(w.y_best.p, w.y.p, sizeof(T) * MK, cudaMemcpyDeviceToDevice, st));
+    w.kshift.alloc(MK);
+    w.sum_weight.alloc(K);
     upload_interleaved(st, w.c0s, n, K, vc);
     upload_interleaved(st, w.q0s, m, K, vq);
     upload_interleaved(st, w.l0s, n, K, vl);
@@ -1097,10 +1067,10 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& cases,
     if (o.detect_infeasibility)
       product<double, T, double>(p, p.dkt, w.dy.p, K, StoreEpi<double>{K, w.ktdy64.p});
     if (refine) {
-      // The judged point is base + iterate / Delta, in FP64.
+      // The judged point is base + offset, in FP64.
       const int64_t tn = static_cast<int64_t>(n) * K, tm = static_cast<int64_t>(m) * K;
-      combine_kernel<T><<<grid_for(tn, 256, 1184), 256, 0, st>>>(tn, K, w.xb.p, xv, w.inv_delta.p, w.x_comb.p);
-      combine_kernel<T><<<grid_for(tm, 256, 1184), 256, 0, st>>>(tm, K, w.yb.p, yv, w.inv_delta.p, w.y_comb.p);
+      combine_kernel<T><<<grid_for(tn, 256, 1184), 256, 0, st>>>(tn, w.xb.p, xv, w.x_comb.p);
+      combine_kernel<T><<<grid_for(tm, 256, 1184), 256, 0, st>>>(tm, w.yb.p, yv, w.y_comb.p);
       ANU_CUDA(cudaGetLastError());
       p.launches += 2;
       product<double, double, double>(p, p.dk, w.x_comb.p, K, StoreEpi<double>{K, w.kx64.p});
@@ -1130,6 +1100,8 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& cases,
   };
 
   auto set_mask = [&](const std::vector<int32_t>& mk) {
+    // The pinned staging buffer may still feed an earlier copy.
+    ANU_CUDA(cudaStreamSynchronize(st));
     for (int k = 0; k < K; ++k) h_mask.p[k] = mk[k];
     ANU_CUDA(cudaMemcpyAsync(w.mask.p, h_mask.p, sizeof(int32_t) * K, cudaMemcpyHostToDevice, st));
   };
@@ -1143,6 +1115,50 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& cases,
     masked_copy<T, T>(p, n, K, w.mask.p, w.avg_x.p, w.x.p);
     masked_copy<T, T>(p, m, K, w.mask.p, w.avg_y.p, w.y.p);
     ANU_CUDA(cudaStreamSynchronize(st));
+  };
+
+  std::vector<CaseResult>* R_ptr = results;
+  // Refinement at a check: fold every active case's FP32 offset into its FP64
+  // base and re-form the correction LP from the FP64 residual there.
+  auto recenter = [&]() {
+    if (!refine) return;
+    std::vector<int32_t> mk(K, 0);
+    bool any = false;
+    for (int k = 0; k < K; ++k)
+      if (S[k].active) {
+        mk[k] = 1;
+        any = true;
+      }
+    if (!any) return;
+    set_mask(mk);
+    if (averaging) {
+      for (int k = 0; k < K; ++k) h_weights.p[k] = S[k].sum_weight;
+      ANU_CUDA(cudaMemcpyAsync(w.sum_weight.p, h_weights.p, sizeof(double) * K, cudaMemcpyHostToDevice, st));
+    }
+    const bool det = o.detect_infeasibility != 0;
+    const int64_t tn = static_cast<int64_t>(n) * K, tm = static_cast<int64_t>(m) * K;
+    ANU_CUDA(cudaMemsetAsync(w.x_comb.p, 0, sizeof(double) * NK, st));
+    recenter_columns_kernel<T><<<grid_for(tn, 256, 1184), 256, 0, st>>>(
+        tn, K, w.mask.p, w.l0s.p, w.u0s.p, w.xb.p, w.x.p, w.anchor_x.p, w.x_restart.p,
+        o.pid_primal_weight ? nullptr : w.x_prev.p, averaging ? w.sum_x.p : nullptr,
+        w.sum_weight.p, w.lo.p, w.hi.p, det ? w.los.p : nullptr, det ? w.his.p : nullptr,
+        w.x_comb.p);
+    ANU_CUDA(cudaGetLastError());
+    product<double, double, double>(p, p.dk, w.x_comb.p, K, StoreEpi<double>{K, w.kshift.p});
+    recenter_rows_kernel<T><<<grid_for(tm, 256, 1184), 256, 0, st>>>(
+        tm, K, p.num_eq, w.mask.p, w.yb.p, w.y.p, w.anchor_y.p, w.y_restart.p,
+        o.pid_primal_weight ? nullptr : w.y_prev.p, averaging ? w.sum_y.p : nullptr,
+        w.sum_weight.p, w.ylo.p, w.kx.p, w.anchor_kx.p, w.kshift.p);
+    ANU_CUDA(cudaGetLastError());
+    product<double, double, double>(p, p.dk, w.xb.p, K, StoreEpi<double>{K, w.kx64.p});
+    product<double, double, double>(p, p.dkt, w.yb.p, K, StoreEpi<double>{K, w.kty64.p});
+    correction_data_kernel<T><<<grid_for(tn + tm, 256, 1184), 256, 0, st>>>(
+        tn, tm, K, w.mask.p, w.c0s.p, w.kty64.p, w.c.p, w.q0s.p, w.kx64.p, w.q.p,
+        det ? w.qs.p : nullptr);
+    ANU_CUDA(cudaGetLastError());
+    p.launches += 3;
+    for (int k = 0; k < K; ++k)
+      if (mk[k]) ++R_ptr->at(k).r.refinement_rounds;
   };
 
   int32_t iteration = 0;
@@ -1309,8 +1325,6 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& cases,
     ANU_CUDA(cudaStreamSynchronize(st));
 
     std::vector<int32_t> adopt_mask(K, 0);
-    std::vector<int32_t> best_mask(K, 0), refine_mask(K, 0);
-    bool any_best = false, any_refine = false;
     std::vector<anu_pdhg_residual> rr(K);
     std::vector<double> candidate_kkt(K, 0.0);
     std::vector<int> polish_cases;
@@ -1360,20 +1374,6 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& cases,
         c.active = false;
         continue;
       }
-      if (refine) {
-        const double worst = worst_relative(r, inf_norm);
-        if (worst < c.best_worst) {
-          c.best_worst = worst;
-          best_mask[k] = 1;
-          any_best = true;
-        }
-        c.history.push_back(worst);
-        const bool gained = worst <= inner_tol * c.round_start_worst;
-        if ((gained || stalled(c.history)) && c.round < o.refinement_rounds) {
-          refine_mask[k] = 1;
-          any_refine = true;
-        }
-      }
       if (polish_on && o.termination == ANU_TERMINATION_FULL &&
           it_idx + 1 >= c.next_polish_iteration) {
         while (c.next_polish_iteration <= it_idx + 1) c.next_polish_iteration *= 2;
@@ -1382,87 +1382,29 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& cases,
       }
     }
     adopt(adopt_mask);
-    if (any_best) {
-      // The round's best iterate so far, which its next round starts from.
-      set_mask(best_mask);
-      masked_copy<T, T>(p, n, K, w.mask.p, w.x.p, w.x_best.p);
-      masked_copy<T, T>(p, m, K, w.mask.p, w.y.p, w.y_best.p);
-    }
-    if (any_refine) {
-      // New rounds: the base moves to base + best / Delta, Delta becomes
-      // 1 / (worst relative KKT error there), and the correction LP -
-      // cost Delta (c~ - K~'y*), rhs Delta (q~ - K~ x*), bounds Delta (l~ - x*),
-      // Delta (u~ - x*), dual floor -Delta y* - replaces the case's data.
-      set_mask(refine_mask);
-      const int64_t tn = static_cast<int64_t>(n) * K, tm = static_cast<int64_t>(m) * K;
-      rebase_kernel<T><<<grid_for(tn, 256, 1184), 256, 0, st>>>(tn, K, w.mask.p, w.xb.p, w.x_best.p, w.inv_delta.p);
-      rebase_kernel<T><<<grid_for(tm, 256, 1184), 256, 0, st>>>(tm, K, w.mask.p, w.yb.p, w.y_best.p, w.inv_delta.p);
-      ANU_CUDA(cudaGetLastError());
-      p.launches += 2;
-      std::vector<double> hd(K), hinv(K);
-      for (int k = 0; k < K; ++k) {
-        if (refine_mask[k]) S[k].delta = std::fmin(1.0 / std::fmax(S[k].best_worst, 1e-14), 1e12);
-        hd[k] = S[k].delta;
-        hinv[k] = 1.0 / S[k].delta;
-      }
-      ANU_CUDA(cudaMemcpyAsync(w.delta.p, hd.data(), sizeof(double) * K, cudaMemcpyHostToDevice, st));
-      ANU_CUDA(cudaMemcpyAsync(w.inv_delta.p, hinv.data(), sizeof(double) * K, cudaMemcpyHostToDevice, st));
-      product<double, double, double>(p, p.dk, w.xb.p, K, StoreEpi<double>{K, w.kx64.p});
-      product<double, double, double>(p, p.dkt, w.yb.p, K, StoreEpi<double>{K, w.kty64.p});
-      refine_columns_kernel<T><<<grid_for(tn, 256, 1184), 256, 0, st>>>(
-          tn, K, w.mask.p, w.delta.p, w.c0s.p, w.l0s.p, w.u0s.p, w.xb.p, w.kty64.p, w.c.p, w.lo.p,
-          w.hi.p, o.detect_infeasibility ? w.los.p : nullptr,
-          o.detect_infeasibility ? w.his.p : nullptr, w.x.p);
-      refine_rows_kernel<T><<<grid_for(tm, 256, 1184), 256, 0, st>>>(
-          tm, K, p.num_eq, w.mask.p, w.delta.p, w.q0s.p, w.yb.p, w.kx64.p, w.q.p,
-          o.detect_infeasibility ? w.qs.p : nullptr, w.ylo.p, w.y.p);
-      ANU_CUDA(cudaGetLastError());
-      p.launches += 2;
-      product<double, T, double>(p, p.dk, w.x.p, K, StoreEpi<double>{K, w.kx64.p});
-      masked_copy<T, double>(p, m, K, w.mask.p, w.kx64.p, w.kx.p);
-      masked_copy<T, T>(p, n, K, w.mask.p, w.x.p, w.x_restart.p);
-      masked_copy<T, T>(p, m, K, w.mask.p, w.y.p, w.y_restart.p);
-      masked_copy<T, T>(p, n, K, w.mask.p, w.x.p, w.x_best.p);
-      masked_copy<T, T>(p, m, K, w.mask.p, w.y.p, w.y_best.p);
-      if (!o.pid_primal_weight) {
-        masked_copy<T, T>(p, n, K, w.mask.p, w.x.p, w.x_prev.p);
-        masked_copy<T, T>(p, m, K, w.mask.p, w.y.p, w.y_prev.p);
-      }
-      if (averaging) {
-        masked_fill<T>(p, n, K, w.mask.p, static_cast<T>(0), w.sum_x.p);
-        masked_fill<T>(p, m, K, w.mask.p, static_cast<T>(0), w.sum_y.p);
-      }
-      ANU_CUDA(cudaStreamSynchronize(st));
-      for (int k = 0; k < K; ++k) {
-        if (!refine_mask[k]) continue;
-        CaseState& c = S[k];
-        ++c.round;
-        c.round_start_worst = c.best_worst;
-        c.best_worst = INFINITY;
-        c.history.clear();
-        c.round_offset = it_idx + 1;
-        c.anchor_needs_reset = true;
-        c.halpern_k = 0;
-        c.iterations_since_restart = 0;
-        c.have_previous_restart = false;
-        c.residual_at_restart = INFINITY;
-        c.last_residual = INFINITY;
-        c.last_candidate_kkt = INFINITY;
-        c.kkt_at_restart = INFINITY;
-        c.weight_error_sum = 0.0;
-        c.weight_error_previous = 0.0;
-        c.sum_weight = 0.0;
-        ++R[k].r.refinement_rounds;
-      }
-    }
     if (!polish_cases.empty()) {
       t_checks += phase_end();
-      std::vector<std::vector<double>> cur_x, cur_y, avg_x, avg_y;
+      std::vector<std::vector<double>> cur_x, cur_y, avg_x, avg_y, bx, by;
       download_all(st, w.x, n, K, &cur_x);
       download_all(st, w.y, m, K, &cur_y);
       if (any_avg) {
         download_all(st, w.avg_x, n, K, &avg_x);
         download_all(st, w.avg_y, m, K, &avg_y);
+      }
+      if (refine) {
+        // Seeds are points of the scaled LP: base + offset.
+        download_all(st, w.xb, n, K, &bx);
+        download_all(st, w.yb, m, K, &by);
+        for (int k = 0; k < K; ++k) {
+          for (int32_t j = 0; j < n; ++j) {
+            cur_x[k][j] += bx[k][j];
+            if (any_avg) avg_x[k][j] += bx[k][j];
+          }
+          for (int32_t i = 0; i < m; ++i) {
+            cur_y[k][i] += by[k][i];
+            if (any_avg) avg_y[k][i] += by[k][i];
+          }
+        }
       }
       std::vector<std::vector<double>> sx, sy;
       for (int k : polish_cases) {
@@ -1517,15 +1459,11 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& cases,
       t_checks += phase_end();
       break;
     }
-    if (!o.restarts) {
-      t_checks += phase_end();
-      continue;
-    }
     std::vector<int32_t> restart_mask(K, 0);
     bool any_restart = false;
-    for (int k = 0; k < K; ++k) {
+    for (int k = 0; k < K && o.restarts; ++k) {
       CaseState& c = S[k];
-      if (!c.active || refine_mask[k]) continue;
+      if (!c.active) continue;
       const double residual = std::sqrt(std::fmax(c.movement, 0.0));
       const bool by_residual = o.restart_on_fixed_point != 0;
       if (by_residual && !std::isfinite(c.residual_at_restart)) c.residual_at_restart = residual;
@@ -1535,7 +1473,7 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& cases,
       const bool sufficient = measure <= 0.2 * at_restart;
       const bool necessary = measure <= 0.8 * at_restart && measure > previous;
       const bool too_long = static_cast<double>(c.iterations_since_restart) >=
-                            0.36 * static_cast<double>(it_idx + 1 - c.round_offset);
+                            0.36 * static_cast<double>(it_idx + 1);
       c.last_candidate_kkt = candidate_kkt[k];
       c.last_residual = residual;
       if (!(sufficient || necessary || too_long)) continue;
@@ -1600,6 +1538,7 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& cases,
       }
       ANU_CUDA(cudaStreamSynchronize(st));
     }
+    recenter();
     t_checks += phase_end();
   }
   for (int k = 0; k < K; ++k)
@@ -1613,18 +1552,13 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& cases,
   download_all(st, w.x, n, K, &fx);
   download_all(st, w.y, m, K, &fy);
   if (refine) {
-    // The answer is base + iterate / Delta: the passing iterate for a case
-    // that converged, the round's best iterate otherwise.
-    std::vector<std::vector<double>> bx, by, bestx, besty;
+    // The answer is base + offset.
+    std::vector<std::vector<double>> bx, by;
     download_all(st, w.xb, n, K, &bx);
     download_all(st, w.yb, m, K, &by);
-    download_all(st, w.x_best, n, K, &bestx);
-    download_all(st, w.y_best, m, K, &besty);
     for (int k = 0; k < K; ++k) {
-      const bool use_best = S[k].status != ANU_PDHG_OPTIMAL;
-      const double inv = 1.0 / S[k].delta;
-      for (int32_t j = 0; j < n; ++j) fx[k][j] = bx[k][j] + (use_best ? bestx[k][j] : fx[k][j]) * inv;
-      for (int32_t i = 0; i < m; ++i) fy[k][i] = by[k][i] + (use_best ? besty[k][i] : fy[k][i]) * inv;
+      for (int32_t j = 0; j < n; ++j) fx[k][j] += bx[k][j];
+      for (int32_t i = 0; i < m; ++i) fy[k][i] += by[k][i];
     }
   }
   std::vector<double> fterms;
@@ -1850,8 +1784,7 @@ void anu_pdhg_default_options(anu_pdhg_options* o) {
   o->log_frequency = 5000;
   o->stop = nullptr;
   o->precision = ANU_PRECISION_FP64;
-  o->refinement_rounds = 8;
-  o->refinement_inner_tolerance = 1e-3;
+  o->refinement = 1;
   o->device = 0;
   o->use_graphs = 1;
   o->profile = 0;

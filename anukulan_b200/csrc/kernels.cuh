@@ -689,90 +689,123 @@ __global__ void average_kernel(int64_t total, int32_t K, const double* __restric
 }
 
 // ------------------------------------------------------------ refinement
+//
+// FP32 iterates are offsets from an FP64 base point, x = x* + x^, y = y* + y^.
+// PDHG's step, projection, reflection and Halpern blend all commute with a
+// shift of origin, so running the iteration on the offsets of the LP
+//   min (c - K'y*)' x^  s.t.  K x^ (=,>=) q - K x*,  l - x* <= x^ <= u - x*,
+//   dual floor -y* on the inequality rows
+// follows the same trajectory; re-forming that correction LP from the FP64
+// residual at every check and folding the offset into the base keeps the FP32
+// numbers as small as the movement since the last check, so their rounding
+// no longer floors the accuracy.
 
-// The judged point of a refinement round: base + iterate / Delta, per case
-// (FP64). In a case's first round the base is zero and 1/Delta is one, so
-// the point is the iterate itself, exactly.
+// The judged point: base + offset, in FP64.
 template <class T>
-__global__ void combine_kernel(int64_t total, int32_t K, const double* __restrict__ base,
-                               const T* __restrict__ it, const double* __restrict__ inv_delta,
-                               double* __restrict__ out) {
+__global__ void combine_kernel(int64_t total, const double* __restrict__ base,
+                               const T* __restrict__ it, double* __restrict__ out) {
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
-       e += (int64_t)gridDim.x * blockDim.x) {
-    out[e] = add(base[e], mul(static_cast<double>(it[e]), inv_delta[e % K]));
-  }
+       e += (int64_t)gridDim.x * blockDim.x)
+    out[e] = add(base[e], static_cast<double>(it[e]));
 }
 
-// base += it / Delta for the masked cases: the new base point of a round.
+// Column side of a re-centring, for the masked cases: the offset moves into
+// the base (kept inside the bounds), every column vector of the iteration
+// state is shifted by it, the offset restarts at zero and the bounds follow
+// the base. sum_weight is the averaged scheme's running weight per case;
+// shift_out receives the column shift for the K x bookkeeping. Masked-out
+// cases leave shift_out untouched, so it must start at zero for them.
 template <class T>
-__global__ void rebase_kernel(int64_t total, int32_t K, const int32_t* __restrict__ mask,
-                              double* __restrict__ base, const T* __restrict__ it,
-                              const double* __restrict__ inv_delta) {
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
-       e += (int64_t)gridDim.x * blockDim.x) {
-    const int32_t k = static_cast<int32_t>(e % K);
-    if (mask[k]) base[e] = add(base[e], mul(static_cast<double>(it[e]), inv_delta[k]));
-  }
-}
-
-// A new refinement round for the masked cases, column side: the correction
-// LP's cost Delta (c~ - K~'y*), bounds Delta (l~ - x*), Delta (u~ - x*), and
-// its start: zero projected into those bounds.
-template <class T>
-__global__ void refine_columns_kernel(int64_t total, int32_t K, const int32_t* __restrict__ mask,
-                                      const double* __restrict__ delta,
-                                      const double* __restrict__ c0,
-                                      const double* __restrict__ l0,
-                                      const double* __restrict__ u0,
-                                      const double* __restrict__ xb,
-                                      const double* __restrict__ ktyb, T* __restrict__ c,
-                                      T* __restrict__ lo, T* __restrict__ hi,
-                                      double* __restrict__ lo64, double* __restrict__ hi64,
-                                      T* __restrict__ x) {
+__global__ void recenter_columns_kernel(int64_t total, int32_t K, const int32_t* __restrict__ mask,
+                                        const double* __restrict__ l0,
+                                        const double* __restrict__ u0, double* __restrict__ xb,
+                                        T* __restrict__ x, T* __restrict__ anchor,
+                                        T* __restrict__ restart, T* __restrict__ prev,
+                                        T* __restrict__ sum, const double* __restrict__ sum_weight,
+                                        T* __restrict__ lo, T* __restrict__ hi,
+                                        double* __restrict__ lo64, double* __restrict__ hi64,
+                                        double* __restrict__ shift_out) {
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
        e += (int64_t)gridDim.x * blockDim.x) {
     const int32_t k = static_cast<int32_t>(e % K);
     if (!mask[k]) continue;
-    const double d = delta[k];
-    const double cc = mul(d, sub(c0[e], ktyb[e]));
-    const double l = mul(d, sub(l0[e], xb[e]));
-    const double u = mul(d, sub(u0[e], xb[e]));
-    c[e] = static_cast<T>(cc);
-    lo[e] = static_cast<T>(l);
-    hi[e] = static_cast<T>(u);
-    if (lo64) lo64[e] = l;
-    if (hi64) hi64[e] = u;
-    double v = 0.0;
-    if (v < l) v = l;
-    if (v > u) v = u;
-    x[e] = static_cast<T>(v);
+    const double off = static_cast<double>(x[e]);
+    double base = add(xb[e], off);
+    const double l = l0[e], u = u0[e];
+    if (base < l) base = l;
+    if (base > u) base = u;
+    const double shift = sub(base, xb[e]);
+    shift_out[e] = shift;
+    xb[e] = base;
+    x[e] = static_cast<T>(sub(off, shift));
+    anchor[e] = static_cast<T>(sub(static_cast<double>(anchor[e]), shift));
+    restart[e] = static_cast<T>(sub(static_cast<double>(restart[e]), shift));
+    if (prev) prev[e] = static_cast<T>(sub(static_cast<double>(prev[e]), shift));
+    if (sum) sum[e] = static_cast<T>(sub(static_cast<double>(sum[e]), mul(sum_weight[k], shift)));
+    const double lo_new = sub(l, base);
+    const double hi_new = sub(u, base);
+    lo[e] = static_cast<T>(lo_new);
+    hi[e] = static_cast<T>(hi_new);
+    if (lo64) lo64[e] = lo_new;
+    if (hi64) hi64[e] = hi_new;
   }
 }
 
-// Row side: right-hand side Delta (q~ - K~ x*), dual floor -Delta y* on the
-// inequality rows, and the start y = max(0, floor) there, 0 elsewhere.
+// Row side: the same for y (kept in the cone on inequality rows), the dual
+// floor -y*, and K x, whose shift is K times the column shift (kshift).
 template <class T>
-__global__ void refine_rows_kernel(int64_t total, int32_t K, int32_t num_eq,
-                                   const int32_t* __restrict__ mask,
-                                   const double* __restrict__ delta,
-                                   const double* __restrict__ q0,
-                                   const double* __restrict__ yb,
-                                   const double* __restrict__ kxb, T* __restrict__ q,
-                                   double* __restrict__ q64, T* __restrict__ ylo,
-                                   T* __restrict__ y) {
+__global__ void recenter_rows_kernel(int64_t total, int32_t K, int32_t num_eq,
+                                     const int32_t* __restrict__ mask, double* __restrict__ yb,
+                                     T* __restrict__ y, T* __restrict__ anchor_y,
+                                     T* __restrict__ restart, T* __restrict__ prev,
+                                     T* __restrict__ sum, const double* __restrict__ sum_weight,
+                                     T* __restrict__ ylo, T* __restrict__ kx,
+                                     T* __restrict__ anchor_kx, const double* __restrict__ kshift) {
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
        e += (int64_t)gridDim.x * blockDim.x) {
     const int32_t k = static_cast<int32_t>(e % K);
     if (!mask[k]) continue;
     const int64_t i = e / K;
-    const double d = delta[k];
-    const double qq = mul(d, sub(q0[e], kxb[e]));
-    q[e] = static_cast<T>(qq);
-    if (q64) q64[e] = qq;
-    double floor_v = 0.0;
-    if (i >= num_eq) floor_v = -mul(d, yb[e]);
-    ylo[e] = static_cast<T>(floor_v);
-    y[e] = static_cast<T>(i >= num_eq ? fmax(0.0, floor_v) : 0.0);
+    const double off = static_cast<double>(y[e]);
+    double base = add(yb[e], off);
+    if (i >= num_eq && base < 0.0) base = 0.0;
+    const double shift = sub(base, yb[e]);
+    yb[e] = base;
+    y[e] = static_cast<T>(sub(off, shift));
+    anchor_y[e] = static_cast<T>(sub(static_cast<double>(anchor_y[e]), shift));
+    restart[e] = static_cast<T>(sub(static_cast<double>(restart[e]), shift));
+    if (prev) prev[e] = static_cast<T>(sub(static_cast<double>(prev[e]), shift));
+    if (sum) sum[e] = static_cast<T>(sub(static_cast<double>(sum[e]), mul(sum_weight[k], shift)));
+    ylo[e] = static_cast<T>(i >= num_eq ? -base : 0.0);
+    const double ks = kshift[e];
+    kx[e] = static_cast<T>(sub(static_cast<double>(kx[e]), ks));
+    anchor_kx[e] = static_cast<T>(sub(static_cast<double>(anchor_kx[e]), ks));
+  }
+}
+
+// The correction LP's cost c~ - K'y* and right-hand side q~ - K x* from the
+// base's FP64 products, for the masked cases.
+template <class T>
+__global__ void correction_data_kernel(int64_t total_n, int64_t total_m, int32_t K,
+                                       const int32_t* __restrict__ mask,
+                                       const double* __restrict__ c0,
+                                       const double* __restrict__ ktyb, T* __restrict__ c,
+                                       const double* __restrict__ q0,
+                                       const double* __restrict__ kxb, T* __restrict__ q,
+                                       double* __restrict__ q64) {
+  const int64_t total = total_n + total_m;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t e = t < total_n ? t : t - total_n;
+    const int32_t k = static_cast<int32_t>(e % K);
+    if (!mask[k]) continue;
+    if (t < total_n) {
+      c[e] = static_cast<T>(sub(c0[e], ktyb[e]));
+    } else {
+      const double v = sub(q0[e], kxb[e]);
+      q[e] = static_cast<T>(v);
+      if (q64) q64[e] = v;
+    }
   }
 }
 

@@ -145,15 +145,14 @@ typedef struct anu_pdhg_options {
 
   /* --- engine additions, no counterpart in PdhgOptions --- */
   int32_t precision;            /* ANU_PRECISION_FP64 (default) or _FP32 */
-  /* Iterative refinement, FP32 only. A refinement round ends when the
-   * worst relative KKT error (FP64) has fallen by refinement_inner_tolerance
-   * from the round's start, or has stopped improving; the next round
-   * re-centres the LP on the round's best point in FP64 and rescales it by
-   * 1/(that error), so the FP32 iterate carries only the correction. The
-   * termination test always judges the recombined FP64 point against the
-   * original LP. Feasibility polishing is off while refining. */
-  int32_t refinement_rounds;    /* 8; 0 = plain FP32 */
-  double refinement_inner_tolerance; /* 1e-3; 0 means 1e-3 */
+  /* Iterative refinement, FP32 only: the FP32 iterate is an offset from an
+   * FP64 base point. At every termination check the offset is folded into
+   * the base and the correction LP is re-formed from the FP64 residual
+   * there (cost c - K'y*, right-hand side q - K x*, bounds and dual floor
+   * shifted by the base); the PDHG state is shifted with it, so the
+   * trajectory continues unchanged while FP32 carries only the movement
+   * since the last check. 0 = plain FP32 iterates. */
+  int32_t refinement;           /* 1 */
   int32_t device;               /* CUDA device ordinal, 0 */
   int32_t use_graphs;           /* capture iteration chunks in CUDA graphs, 1 */
   /* Record CUDA events around every iteration chunk on the engine's stream
@@ -210,7 +209,7 @@ typedef struct anu_pdhg_result {
   double col_spread_before;
   double col_spread_after;
   /* engine additions */
-  int32_t refinement_rounds; /* outer refinement rounds actually run */
+  int32_t refinement_rounds; /* refinements (re-centrings) performed */
   int32_t kernel_launches;   /* kernels this solve launched (graph nodes included) */
   /* With options.profile: device time of the iteration chunks (CUDA events
    * on the engine stream) and the iterations they ran, summed over every

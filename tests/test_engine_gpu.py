@@ -90,6 +90,28 @@ def test_random_lp_fp32_reaches_tolerance(engine):
     assert abs(r.objective - obj) <= 1e-5 * abs(obj)
 
 
+@pytest.mark.parametrize("tol", [1e-6, 1e-8])
+def test_fp32_refinement_tracks_fp64(engine, tol):
+    """FP32 offsets on an FP64 base, re-formed at every check, follow the FP64
+    trajectory: same status, iteration count within one check period per
+    thousand iterations, objective within the tolerance, and the oracle's
+    FP64 residual of the returned point meets the tolerance."""
+    lp, obj = lpgen.random_lp()
+    a = engine.solve_pdhg(lp, tolerance=tol)
+    b = engine.solve_pdhg(lp, tolerance=tol, precision=PRECISION_FP32)
+    assert a.status == b.status == OPTIMAL
+    assert abs(a.iterations - b.iterations) <= 40 * (1 + a.iterations // 1000)
+    assert b.refinement_rounds > 0
+    assert oracle.oracle_residual(lp, b.x, b.y).converged(tol)
+    assert abs(a.objective - b.objective) <= 10 * tol * abs(a.objective)
+
+
+def test_fp32_plain_without_refinement_runs(engine):
+    lp, _ = lpgen.random_lp(300, 450, 8, seed=4)
+    r = engine.solve_pdhg(lp, tolerance=1e-4, precision=PRECISION_FP32, refinement=0)
+    assert r.status == OPTIMAL and r.refinement_rounds == 0
+
+
 def test_iteration_limit_exact(engine):
     lp = lp_cases.standard(lp_cases.wyndor())
     r = engine.solve_pdhg(lp, tolerance=1e-14, max_iterations=80,
