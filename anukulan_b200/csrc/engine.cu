@@ -19,6 +19,7 @@
 #include <utility>
 
 #include "engine.hpp"
+#include "resident.cuh"
 
 namespace anu {
 
@@ -84,7 +85,8 @@ void DevCsr::upload(const HostCsr& a, bool with_fp32, cudaStream_t s) {
   if (!bd.empty())
     ANU_CUDA(cudaMemcpyAsync(blocks.p, bd.data(), sizeof(RowBlockDev) * bd.size(),
                              cudaMemcpyHostToDevice, s));
-  const SegmentSchedule sch = segment_schedule(a, kSegNnz, kSegPerCta, kSegRows);
+  schedule = segment_schedule(a, kSegNnz, kSegPerCta, kSegRows);
+  const SegmentSchedule& sch = schedule;
   num_ctas = static_cast<int32_t>(sch.cta_row.size()) - 1;
   auto put = [&](DevBuf<int32_t>& d, const std::vector<int32_t>& h) {
     d.alloc(std::max<size_t>(h.size(), 1));
@@ -166,6 +168,137 @@ __global__ void normalize_kernel(int32_t n, const double* __restrict__ in,
 }
 
 }  // namespace
+
+// ------------------------------------------------------ resident plan
+
+namespace {
+
+// Assigns the segment-schedule units of one matrix to `grid` CTAs, longest
+// first to the least loaded CTA, and flattens what each CTA owns.
+void plan_side(const SegmentSchedule& sch, int grid, cudaStream_t s, ResidentSideTables* out) {
+  const int units = static_cast<int>(sch.cta_row.size()) - 1;
+  std::vector<int64_t> work(units);
+  for (int u = 0; u < units; ++u) {
+    const int32_t nnz = sch.seg_begin[sch.cta_seg[u + 1]] - sch.seg_begin[sch.cta_seg[u]];
+    work[u] = nnz + 4 * (sch.cta_row[u + 1] - sch.cta_row[u]);
+  }
+  std::vector<int> order(units);
+  for (int u = 0; u < units; ++u) order[u] = u;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return work[a] > work[b]; });
+  std::vector<std::vector<int>> owned(grid);
+  std::vector<int64_t> load(grid, 0);
+  for (int u : order) {
+    int best = 0;
+    for (int c = 1; c < grid; ++c)
+      if (load[c] < load[best]) best = c;
+    owned[best].push_back(u);
+    load[best] += work[u];
+  }
+  std::vector<int32_t> seg_off, segs, row_off, rows, row_lseg;
+  int32_t max_rows = 0, max_segs = 0;
+  for (int c = 0; c < grid; ++c) {
+    std::sort(owned[c].begin(), owned[c].end());
+    seg_off.push_back(static_cast<int32_t>(segs.size()));
+    row_off.push_back(static_cast<int32_t>(rows.size()));
+    const size_t s_begin = segs.size(), r_begin = rows.size();
+    for (int u : owned[c]) {
+      const int32_t s0 = sch.cta_seg[u], s1 = sch.cta_seg[u + 1];
+      const int32_t base = static_cast<int32_t>(segs.size());
+      for (int32_t g = s0; g < s1; ++g) segs.push_back(g);
+      for (int32_t r = sch.cta_row[u]; r < sch.cta_row[u + 1]; ++r) {
+        rows.push_back(r);
+        row_lseg.push_back(base + (sch.row_seg[r] - s0));
+      }
+    }
+    row_lseg.push_back(static_cast<int32_t>(segs.size()));
+    max_rows = std::max<int32_t>(max_rows, static_cast<int32_t>(rows.size() - r_begin));
+    max_segs = std::max<int32_t>(max_segs, static_cast<int32_t>(segs.size() - s_begin));
+  }
+  seg_off.push_back(static_cast<int32_t>(segs.size()));
+  row_off.push_back(static_cast<int32_t>(rows.size()));
+  auto put = [&](DevBuf<int32_t>& d, const std::vector<int32_t>& h) {
+    d.alloc(std::max<size_t>(h.size(), 1));
+    if (!h.empty())
+      ANU_CUDA(cudaMemcpyAsync(d.p, h.data(), sizeof(int32_t) * h.size(), cudaMemcpyHostToDevice, s));
+  };
+  put(out->seg_off, seg_off);
+  put(out->segs, segs);
+  put(out->row_off, row_off);
+  put(out->rows, rows);
+  put(out->row_lseg, row_lseg);
+  ANU_CUDA(cudaStreamSynchronize(s));
+  out->max_rows = max_rows;
+  out->max_segs = max_segs;
+}
+
+size_t resident_smem_bytes(const ResidentPlan& plan, int K, size_t elem) {
+  const size_t max_segs = std::max(plan.primal.max_segs, plan.dual.max_segs);
+  return sizeof(double) * kMaxCaseLanes + elem * max_segs * kMaxCaseLanes +
+         elem * 6 * static_cast<size_t>(plan.primal.max_rows) * K +
+         elem * 7 * static_cast<size_t>(plan.dual.max_rows) * K;
+}
+
+constexpr size_t kResidentSmemCap = 200 * 1024;
+
+template <class T, int L, int CPL>
+bool resident_fits(size_t smem) {
+  auto fn = resident_chunk_kernel<T, L, CPL>;
+  if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           static_cast<int>(smem)) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  int blocks = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, fn, kResidentThreads, smem) !=
+      cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return blocks >= 1;
+}
+
+template <class T>
+bool resident_fits_k(int K, size_t smem) {
+  if (K <= 4) return resident_fits<T, 4, 1>(smem);
+  if (K <= 8) return resident_fits<T, 8, 1>(smem);
+  if (K <= 16) return resident_fits<T, 16, 1>(smem);
+  if (K <= 32) return resident_fits<T, 32, 1>(smem);
+  return resident_fits<T, 32, 2>(smem);
+}
+
+template <class T>
+void launch_resident(const ResidentArgs<T>& args, int grid, size_t smem, cudaStream_t s) {
+  ResidentArgs<T> a = args;
+  void* params[] = {&a};
+  cudaError_t e;
+#define ANU_RES(L_, CPL_)                                                                      \
+  e = cudaLaunchCooperativeKernel(reinterpret_cast<void*>(resident_chunk_kernel<T, L_, CPL_>), \
+                                  dim3(grid), dim3(kResidentThreads), params, smem, s)
+  if (a.K <= 4) ANU_RES(4, 1);
+  else if (a.K <= 8) ANU_RES(8, 1);
+  else if (a.K <= 16) ANU_RES(16, 1);
+  else if (a.K <= 32) ANU_RES(32, 1);
+  else ANU_RES(32, 2);
+#undef ANU_RES
+  cuda_check(e, "cooperative launch of the resident kernel");
+}
+
+}  // namespace
+
+// Plans the resident kernel for this problem once: one CTA per SM (fewer when
+// the schedule has fewer units).
+void ensure_resident_plan(Problem& p) {
+  if (p.resident.built) return;
+  p.resident.built = true;
+  int sms = 0, coop = 0;
+  ANU_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p.device));
+  ANU_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, p.device));
+  if (!coop || p.dk.num_ctas == 0 || p.dkt.num_ctas == 0) return;
+  const int grid = std::min(sms, std::max(p.dk.num_ctas, p.dkt.num_ctas));
+  plan_side(p.dkt.schedule, grid, p.stream, &p.resident.primal);
+  plan_side(p.dk.schedule, grid, p.stream, &p.resident.dual);
+  p.resident.grid = grid;
+}
 
 // ------------------------------------------------------ ||K|| estimate
 
@@ -489,6 +622,8 @@ struct Workspace {
   DevBuf<double> xb, yb, x_comb, y_comb, c0s, q0s, l0s, u0s, kshift, sum_weight;
   DevBuf<StepParams> params;
   DevBuf<double> w_table;
+  DevBuf<unsigned int> counter;  // resident kernel: grid barrier arrivals
+  DevBuf<int> error;             // resident kernel: a barrier wait gave up
   DevBuf<int32_t> mask;
   DevBuf<double> partial, terms, kkt, weights;
   std::map<std::pair<int, int>, cudaGraphExec_t> graphs;
@@ -539,7 +674,9 @@ template <class T>
 void run_cases_t(Problem& p, const std::vector<const CaseData*>& cases,
                  const anu_pdhg_options& o, const std::vector<const std::vector<double>*>& warm_x,
                  const std::vector<const std::vector<double>*>& warm_y,
-                 std::vector<CaseResult>* results, double start_time, bool unit);
+                 std::vector<CaseResult>* results, double start_time, bool unit,
+                 const std::vector<double>* init_eta = nullptr,
+                 const std::vector<double>* init_omega = nullptr);
 
 // Feasibility polishing of a set of cases (pdhg.cpp:666-751): a primal
 // sub-stack (c = 0) warm started from the seeds' x, then a dual sub-stack
@@ -597,11 +734,13 @@ void run_polish(Problem& p, bool unit, const std::vector<const CaseData*>& paren
   sub.termination_check_frequency =
       std::max<int32_t>(10, std::min(o.termination_check_frequency, budget / 4));
   sub.time_limit_seconds = std::fmax(0.0, o.time_limit_seconds - (now_seconds() - start_time));
-  // The sub-stacks get the parent's step size and weight per case.
+  // One sub-stack per side for every polishing case, each case started from
+  // its parent's step size and primal weight (pdhg.cpp:703-704).
   std::vector<const CaseData*> pp(W), dd(W);
   std::vector<std::vector<double>> zx(W, std::vector<double>(p.n, 0.0)),
       zy(W, std::vector<double>(p.m, 0.0));
   std::vector<const std::vector<double>*> wx(W), wy(W), wx2(W), wy2(W);
+  std::vector<double> etas(W), omegas(W);
   for (size_t w = 0; w < W; ++w) {
     pp[w] = &primal[w];
     dd[w] = &dual[w];
@@ -609,42 +748,14 @@ void run_polish(Problem& p, bool unit, const std::vector<const CaseData*>& paren
     wy[w] = &zy[w];
     wx2[w] = &zx[w];
     wy2[w] = &seed_y[w];
+    etas[w] = states[which[w]].eta;
+    omegas[w] = states[which[w]].omega;
   }
-  // Step size and primal weight differ per case, so each case runs as its own
-  // sub-stack when they differ; cases with equal values share one.
-  std::vector<CaseResult> pres(W), dres(W);
-  std::vector<bool> done(W, false);
-  for (size_t w0 = 0; w0 < W; ++w0) {
-    if (done[w0]) continue;
-    std::vector<size_t> group;
-    for (size_t w = w0; w < W; ++w)
-      if (!done[w] && states[which[w]].eta == states[which[w0]].eta &&
-          states[which[w]].omega == states[which[w0]].omega)
-        group.push_back(w);
-    anu_pdhg_options g = sub;
-    g.initial_step_size = states[which[w0]].eta;
-    g.initial_primal_weight = states[which[w0]].omega;
-    std::vector<const CaseData*> gp, gd;
-    std::vector<const std::vector<double>*> gwx, gwy, gwx2, gwy2;
-    for (size_t w : group) {
-      gp.push_back(pp[w]);
-      gd.push_back(dd[w]);
-      gwx.push_back(wx[w]);
-      gwy.push_back(wy[w]);
-      gwx2.push_back(wx2[w]);
-      gwy2.push_back(wy2[w]);
-      done[w] = true;
-    }
-    std::vector<CaseResult> rp, rd;
-    g.termination = ANU_TERMINATION_PRIMAL_FEASIBILITY;
-    run_cases_t<T>(p, gp, g, gwx, gwy, &rp, now_seconds(), true);
-    g.termination = ANU_TERMINATION_DUAL_FEASIBILITY;
-    run_cases_t<T>(p, gd, g, gwx2, gwy2, &rd, now_seconds(), true);
-    for (size_t i = 0; i < group.size(); ++i) {
-      pres[group[i]] = std::move(rp[i]);
-      dres[group[i]] = std::move(rd[i]);
-    }
-  }
+  std::vector<CaseResult> pres, dres;
+  sub.termination = ANU_TERMINATION_PRIMAL_FEASIBILITY;
+  run_cases_t<T>(p, pp, sub, wx, wy, &pres, now_seconds(), true, &etas, &omegas);
+  sub.termination = ANU_TERMINATION_DUAL_FEASIBILITY;
+  run_cases_t<T>(p, dd, sub, wx2, wy2, &dres, now_seconds(), true, &etas, &omegas);
   out_xs->assign(W, {});
   out_ys->assign(W, {});
   out_x->assign(W, {});
@@ -675,7 +786,8 @@ template <class T>
 void run_cases_t(Problem& p, const std::vector<const CaseData*>& cases,
                  const anu_pdhg_options& o, const std::vector<const std::vector<double>*>& warm_x,
                  const std::vector<const std::vector<double>*>& warm_y,
-                 std::vector<CaseResult>* results, double start_time, bool unit) {
+                 std::vector<CaseResult>* results, double start_time, bool unit,
+                 const std::vector<double>* init_eta, const std::vector<double>* init_omega) {
   const int K = static_cast<int>(cases.size());
   const int32_t n = p.n, m = p.m;
   results->assign(K, CaseResult{});
@@ -779,6 +891,9 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& cases,
     }
     if (o.initial_step_size > 0.0) eta = o.initial_step_size;
     if (o.initial_primal_weight > 0.0) omega = o.initial_primal_weight;
+    // Polishing sub-stacks hand each case its parent's values.
+    if (init_eta != nullptr && (*init_eta)[k] > 0.0) eta = (*init_eta)[k];
+    if (init_omega != nullptr && (*init_omega)[k] > 0.0) omega = (*init_omega)[k];
     S[k].eta = eta;
     S[k].omega = omega;
   }
@@ -973,7 +1088,7 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& cases,
       P.active = S[k].active ? 1 : 0;
       P.halpern = halpern ? 1 : 0;
       P.reset_pending = (halpern && S[k].anchor_needs_reset) ? 1 : 0;
-      P.pad = 0;
+      P.k_base = S[k].halpern_k;
       for (int it = 0; it < len; ++it) {
         double wv = 1.0;
         if (halpern) {
@@ -989,6 +1104,32 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& cases,
   };
 
   const T* ylo_ptr = any_ylo ? w.ylo.p : nullptr;
+
+  // The resident iteration kernel serves case stacks whose owned state fits
+  // in one CTA's shared memory per SM; other runs use graph chunks of the
+  // two fused kernels.
+  bool use_resident = false;
+  size_t resident_smem = 0;
+  if (!slow && K >= 2 && o.resident) {
+    ensure_resident_plan(p);
+    if (p.resident.grid > 0) {
+      resident_smem = resident_smem_bytes(p.resident, K, sizeof(T));
+      use_resident = resident_smem <= kResidentSmemCap && resident_fits_k<T>(K, resident_smem);
+    }
+  }
+  if (use_resident) {
+    w.counter.alloc(1);
+    w.error.alloc(1);
+    ANU_CUDA(cudaMemsetAsync(w.error.p, 0, sizeof(int), st));
+  }
+  auto check_resident_error = [&]() {
+    if (!use_resident) return;
+    int err = 0;
+    ANU_CUDA(cudaMemcpyAsync(&err, w.error.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    ANU_CUDA(cudaStreamSynchronize(st));
+    if (err != 0)
+      throw Error(ANU_ERR_DEVICE_WAIT, "a grid barrier of the resident kernel timed out");
+  };
   // One fast-path iteration (in place).
   auto launch_iteration = [&](int it, uint32_t flags) {
     PrimalEpi<T> pe{K, it, flags, w.params.p, w.w_table.p, w.x.p, w.x.p, w.c.p, w.lo.p, w.hi.p,
@@ -1001,6 +1142,46 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& cases,
 
   auto run_chunk_body = [&](int len, bool check_at_end) {
     const uint32_t base_flags = averaging ? kAccumulate : 0u;
+    if (use_resident) {
+      ResidentArgs<T> A;
+      A.kt = p.dkt.view<T>();
+      A.k = p.dk.view<T>();
+      const ResidentSideTables& ps = p.resident.primal;
+      const ResidentSideTables& ds = p.resident.dual;
+      A.ps = {ps.seg_off.p, ps.segs.p, ps.row_off.p, ps.rows.p, ps.row_lseg.p};
+      A.ds = {ds.seg_off.p, ds.segs.p, ds.row_off.p, ds.rows.p, ds.row_lseg.p};
+      A.K = K;
+      A.num_eq = p.num_eq;
+      A.len = len;
+      A.flags_last = check_at_end ? kWriteDelta : 0u;
+      A.flags = base_flags;
+      A.params = w.params.p;
+      A.x = w.x.p;
+      A.x_bar = w.x_bar.p;
+      A.c = w.c.p;
+      A.lo = w.lo.p;
+      A.hi = w.hi.p;
+      A.anchor_x = w.anchor_x.p;
+      A.dx = w.dx.p;
+      A.sum_x = w.sum_x.p;
+      A.y = w.y.p;
+      A.q = w.q.p;
+      A.kx = w.kx.p;
+      A.anchor_y = w.anchor_y.p;
+      A.anchor_kx = w.anchor_kx.p;
+      A.dy = w.dy.p;
+      A.sum_y = w.sum_y.p;
+      A.ylo = ylo_ptr;
+      A.counter = w.counter.p;
+      A.error = w.error.p;
+      A.max_cols = ps.max_rows;
+      A.max_rows = ds.max_rows;
+      A.max_segs = std::max(ps.max_segs, ds.max_segs);
+      ANU_CUDA(cudaMemsetAsync(w.counter.p, 0, sizeof(unsigned int), st));
+      launch_resident<T>(A, p.resident.grid, resident_smem, st);
+      p.launches += 1;
+      return;
+    }
     if (o.use_graphs) {
       const auto key = std::make_pair(len, check_at_end ? 1 : 0);
       auto found = w.graphs.find(key);
@@ -1220,6 +1401,7 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& cases,
         P.active = 1;
         P.halpern = blend ? 1 : 0;
         P.reset_pending = 0;
+        P.k_base = 0;
         h_w.p[0] = hw;
         ANU_CUDA(cudaMemcpyAsync(w.params.p, h_params.p, sizeof(StepParams), cudaMemcpyHostToDevice, st));
         ANU_CUDA(cudaMemcpyAsync(w.w_table.p, h_w.p, sizeof(double), cudaMemcpyHostToDevice, st));
@@ -1295,6 +1477,7 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& cases,
     iteration = last + 1;
     if (!is_check) continue;
     ANU_CUDA(cudaStreamSynchronize(st));
+    check_resident_error();
     t_iter += phase_end();
 
     // ------------------------------------------------------------- check
@@ -1541,6 +1724,7 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& cases,
     recenter();
     t_checks += phase_end();
   }
+  check_resident_error();
   for (int k = 0; k < K; ++k)
     if (S[k].active) {
       S[k].final_iteration = iteration;
@@ -1788,6 +1972,7 @@ void anu_pdhg_default_options(anu_pdhg_options* o) {
   o->device = 0;
   o->use_graphs = 1;
   o->profile = 0;
+  o->resident = 1;
 }
 
 int anu_last_error(char* buf, int32_t size) { return anu::copy_last_error(buf, size); }

@@ -94,7 +94,7 @@ struct StepParams {
   int32_t active;      // 0: retired, its lanes do nothing
   int32_t halpern;     // Halpern blending on for this case
   int32_t reset_pending;  // the chunk's first step starts a new epoch
-  int32_t pad;
+  int32_t k_base;         // Halpern counter at the chunk's first step
 };
 
 enum : uint32_t {
