@@ -85,8 +85,7 @@ void DevCsr::upload(const HostCsr& a, bool with_fp32, cudaStream_t s) {
   if (!bd.empty())
     ANU_CUDA(cudaMemcpyAsync(blocks.p, bd.data(), sizeof(RowBlockDev) * bd.size(),
                              cudaMemcpyHostToDevice, s));
-  schedule = segment_schedule(a, kSegNnz, kSegPerCta, kSegRows);
-  const SegmentSchedule& sch = schedule;
+  const SegmentSchedule sch = segment_schedule(a, kSegNnz, kSegPerCta, kSegRows);
   num_ctas = static_cast<int32_t>(sch.cta_row.size()) - 1;
   auto put = [&](DevBuf<int32_t>& d, const std::vector<int32_t>& h) {
     d.alloc(std::max<size_t>(h.size(), 1));
@@ -169,87 +168,22 @@ __global__ void normalize_kernel(int32_t n, const double* __restrict__ in,
 
 }  // namespace
 
-// ------------------------------------------------------ resident plan
+// ------------------------------------------------------ case-resident kernel
 
 namespace {
 
-// Assigns the segment-schedule units of one matrix to `grid` CTAs, longest
-// first to the least loaded CTA, and flattens what each CTA owns.
-void plan_side(const SegmentSchedule& sch, int grid, cudaStream_t s, ResidentSideTables* out) {
-  const int units = static_cast<int>(sch.cta_row.size()) - 1;
-  std::vector<int64_t> work(units);
-  for (int u = 0; u < units; ++u) {
-    const int32_t nnz = sch.seg_begin[sch.cta_seg[u + 1]] - sch.seg_begin[sch.cta_seg[u]];
-    work[u] = nnz + 4 * (sch.cta_row[u + 1] - sch.cta_row[u]);
-  }
-  std::vector<int> order(units);
-  for (int u = 0; u < units; ++u) order[u] = u;
-  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return work[a] > work[b]; });
-  std::vector<std::vector<int>> owned(grid);
-  std::vector<int64_t> load(grid, 0);
-  for (int u : order) {
-    int best = 0;
-    for (int c = 1; c < grid; ++c)
-      if (load[c] < load[best]) best = c;
-    owned[best].push_back(u);
-    load[best] += work[u];
-  }
-  std::vector<int32_t> seg_off, segs, row_off, rows, row_lseg;
-  int32_t max_rows = 0, max_segs = 0;
-  for (int c = 0; c < grid; ++c) {
-    std::sort(owned[c].begin(), owned[c].end());
-    seg_off.push_back(static_cast<int32_t>(segs.size()));
-    row_off.push_back(static_cast<int32_t>(rows.size()));
-    const size_t s_begin = segs.size(), r_begin = rows.size();
-    for (int u : owned[c]) {
-      const int32_t s0 = sch.cta_seg[u], s1 = sch.cta_seg[u + 1];
-      const int32_t base = static_cast<int32_t>(segs.size());
-      for (int32_t g = s0; g < s1; ++g) segs.push_back(g);
-      for (int32_t r = sch.cta_row[u]; r < sch.cta_row[u + 1]; ++r) {
-        rows.push_back(r);
-        row_lseg.push_back(base + (sch.row_seg[r] - s0));
-      }
-    }
-    row_lseg.push_back(static_cast<int32_t>(segs.size()));
-    max_rows = std::max<int32_t>(max_rows, static_cast<int32_t>(rows.size() - r_begin));
-    max_segs = std::max<int32_t>(max_segs, static_cast<int32_t>(segs.size() - s_begin));
-  }
-  seg_off.push_back(static_cast<int32_t>(segs.size()));
-  row_off.push_back(static_cast<int32_t>(rows.size()));
-  auto put = [&](DevBuf<int32_t>& d, const std::vector<int32_t>& h) {
-    d.alloc(std::max<size_t>(h.size(), 1));
-    if (!h.empty())
-      ANU_CUDA(cudaMemcpyAsync(d.p, h.data(), sizeof(int32_t) * h.size(), cudaMemcpyHostToDevice, s));
-  };
-  put(out->seg_off, seg_off);
-  put(out->segs, segs);
-  put(out->row_off, row_off);
-  put(out->rows, rows);
-  put(out->row_lseg, row_lseg);
-  ANU_CUDA(cudaStreamSynchronize(s));
-  out->max_rows = max_rows;
-  out->max_segs = max_segs;
-}
+constexpr size_t kCaseSmemCap = 200 * 1024;
 
-size_t resident_smem_bytes(const ResidentPlan& plan, int K, size_t elem) {
-  const size_t max_segs = std::max(plan.primal.max_segs, plan.dual.max_segs);
-  return sizeof(double) * kMaxCaseLanes + elem * max_segs * kMaxCaseLanes +
-         elem * 6 * static_cast<size_t>(plan.primal.max_rows) * K +
-         elem * 7 * static_cast<size_t>(plan.dual.max_rows) * K;
-}
-
-constexpr size_t kResidentSmemCap = 200 * 1024;
-
-template <class T, int L, int CPL>
-bool resident_fits(size_t smem) {
-  auto fn = resident_chunk_kernel<T, L, CPL>;
+template <class T, int VP, int VD>
+bool case_chunk_fits(size_t smem) {
+  auto fn = case_chunk_kernel<T, VP, VD>;
   if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            static_cast<int>(smem)) != cudaSuccess) {
     cudaGetLastError();
     return false;
   }
   int blocks = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, fn, kResidentThreads, smem) !=
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, fn, kCaseThreads, smem) !=
       cudaSuccess) {
     cudaGetLastError();
     return false;
@@ -257,48 +191,53 @@ bool resident_fits(size_t smem) {
   return blocks >= 1;
 }
 
+// Runs F(VP, VD) with the compile-time vector widths matching vp, vd.
+#define ANU_CASE_DISPATCH(vp, vd, CALL)                     \
+  do {                                                      \
+    if ((vp) == 4) {                                        \
+      if ((vd) == 4) CALL(4, 4);                            \
+      else if ((vd) == 8) CALL(4, 8);                       \
+      else if ((vd) == 16) CALL(4, 16);                     \
+      else CALL(4, 32);                                     \
+    } else if ((vp) == 8) {                                 \
+      if ((vd) == 4) CALL(8, 4);                            \
+      else if ((vd) == 8) CALL(8, 8);                       \
+      else if ((vd) == 16) CALL(8, 16);                     \
+      else CALL(8, 32);                                     \
+    } else if ((vp) == 16) {                                \
+      if ((vd) == 4) CALL(16, 4);                           \
+      else if ((vd) == 8) CALL(16, 8);                      \
+      else if ((vd) == 16) CALL(16, 16);                    \
+      else CALL(16, 32);                                    \
+    } else {                                                \
+      if ((vd) == 4) CALL(32, 4);                           \
+      else if ((vd) == 8) CALL(32, 8);                      \
+      else if ((vd) == 16) CALL(32, 16);                    \
+      else CALL(32, 32);                                    \
+    }                                                       \
+  } while (0)
+
 template <class T>
-bool resident_fits_k(int K, size_t smem) {
-  if (K <= 4) return resident_fits<T, 4, 1>(smem);
-  if (K <= 8) return resident_fits<T, 8, 1>(smem);
-  if (K <= 16) return resident_fits<T, 16, 1>(smem);
-  if (K <= 32) return resident_fits<T, 32, 1>(smem);
-  return resident_fits<T, 32, 2>(smem);
+bool case_chunk_eligible(int vp, int vd, size_t smem) {
+  if (smem > kCaseSmemCap) return false;
+  bool ok = false;
+#define ANU_FITS(a_, b_) ok = case_chunk_fits<T, a_, b_>(smem)
+  ANU_CASE_DISPATCH(vp, vd, ANU_FITS);
+#undef ANU_FITS
+  return ok;
 }
 
 template <class T>
-void launch_resident(const ResidentArgs<T>& args, int grid, size_t smem, cudaStream_t s) {
-  ResidentArgs<T> a = args;
-  void* params[] = {&a};
-  cudaError_t e;
-#define ANU_RES(L_, CPL_)                                                                      \
-  e = cudaLaunchCooperativeKernel(reinterpret_cast<void*>(resident_chunk_kernel<T, L_, CPL_>), \
-                                  dim3(grid), dim3(kResidentThreads), params, smem, s)
-  if (a.K <= 4) ANU_RES(4, 1);
-  else if (a.K <= 8) ANU_RES(8, 1);
-  else if (a.K <= 16) ANU_RES(16, 1);
-  else if (a.K <= 32) ANU_RES(32, 1);
-  else ANU_RES(32, 2);
-#undef ANU_RES
-  cuda_check(e, "cooperative launch of the resident kernel");
+void launch_case_chunk(const CaseChunkArgs<T>& args, int vp, int vd, size_t smem,
+                       cudaStream_t s) {
+#define ANU_LAUNCH(a_, b_) \
+  case_chunk_kernel<T, a_, b_><<<args.K, kCaseThreads, smem, s>>>(args)
+  ANU_CASE_DISPATCH(vp, vd, ANU_LAUNCH);
+#undef ANU_LAUNCH
+  cuda_check(cudaGetLastError(), "case-resident kernel launch");
 }
 
 }  // namespace
-
-// Plans the resident kernel for this problem once: one CTA per SM (fewer when
-// the schedule has fewer units).
-void ensure_resident_plan(Problem& p) {
-  if (p.resident.built) return;
-  p.resident.built = true;
-  int sms = 0, coop = 0;
-  ANU_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p.device));
-  ANU_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, p.device));
-  if (!coop || p.dk.num_ctas == 0 || p.dkt.num_ctas == 0) return;
-  const int grid = std::min(sms, std::max(p.dk.num_ctas, p.dkt.num_ctas));
-  plan_side(p.dkt.schedule, grid, p.stream, &p.resident.primal);
-  plan_side(p.dk.schedule, grid, p.stream, &p.resident.dual);
-  p.resident.grid = grid;
-}
 
 // ------------------------------------------------------ ||K|| estimate
 
@@ -622,8 +561,6 @@ struct Workspace {
   DevBuf<double> xb, yb, x_comb, y_comb, c0s, q0s, l0s, u0s, kshift, sum_weight;
   DevBuf<StepParams> params;
   DevBuf<double> w_table;
-  DevBuf<unsigned int> counter;  // resident kernel: grid barrier arrivals
-  DevBuf<int> error;             // resident kernel: a barrier wait gave up
   DevBuf<int32_t> mask;
   DevBuf<double> partial, terms, kkt, weights;
   std::map<std::pair<int, int>, cudaGraphExec_t> graphs;
@@ -1105,31 +1042,14 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& cases,
 
   const T* ylo_ptr = any_ylo ? w.ylo.p : nullptr;
 
-  // The resident iteration kernel serves case stacks whose owned state fits
-  // in one CTA's shared memory per SM; other runs use graph chunks of the
-  // two fused kernels.
-  bool use_resident = false;
-  size_t resident_smem = 0;
-  if (!slow && K >= 2 && o.resident) {
-    ensure_resident_plan(p);
-    if (p.resident.grid > 0) {
-      resident_smem = resident_smem_bytes(p.resident, K, sizeof(T));
-      use_resident = resident_smem <= kResidentSmemCap && resident_fits_k<T>(K, resident_smem);
-    }
-  }
-  if (use_resident) {
-    w.counter.alloc(1);
-    w.error.alloc(1);
-    ANU_CUDA(cudaMemsetAsync(w.error.p, 0, sizeof(int), st));
-  }
-  auto check_resident_error = [&]() {
-    if (!use_resident) return;
-    int err = 0;
-    ANU_CUDA(cudaMemcpyAsync(&err, w.error.p, sizeof(int), cudaMemcpyDeviceToHost, st));
-    ANU_CUDA(cudaStreamSynchronize(st));
-    if (err != 0)
-      throw Error(ANU_ERR_DEVICE_WAIT, "a grid barrier of the resident kernel timed out");
-  };
+  // The case-resident kernel serves case stacks whose per-case state fits in
+  // one CTA's shared memory; other runs use graph chunks of the two fused
+  // kernels.
+  const int vp = vector_width(p.dkt.rows, p.dkt.nnz);
+  const int vd = vector_width(p.dk.rows, p.dk.nnz);
+  const size_t case_smem = case_chunk_smem(m, n, sizeof(T));
+  const bool use_resident = !slow && K >= 2 && o.resident && !averaging &&
+                            case_chunk_eligible<T>(vp, vd, case_smem);
   // One fast-path iteration (in place).
   auto launch_iteration = [&](int it, uint32_t flags) {
     PrimalEpi<T> pe{K, it, flags, w.params.p, w.w_table.p, w.x.p, w.x.p, w.c.p, w.lo.p, w.hi.p,
@@ -1143,42 +1063,30 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& cases,
   auto run_chunk_body = [&](int len, bool check_at_end) {
     const uint32_t base_flags = averaging ? kAccumulate : 0u;
     if (use_resident) {
-      ResidentArgs<T> A;
+      CaseChunkArgs<T> A;
       A.kt = p.dkt.view<T>();
       A.k = p.dk.view<T>();
-      const ResidentSideTables& ps = p.resident.primal;
-      const ResidentSideTables& ds = p.resident.dual;
-      A.ps = {ps.seg_off.p, ps.segs.p, ps.row_off.p, ps.rows.p, ps.row_lseg.p};
-      A.ds = {ds.seg_off.p, ds.segs.p, ds.row_off.p, ds.rows.p, ds.row_lseg.p};
       A.K = K;
+      A.m = m;
+      A.n = n;
       A.num_eq = p.num_eq;
       A.len = len;
       A.flags_last = check_at_end ? kWriteDelta : 0u;
-      A.flags = base_flags;
       A.params = w.params.p;
       A.x = w.x.p;
-      A.x_bar = w.x_bar.p;
       A.c = w.c.p;
       A.lo = w.lo.p;
       A.hi = w.hi.p;
       A.anchor_x = w.anchor_x.p;
       A.dx = w.dx.p;
-      A.sum_x = w.sum_x.p;
       A.y = w.y.p;
       A.q = w.q.p;
       A.kx = w.kx.p;
       A.anchor_y = w.anchor_y.p;
       A.anchor_kx = w.anchor_kx.p;
       A.dy = w.dy.p;
-      A.sum_y = w.sum_y.p;
       A.ylo = ylo_ptr;
-      A.counter = w.counter.p;
-      A.error = w.error.p;
-      A.max_cols = ps.max_rows;
-      A.max_rows = ds.max_rows;
-      A.max_segs = std::max(ps.max_segs, ds.max_segs);
-      ANU_CUDA(cudaMemsetAsync(w.counter.p, 0, sizeof(unsigned int), st));
-      launch_resident<T>(A, p.resident.grid, resident_smem, st);
+      launch_case_chunk<T>(A, vp, vd, case_smem, st);
       p.launches += 1;
       return;
     }
@@ -1477,7 +1385,6 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& cases,
     iteration = last + 1;
     if (!is_check) continue;
     ANU_CUDA(cudaStreamSynchronize(st));
-    check_resident_error();
     t_iter += phase_end();
 
     // ------------------------------------------------------------- check
@@ -1724,7 +1631,6 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& cases,
     recenter();
     t_checks += phase_end();
   }
-  check_resident_error();
   for (int k = 0; k < K; ++k)
     if (S[k].active) {
       S[k].final_iteration = iteration;

@@ -77,25 +77,9 @@ struct DevCsr {
   int32_t num_blocks = 0;
   DevBuf<int32_t> seg_begin, row_seg, cta_row, cta_seg;
   int32_t num_ctas = 0;
-  SegmentSchedule schedule;  // host copy, for planning the resident kernel
   void upload(const HostCsr& a, bool with_fp32, cudaStream_t s);
   template <class V>
   CsrView<V> view() const;
-};
-
-// Ownership tables of the resident kernel for one side (see resident.cuh):
-// which segment-schedule units each CTA owns, flattened.
-struct ResidentSideTables {
-  DevBuf<int32_t> seg_off, segs, row_off, rows, row_lseg;
-  int32_t max_rows = 0;
-  int32_t max_segs = 0;
-};
-
-struct ResidentPlan {
-  bool built = false;
-  int grid = 0;
-  ResidentSideTables primal;  // over K' (columns)
-  ResidentSideTables dual;    // over K (rows)
 };
 
 // Everything that depends on the matrix alone: the scaled matrix and its
@@ -113,7 +97,6 @@ struct Problem : Exec {
   double matrix_norm = 0.0;
   bool owns_stream = false;
   int device = 0;
-  ResidentPlan resident;
   ~Problem();
 };
 
@@ -149,8 +132,6 @@ void run_cases(Problem& problem, const std::vector<const CaseData*>& cases,
                const std::vector<const std::vector<double>*>& warm_x,
                const std::vector<const std::vector<double>*>& warm_y,
                std::vector<CaseResult>* results, double start_time);
-
-void ensure_resident_plan(Problem& p);
 
 // ||K~|| by power iteration on the device, FP64 (pdhg.cpp:223-282).
 double device_matrix_norm(Problem& p, int iterations, double tolerance);

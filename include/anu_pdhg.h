@@ -159,10 +159,10 @@ typedef struct anu_pdhg_options {
    * and report their total in anu_pdhg_result::device_iteration_seconds.
    * Events do not serialise the stream. 0 = off. */
   int32_t profile;
-  /* Case stacks whose per-SM share of the iteration state fits in shared
-   * memory run each check period as one persistent cooperative kernel
-   * (state resident in shared memory, grid barriers between the primal and
-   * dual phases). 0 = always use graph chunks of the two fused kernels. */
+  /* Case stacks whose per-case iteration state fits in one CTA's shared
+   * memory run each check period as one launch with a CTA per case, the
+   * state resident in shared memory for the whole period. 0 = always use
+   * graph chunks of the two fused SpMM kernels. */
   int32_t resident;             /* 1 */
 } anu_pdhg_options;
 
