@@ -19,7 +19,6 @@
 #include <utility>
 
 #include "engine.hpp"
-#include "resident.cuh"
 
 namespace anu {
 
@@ -164,77 +163,6 @@ __global__ void normalize_kernel(int32_t n, const double* __restrict__ in,
   for (int32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
     out[j] = next != 0.0 ? in[j] / next : 0.0;
   if (blockIdx.x == 0 && threadIdx.x == 0) estimates[slot] = next;
-}
-
-}  // namespace
-
-// ------------------------------------------------------ case-resident kernel
-
-namespace {
-
-constexpr size_t kCaseSmemCap = 200 * 1024;
-
-template <class T, int VP, int VD>
-bool case_chunk_fits(size_t smem) {
-  auto fn = case_chunk_kernel<T, VP, VD>;
-  if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           static_cast<int>(smem)) != cudaSuccess) {
-    cudaGetLastError();
-    return false;
-  }
-  int blocks = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, fn, kCaseThreads, smem) !=
-      cudaSuccess) {
-    cudaGetLastError();
-    return false;
-  }
-  return blocks >= 1;
-}
-
-// Runs F(VP, VD) with the compile-time vector widths matching vp, vd.
-#define ANU_CASE_DISPATCH(vp, vd, CALL)                     \
-  do {                                                      \
-    if ((vp) == 4) {                                        \
-      if ((vd) == 4) CALL(4, 4);                            \
-      else if ((vd) == 8) CALL(4, 8);                       \
-      else if ((vd) == 16) CALL(4, 16);                     \
-      else CALL(4, 32);                                     \
-    } else if ((vp) == 8) {                                 \
-      if ((vd) == 4) CALL(8, 4);                            \
-      else if ((vd) == 8) CALL(8, 8);                       \
-      else if ((vd) == 16) CALL(8, 16);                     \
-      else CALL(8, 32);                                     \
-    } else if ((vp) == 16) {                                \
-      if ((vd) == 4) CALL(16, 4);                           \
-      else if ((vd) == 8) CALL(16, 8);                      \
-      else if ((vd) == 16) CALL(16, 16);                    \
-      else CALL(16, 32);                                    \
-    } else {                                                \
-      if ((vd) == 4) CALL(32, 4);                           \
-      else if ((vd) == 8) CALL(32, 8);                      \
-      else if ((vd) == 16) CALL(32, 16);                    \
-      else CALL(32, 32);                                    \
-    }                                                       \
-  } while (0)
-
-template <class T>
-bool case_chunk_eligible(int vp, int vd, size_t smem) {
-  if (smem > kCaseSmemCap) return false;
-  bool ok = false;
-#define ANU_FITS(a_, b_) ok = case_chunk_fits<T, a_, b_>(smem)
-  ANU_CASE_DISPATCH(vp, vd, ANU_FITS);
-#undef ANU_FITS
-  return ok;
-}
-
-template <class T>
-void launch_case_chunk(const CaseChunkArgs<T>& args, int vp, int vd, size_t smem,
-                       cudaStream_t s) {
-#define ANU_LAUNCH(a_, b_) \
-  case_chunk_kernel<T, a_, b_><<<args.K, kCaseThreads, smem, s>>>(args)
-  ANU_CASE_DISPATCH(vp, vd, ANU_LAUNCH);
-#undef ANU_LAUNCH
-  cuda_check(cudaGetLastError(), "case-resident kernel launch");
 }
 
 }  // namespace
@@ -1042,54 +970,18 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& cases,
 
   const T* ylo_ptr = any_ylo ? w.ylo.p : nullptr;
 
-  // The case-resident kernel serves case stacks whose per-case state fits in
-  // one CTA's shared memory; other runs use graph chunks of the two fused
-  // kernels.
-  const int vp = vector_width(p.dkt.rows, p.dkt.nnz);
-  const int vd = vector_width(p.dk.rows, p.dk.nnz);
-  const size_t case_smem = case_chunk_smem(m, n, sizeof(T));
-  const bool use_resident = !slow && K >= 2 && o.resident && !averaging &&
-                            case_chunk_eligible<T>(vp, vd, case_smem);
   // One fast-path iteration (in place).
   auto launch_iteration = [&](int it, uint32_t flags) {
     PrimalEpi<T> pe{K, it, flags, w.params.p, w.w_table.p, w.x.p, w.x.p, w.c.p, w.lo.p, w.hi.p,
                     w.x_bar.p, w.anchor_x.p, w.dx.p, w.sum_x.p};
-    product<T, T, T>(p, p.dkt, w.y.p, K, pe);
+    product<T, T, T>(p, p.dkt, w.y.p, K, pe, true);
     DualEpi<T> de{K, it, flags, p.num_eq, w.params.p, w.w_table.p, w.y.p, w.y.p, w.q.p, w.kx.p,
                   w.kx.p, w.anchor_y.p, w.anchor_kx.p, w.dy.p, nullptr, w.sum_y.p, ylo_ptr};
-    product<T, T, T>(p, p.dk, w.x_bar.p, K, de);
+    product<T, T, T>(p, p.dk, w.x_bar.p, K, de, true);
   };
 
   auto run_chunk_body = [&](int len, bool check_at_end) {
     const uint32_t base_flags = averaging ? kAccumulate : 0u;
-    if (use_resident) {
-      CaseChunkArgs<T> A;
-      A.kt = p.dkt.view<T>();
-      A.k = p.dk.view<T>();
-      A.K = K;
-      A.m = m;
-      A.n = n;
-      A.num_eq = p.num_eq;
-      A.len = len;
-      A.flags_last = check_at_end ? kWriteDelta : 0u;
-      A.params = w.params.p;
-      A.x = w.x.p;
-      A.c = w.c.p;
-      A.lo = w.lo.p;
-      A.hi = w.hi.p;
-      A.anchor_x = w.anchor_x.p;
-      A.dx = w.dx.p;
-      A.y = w.y.p;
-      A.q = w.q.p;
-      A.kx = w.kx.p;
-      A.anchor_y = w.anchor_y.p;
-      A.anchor_kx = w.anchor_kx.p;
-      A.dy = w.dy.p;
-      A.ylo = ylo_ptr;
-      launch_case_chunk<T>(A, vp, vd, case_smem, st);
-      p.launches += 1;
-      return;
-    }
     if (o.use_graphs) {
       const auto key = std::make_pair(len, check_at_end ? 1 : 0);
       auto found = w.graphs.find(key);
@@ -1878,7 +1770,6 @@ void anu_pdhg_default_options(anu_pdhg_options* o) {
   o->device = 0;
   o->use_graphs = 1;
   o->profile = 0;
-  o->resident = 1;
 }
 
 int anu_last_error(char* buf, int32_t size) { return anu::copy_last_error(buf, size); }

@@ -55,6 +55,16 @@ __device__ __forceinline__ float madd(float acc, float a, float b) { return fmaf
 
 template <class T> __device__ __forceinline__ T load(const T* p) { return __ldg(p); }
 
+// Programmatic dependent launch. A kernel launched with programmatic stream
+// serialisation may start while its predecessor drains; it must not touch
+// the predecessor's output before pdl_wait(), and it lets its own successor
+// start only after that wait, so anything two launches back is complete when
+// a kernel starts. Outside such a launch both are no-ops.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_launch() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // -------------------------------------------------------------- matrices
 
 struct RowBlockDev {
@@ -109,6 +119,12 @@ template <class Out>
 struct StoreEpi {
   int32_t K;
   Out* __restrict__ out;
+  struct Pre {};
+  __device__ __forceinline__ Pre prefetch(int32_t, int32_t) const { return Pre{}; }
+  template <class Acc>
+  __device__ __forceinline__ void finish(int32_t r, int32_t k, Acc s, const Pre&) const {
+    out[(size_t)r * K + k] = static_cast<Out>(s);
+  }
   template <class Acc>
   __device__ __forceinline__ void operator()(int32_t r, int32_t k, Acc s) const {
     out[(size_t)r * K + k] = static_cast<Out>(s);
@@ -136,16 +152,34 @@ struct PrimalEpi {
   T* __restrict__ dx;
   T* __restrict__ sum_x;
 
-  __device__ __forceinline__ void operator()(int32_t j, int32_t k, T kty) const {
+  // The column's vectors the step reads besides (K'y)_j, loaded before the
+  // kernel waits on the product's input. The per-case parameters stay in L1
+  // and are read again in finish().
+  struct Pre {
+    T x, c, lo, hi, anchor, sum;
+  };
+  __device__ __forceinline__ Pre prefetch(int32_t j, int32_t k) const {
+    Pre r;
+    const StepParams& P = p[k];
+    if (!P.active) return r;
+    const size_t e = (size_t)j * K + k;
+    r.x = x_in[e];
+    r.c = c[e];
+    r.lo = lo[e];
+    r.hi = hi[e];
+    const bool blend = P.halpern && !(P.reset_pending && it == 0);
+    r.anchor = blend ? anchor[e] : static_cast<T>(0);
+    r.sum = (flags & kAccumulate) ? sum_x[e] : static_cast<T>(0);
+    return r;
+  }
+  __device__ __forceinline__ void finish(int32_t j, int32_t k, T kty, const Pre& r) const {
     const StepParams& P = p[k];
     if (!P.active) return;
     const size_t e = (size_t)j * K + k;
-    const T xj = x_in[e];
-    T v = sub(xj, mul(static_cast<T>(P.tau), sub(c[e], kty)));
-    const T l = lo[e];
-    const T u = hi[e];
-    if (v < l) v = l;
-    if (v > u) v = u;
+    const T xj = r.x;
+    T v = sub(xj, mul(static_cast<T>(P.tau), sub(r.c, kty)));
+    if (v < r.lo) v = r.lo;
+    if (v > r.hi) v = r.hi;
     const T d = sub(v, xj);
     if (flags & kWriteDelta) dx[e] = d;
     x_bar[e] = add(v, d);
@@ -154,11 +188,14 @@ struct PrimalEpi {
     const bool reset_now = P.reset_pending && it == 0;
     if (P.halpern && !reset_now) {
       const double w = w_table[(size_t)it * K + k];
-      next = add(mul(static_cast<T>(w), next), mul(static_cast<T>(1.0 - w), anchor[e]));
+      next = add(mul(static_cast<T>(w), next), mul(static_cast<T>(1.0 - w), r.anchor));
     }
     x_out[e] = next;
     if (P.halpern && reset_now) anchor[e] = next;
-    if (flags & kAccumulate) sum_x[e] = add(sum_x[e], mul(static_cast<T>(P.eta), next));
+    if (flags & kAccumulate) sum_x[e] = add(r.sum, mul(static_cast<T>(P.eta), next));
+  }
+  __device__ __forceinline__ void operator()(int32_t j, int32_t k, T kty) const {
+    finish(j, k, kty, prefetch(j, k));
   }
 };
 
@@ -188,17 +225,33 @@ struct DualEpi {
   T* __restrict__ sum_y;
   const T* __restrict__ ylo;  // may be null (zero)
 
-  __device__ __forceinline__ void operator()(int32_t i, int32_t k, T bar) const {
+  // The row's vectors, loaded before the kernel waits on the product's input.
+  struct Pre {
+    T y, q, kx, anchor_y, anchor_kx, floor_v, sum;
+  };
+  __device__ __forceinline__ Pre prefetch(int32_t i, int32_t k) const {
+    Pre r;
+    const StepParams& P = p[k];
+    if (!P.active) return r;
+    const size_t e = (size_t)i * K + k;
+    r.y = y_in[e];
+    r.q = q[e];
+    r.kx = kx_in[e];
+    r.floor_v = (i >= num_eq && ylo) ? ylo[e] : static_cast<T>(0);
+    const bool blend = P.halpern && !(P.reset_pending && it == 0);
+    r.anchor_y = blend ? anchor_y[e] : static_cast<T>(0);
+    r.anchor_kx = blend ? anchor_kx[e] : static_cast<T>(0);
+    r.sum = (flags & kAccumulate) ? sum_y[e] : static_cast<T>(0);
+    return r;
+  }
+  __device__ __forceinline__ void finish(int32_t i, int32_t k, T bar, const Pre& r) const {
     const StepParams& P = p[k];
     if (!P.active) return;
     const size_t e = (size_t)i * K + k;
-    const T yi = y_in[e];
-    const T kx = kx_in[e];
-    T v = add(yi, mul(static_cast<T>(P.sigma), sub(q[e], bar)));
-    if (i >= num_eq) {
-      const T floor_v = ylo ? ylo[e] : static_cast<T>(0);
-      if (v < floor_v) v = floor_v;
-    }
+    const T yi = r.y;
+    const T kx = r.kx;
+    T v = add(yi, mul(static_cast<T>(P.sigma), sub(r.q, bar)));
+    if (i >= num_eq && v < r.floor_v) v = r.floor_v;
     const T d = sub(v, yi);
     const T kd = mul(static_cast<T>(0.5), sub(bar, kx));
     if (flags & kWriteDelta) {
@@ -216,8 +269,8 @@ struct DualEpi {
       const double w = w_table[(size_t)it * K + k];
       const T wt = static_cast<T>(w);
       const T wc = static_cast<T>(1.0 - w);
-      next_y = add(mul(wt, next_y), mul(wc, anchor_y[e]));
-      next_k = add(mul(wt, next_k), mul(wc, anchor_kx[e]));
+      next_y = add(mul(wt, next_y), mul(wc, r.anchor_y));
+      next_k = add(mul(wt, next_k), mul(wc, r.anchor_kx));
     }
     y_out[e] = next_y;
     kx_out[e] = next_k;
@@ -225,7 +278,10 @@ struct DualEpi {
       anchor_y[e] = next_y;
       anchor_kx[e] = next_k;
     }
-    if (flags & kAccumulate) sum_y[e] = add(sum_y[e], mul(static_cast<T>(P.eta), next_y));
+    if (flags & kAccumulate) sum_y[e] = add(r.sum, mul(static_cast<T>(P.eta), next_y));
+  }
+  __device__ __forceinline__ void operator()(int32_t i, int32_t k, T bar) const {
+    finish(i, k, bar, prefetch(i, k));
   }
 };
 
@@ -337,7 +393,9 @@ __global__ void __launch_bounds__(kThreads) cases_kernel(CsrView<V> a, const X* 
 template <class V, class X, class Acc, class Epi, int L, int CPL>
 __global__ void __launch_bounds__(kThreads) seg_kernel(CsrView<V> a, const X* __restrict__ x,
                                                         int32_t K, Epi epi) {
-  constexpr int kGroups = kThreads / L;
+  constexpr int kGroups = kThreads / L;  // >= kSegPerCta: one segment per group
+  constexpr int kPrefetch = 2;           // epilogue items prefetched per thread
+  static_assert(kGroups >= kSegPerCta, "one segment per lane group");
   __shared__ Acc part[kSegPerCta][kMaxCaseLanes];
   const int32_t cta = blockIdx.x;
   const int32_t r0 = a.cta_row[cta];
@@ -346,53 +404,78 @@ __global__ void __launch_bounds__(kThreads) seg_kernel(CsrView<V> a, const X* __
   const int32_t s1 = a.cta_seg[cta + 1];
   const int group = threadIdx.x / L;
   const int lane = threadIdx.x % L;
-  for (int32_t sb = s0; sb < s1; sb += kGroups) {
-    const int32_t sg = sb + group;
-    const bool active = sg < s1;
-    const int32_t b = active ? a.seg_begin[sg] : 0;
-    const int32_t e = active ? a.seg_begin[sg + 1] : 0;
-    Acc acc[CPL];
+  // ---- independent of the previous launch: the schedule, this group's
+  // first indices and values, and the epilogue's own vectors.
+  const int32_t sg = s0 + group;
+  const bool active = sg < s1;
+  const int32_t b = active ? a.seg_begin[sg] : 0;
+  const int32_t e = active ? a.seg_begin[sg + 1] : 0;
+  const int32_t len = e - b;
+  int32_t idx0 = 0;
+  Acc val0 = 0;
+  if (lane < len) {
+    idx0 = a.index[b + lane];
+    val0 = static_cast<Acc>(a.value[b + lane]);
+  }
+  const int32_t items = (r1 - r0) * K;
+  typename Epi::Pre pre[kPrefetch];
 #pragma unroll
-    for (int c = 0; c < CPL; ++c) acc[c] = 0;
-    // Every lane of the warp walks the warp's longest segment so the
-    // shuffles below see full participation.
-    const int32_t len = e - b;
-    const int32_t warp_len = __reduce_max_sync(0xffffffffu, static_cast<unsigned>(len));
-    for (int32_t base = 0; base < warp_len; base += L) {
-      int32_t idx = 0;
-      Acc val = 0;
+  for (int q = 0; q < kPrefetch; ++q) {
+    const int32_t t = threadIdx.x + q * kThreads;
+    if (t < items) pre[q] = epi.prefetch(r0 + t / K, t % K);
+  }
+  // ---- the gather reads the previous launch's output.
+  pdl_wait();
+  pdl_launch();
+  Acc acc[CPL];
+#pragma unroll
+  for (int c = 0; c < CPL; ++c) acc[c] = 0;
+  const int32_t warp_len = __reduce_max_sync(0xffffffffu, static_cast<unsigned>(len));
+  for (int32_t base = 0; base < warp_len; base += L) {
+    int32_t idx = idx0;
+    Acc val = val0;
+    if (base > 0) {
+      idx = 0;
+      val = 0;
       if (base + lane < len) {
         idx = a.index[b + base + lane];
         val = static_cast<Acc>(a.value[b + base + lane]);
       }
-      const int32_t cnt = min(L, warp_len - base);
+    }
+    const int32_t cnt = min(L, warp_len - base);
 #pragma unroll 8
-      for (int t = 0; t < cnt; ++t) {
-        const int32_t col = __shfl_sync(0xffffffffu, idx, t, L);
-        const Acc v = __shfl_sync(0xffffffffu, val, t, L);
-        if (base + t < len) {
-          const X* xc = x + (size_t)col * K;
+    for (int t = 0; t < cnt; ++t) {
+      const int32_t col = __shfl_sync(0xffffffffu, idx, t, L);
+      const Acc v = __shfl_sync(0xffffffffu, val, t, L);
+      if (base + t < len) {
+        const X* xc = x + (size_t)col * K;
 #pragma unroll
-          for (int c = 0; c < CPL; ++c) {
-            const int32_t cs = lane + c * L;
-            if (cs < K) acc[c] = madd(acc[c], v, static_cast<Acc>(xc[cs]));
-          }
+        for (int c = 0; c < CPL; ++c) {
+          const int32_t cs = lane + c * L;
+          if (cs < K) acc[c] = madd(acc[c], v, static_cast<Acc>(xc[cs]));
         }
       }
     }
-    if (active) {
+  }
+  if (active) {
 #pragma unroll
-      for (int c = 0; c < CPL; ++c) part[sg - s0][lane + c * L] = acc[c];
-    }
+    for (int c = 0; c < CPL; ++c) part[sg - s0][lane + c * L] = acc[c];
   }
   __syncthreads();
-  const int32_t items = (r1 - r0) * K;
-  for (int32_t it = threadIdx.x; it < items; it += kThreads) {
-    const int32_t row = r0 + it / K;
-    const int32_t k = it % K;
+  for (int32_t t = threadIdx.x, q = 0; t < items; t += kThreads, ++q) {
+    const int32_t row = r0 + t / K;
+    const int32_t k = t % K;
     Acc sum = 0;
-    for (int32_t sg = a.row_seg[row]; sg < a.row_seg[row + 1]; ++sg) sum = add(sum, part[sg - s0][k]);
-    epi(row, k, sum);
+    for (int32_t g = a.row_seg[row]; g < a.row_seg[row + 1]; ++g) sum = add(sum, part[g - s0][k]);
+    if (q < kPrefetch) {
+      typename Epi::Pre r;
+#pragma unroll
+      for (int qq = 0; qq < kPrefetch; ++qq)
+        if (qq == q) r = pre[qq];
+      epi.finish(row, k, sum, r);
+    } else {
+      epi.finish(row, k, sum, epi.prefetch(row, k));
+    }
   }
 }
 

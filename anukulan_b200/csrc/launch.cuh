@@ -30,15 +30,27 @@ inline int grid_for(int64_t items, int per_block, int cap) {
 
 // y = A x (any epilogue) for K cases.
 template <class V, class X, class Acc, class Epi, class Mat>
-void product(Exec& p, const Mat& a, const X* x, int K, const Epi& epi) {
+void product(Exec& p, const Mat& a, const X* x, int K, const Epi& epi, bool pdl = false) {
   if (a.rows == 0) return;
   cudaStream_t s = p.stream;
   if (K == 1) {
     rows_kernel<V, X, Acc, Epi><<<a.num_blocks, kThreads, 0, s>>>(a.template view<V>(), x, epi);
   } else {
-#define ANU_CASES(L_, CPL_)                                                                  \
-  seg_kernel<V, X, Acc, Epi, L_, CPL_>                                                       \
-      <<<a.num_ctas, kThreads, 0, s>>>(a.template view<V>(), x, K, epi)
+#define ANU_CASES(L_, CPL_)                                                              \
+  do {                                                                                   \
+    cudaLaunchConfig_t cfg = {};                                                         \
+    cfg.gridDim = dim3(a.num_ctas);                                                      \
+    cfg.blockDim = dim3(kThreads);                                                       \
+    cfg.stream = s;                                                                      \
+    cudaLaunchAttribute attr[1];                                                         \
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;                     \
+    attr[0].val.programmaticStreamSerializationAllowed = 1;                              \
+    cfg.attrs = attr;                                                                    \
+    cfg.numAttrs = pdl ? 1 : 0;                                                          \
+    cuda_check(cudaLaunchKernelEx(&cfg, seg_kernel<V, X, Acc, Epi, L_, CPL_>,            \
+                                  a.template view<V>(), x, K, epi),                      \
+               "seg_kernel launch");                                                     \
+  } while (0)
     if (K <= 4) ANU_CASES(4, 1);
     else if (K <= 8) ANU_CASES(8, 1);
     else if (K <= 16) ANU_CASES(16, 1);

@@ -159,11 +159,6 @@ typedef struct anu_pdhg_options {
    * and report their total in anu_pdhg_result::device_iteration_seconds.
    * Events do not serialise the stream. 0 = off. */
   int32_t profile;
-  /* Case stacks whose per-case iteration state fits in one CTA's shared
-   * memory run each check period as one launch with a CTA per case, the
-   * state resident in shared memory for the whole period. 0 = always use
-   * graph chunks of the two fused SpMM kernels. */
-  int32_t resident;             /* 1 */
 } anu_pdhg_options;
 
 /* PdhgResidual, src/anukulan/pdhg.hpp:429-496. */
