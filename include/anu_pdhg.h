@@ -322,8 +322,8 @@ int anu_backend_convergence_terms(int64_t n, int64_t m, const double* c,
  * No counterpart in the reference, whose solve_pdhg takes one LP. The stack
  * runs as one SpMM-shaped iteration over case-interleaved vectors: every
  * nonzero of the matrix read serves all active cases. Each case keeps its own
- * step size, primal weight, restarts and termination; a converged case is
- * retired and its slot is free for anu_pdhg_batch_admit.
+ * step size, primal weight, restarts and termination; a case that terminates
+ * is retired, and its lanes skip their updates from then on.
  *
  * Case arrays are case-major: c[k*n + j], q[k*m + i], and so on. A NULL case
  * array means every case uses the base LP's vector. */
