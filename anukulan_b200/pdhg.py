@@ -35,6 +35,7 @@ EXPORTS = (
     "anu_backend_inf_norm", "anu_backend_primal_update", "anu_backend_dual_update",
     "anu_backend_accumulate", "anu_backend_scale_into", "anu_backend_weighted_norm_squared",
     "anu_backend_step_size_terms", "anu_backend_convergence_terms",
+    "anu_backend_convergence_terms_noalloc",
     "anu_pdhg_batch_create", "anu_pdhg_batch_solve", "anu_pdhg_batch_destroy",
 )
 
@@ -104,6 +105,8 @@ def lib():
     d("anu_backend_step_size_terms", C.c_int, [i64, i64, vp, vp, vp, dbl, _P(dbl), _P(dbl)])
     d("anu_backend_convergence_terms", C.c_int, [i64, i64] + [vp] * 6 + [i64] + [vp] * 4
       + [_P(dbl)])
+    d("anu_backend_convergence_terms_noalloc", C.c_int,
+      [i64, i64] + [vp] * 6 + [i64] + [vp] * 4 + [_P(dbl)])
     _lib = L
     return L
 

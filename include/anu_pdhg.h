@@ -317,6 +317,36 @@ int anu_backend_convergence_terms(int64_t n, int64_t m, const double* c,
                                   const double* y, const double* kt_y,
                                   double* out);                   /* backend.hpp:198-202 */
 
+/* anu_backend_convergence_terms without any device allocation. There is no
+ * counterpart in the reference.
+ *
+ * It is for hosts that may not call cudaMalloc: a plugin inside an application
+ * that owns the device memory pool, a process whose allocations all go
+ * through another runtime's allocator, or code that runs while such an
+ * application holds a stream capture. The caller passes inputs and outputs
+ * exactly as for anu_backend_convergence_terms and gets the same 7 terms.
+ *
+ * - Scratch: the partial sums live in one fixed array in the library's device
+ *   image, 42,768 bytes, which every GPU that loads the library holds until
+ *   the process exits.
+ * - Limits: n and m up to 2^31-1. Larger or negative lengths return
+ *   ANU_ERR_INVALID with a message.
+ * - Set-up: the first call on each device looks the array up on that device
+ *   (cudaGetSymbolAddress). Make that first call before any stream capture
+ *   begins.
+ * - Stream: work runs on the legacy default stream, and the call returns when
+ *   it is done.
+ * - Sharing: every call shares the one array. Calls that overlap on the same
+ *   GPU (from several host threads, say) race on it and must be serialised by
+ *   the caller. */
+int anu_backend_convergence_terms_noalloc(int64_t n, int64_t m, const double* c,
+                                          const double* lower, const double* upper,
+                                          const double* q, const double* row_scale,
+                                          const double* col_scale,
+                                          int64_t num_equalities, const double* x,
+                                          const double* k_x, const double* y,
+                                          const double* kt_y, double* out);
+
 /* ------------------------------------------------------ batched case stack
  * K cases that share K (the matrix) and differ in c, q, lower and upper.
  * No counterpart in the reference, whose solve_pdhg takes one LP. The stack
