@@ -80,7 +80,8 @@ void DevCsr::upload(const HostCsr& a, bool with_fp32, cudaStream_t s) {
   num_blocks = static_cast<int32_t>(b.size());
   blocks.alloc(std::max<size_t>(b.size(), 1));
   std::vector<RowBlockDev> bd(b.size());
-  for (size_t i = 0; i < b.size(); ++i) bd[i] = {b[i].row_begin, b[i].row_end};
+  for (size_t i = 0; i < b.size(); ++i)
+    bd[i] = {b[i].row_begin, b[i].row_end, a.start[b[i].row_begin], a.start[b[i].row_end]};
   if (!bd.empty())
     ANU_CUDA(cudaMemcpyAsync(blocks.p, bd.data(), sizeof(RowBlockDev) * bd.size(),
                              cudaMemcpyHostToDevice, s));

@@ -4,20 +4,20 @@
 //
 //  * rows_kernel - one LP. CSR-adaptive: each CTA takes one row block (a run
 //    of consecutive rows holding at most kBlockNnz nonzeros, or one longer
-//    row). The block's value*x products are streamed into shared memory with
+//    row). The block's value*x products are staged into shared memory with
 //    coalesced loads of the index and value arrays, summed per row (one
-//    thread per row while rows are short, a shuffle group when they are long,
-//    a CTA-wide tree for a row longer than the block), and the row sums feed
+//    thread per short row, a warp per long row, a CTA-wide tree for a row
+//    longer than the block), and the row sums feed
 //    an epilogue over the block's rows - contiguous, so the epilogue's vector
 //    traffic is coalesced too. The epilogue is where the PDHG step is fused:
 //    the primal step, bound projection, reflection and Halpern blend after
 //    K'y, the dual step, cone projection and K x bookkeeping after K x_bar.
 //
-//  * cases_kernel - a case stack of K LPs sharing A, vectors case-interleaved
-//    (element (row, case) at row*K + case). A group of L lanes takes a row;
-//    lane l owns cases l, l+L, ... Every nonzero of A is loaded once per row
-//    group and serves all K cases; the x loads of the K cases are one
-//    contiguous run. Each (row, case) sum is accumulated left to right.
+//  * seg_kernel - a case stack of K LPs sharing A, vectors case-interleaved
+//    (element (row, case) at row*K + case). Rows are cut into segments of a
+//    few nonzeros; a group of lanes takes a segment, and lane l owns cases
+//    l, l+L, ... Every nonzero of A is loaded once per segment and serves
+//    all K cases; the x loads of the K cases are one contiguous run.
 //
 // Sums are deterministic: the order depends only on the row-block schedule,
 // never on timing. FP64 arithmetic in the epilogues and sums is written with
@@ -32,8 +32,11 @@
 namespace anu {
 
 constexpr int kThreads = 256;
-constexpr int kBlockNnz = 2048;
-constexpr int kBlockRows = 256;
+// Single-LP product: threads per CTA, and the most nonzeros and rows a row
+// block holds.
+constexpr int kRowThreads = 128;
+constexpr int kBlockNnz = 1024;
+constexpr int kBlockRows = 128;
 // Case-stack product: nonzeros per segment, segments per CTA, rows per CTA,
 // and the most cases one launch carries.
 constexpr int kSegNnz = 16;
@@ -70,6 +73,8 @@ __device__ __forceinline__ void pdl_launch() {
 struct RowBlockDev {
   int32_t row_begin;
   int32_t row_end;
+  int32_t nz_begin;  // start[row_begin], stored so a CTA's first index load
+  int32_t nz_end;    // does not wait on a load of start[]
 };
 
 template <class V>
@@ -287,12 +292,12 @@ struct DualEpi {
 
 // ------------------------------------------------------- block reductions
 
-template <class Acc>
+template <int kWidth, class Acc>
 __device__ __forceinline__ Acc block_sum(Acc v, Acc* scratch) {
-  // Deterministic tree over the CTA.
+  // Deterministic tree over a CTA of kWidth threads.
   scratch[threadIdx.x] = v;
   __syncthreads();
-  for (int s = kThreads / 2; s > 0; s >>= 1) {
+  for (int s = kWidth / 2; s > 0; s >>= 1) {
     if (threadIdx.x < s) scratch[threadIdx.x] = add(scratch[threadIdx.x], scratch[threadIdx.x + s]);
     __syncthreads();
   }
@@ -303,80 +308,126 @@ __device__ __forceinline__ Acc block_sum(Acc v, Acc* scratch) {
 
 // ----------------------------------------------------------- rows_kernel
 
+// One LP, one row block per CTA. Each thread first loads its share of the
+// block's indices and values into registers (kPerThread of each, all issued
+// before any is used), together with the epilogue's vectors for its row;
+// none of that depends on the previous launch, so under programmatic
+// dependent launch it overlaps the predecessor's tail. After the wait it
+// gathers x for all its nonzeros at once and stores the products in shared
+// memory. Rows of at most kSerialRow nonzeros are then summed by their own
+// thread, left to right from zero - the reference's order, so FP64 sums of
+// short rows match it bit for bit. Longer rows are listed in row order and
+// taken by whole warps (lane-strided partial sums, then a fixed shuffle
+// tree). A row longer than the block has a CTA to itself.
+constexpr int kSerialRow = 32;
+constexpr int kPerThread = kBlockNnz / kRowThreads;
+static_assert(kBlockRows <= kRowThreads, "one epilogue row per thread");
+static_assert(kBlockNnz >= kRowThreads, "block_sum scratch");
+
 template <class V, class X, class Acc, class Epi>
-__global__ void __launch_bounds__(kThreads) rows_kernel(CsrView<V> a, const X* __restrict__ x,
-                                                         Epi epi) {
+__global__ void __launch_bounds__(kRowThreads)
+    rows_kernel(CsrView<V> a, const X* __restrict__ x, Epi epi) {
+  constexpr int kWarps = kRowThreads / 32;
   __shared__ Acc prod[kBlockNnz];
   __shared__ Acc rowsum[kBlockRows];
+  __shared__ int32_t long_rows[kBlockRows];
+  __shared__ int32_t warp_long[kWarps];
   const RowBlockDev blk = a.blocks[blockIdx.x];
   const int32_t r0 = blk.row_begin;
   const int32_t nrows = blk.row_end - r0;
-  const int32_t nz0 = a.start[r0];
-  const int32_t nnz = a.start[blk.row_end] - nz0;
+  const int32_t nz0 = blk.nz_begin;
+  const int32_t nnz = blk.nz_end - nz0;
+  const int t = threadIdx.x;
   if (nnz > kBlockNnz) {
-    // One long row: strided partial sums, then a fixed-order tree.
+    // One long row: strided partial sums (k = t, t + kRowThreads, ...), then
+    // a fixed-order tree over the CTA.
+    typename Epi::Pre pre{};
+    if (t == 0) pre = epi.prefetch(r0, 0);
+    pdl_wait();
+    pdl_launch();
     Acc s = 0;
-    for (int32_t k = nz0 + threadIdx.x; k < nz0 + nnz; k += kThreads)
-      s = madd(s, static_cast<Acc>(a.value[k]), static_cast<Acc>(x[a.index[k]]));
-    s = block_sum(s, prod);
-    if (threadIdx.x == 0) epi(r0, 0, s);
+    const int32_t end = nz0 + nnz;
+    for (int32_t base = nz0; base < end; base += kRowThreads * kPerThread) {
+      int32_t col[kPerThread];
+      Acc val[kPerThread];
+#pragma unroll
+      for (int q = 0; q < kPerThread; ++q) {
+        const int32_t k = base + q * kRowThreads + t;
+        col[q] = k < end ? a.index[k] : -1;
+        val[q] = k < end ? static_cast<Acc>(a.value[k]) : static_cast<Acc>(0);
+      }
+      Acc xv[kPerThread];
+#pragma unroll
+      for (int q = 0; q < kPerThread; ++q)
+        xv[q] = col[q] >= 0 ? static_cast<Acc>(x[col[q]]) : static_cast<Acc>(0);
+#pragma unroll
+      for (int q = 0; q < kPerThread; ++q)
+        if (col[q] >= 0) s = madd(s, val[q], xv[q]);
+    }
+    s = block_sum<kRowThreads>(s, prod);
+    if (t == 0) epi.finish(r0, 0, s, pre);
     return;
   }
-  for (int32_t k = threadIdx.x; k < nnz; k += kThreads)
-    prod[k] = mul(static_cast<Acc>(a.value[nz0 + k]), static_cast<Acc>(x[a.index[nz0 + k]]));
-  __syncthreads();
-  // Lanes per row: one while rows average at most 32 nonzeros (a serial sum
-  // over shared memory, the reference's own order), else a shuffle group.
-  int g = 1;
-  if (nrows > 0 && nnz > 32 * nrows) {
-    g = 32;
-    while (g > 1 && g * nrows > kThreads) g >>= 1;
+  // ---- independent of the previous launch
+  int32_t col[kPerThread];
+  V val[kPerThread];
+#pragma unroll
+  for (int q = 0; q < kPerThread; ++q) {
+    const int32_t k = q * kRowThreads + t;
+    col[q] = k < nnz ? a.index[nz0 + k] : -1;
+    val[q] = k < nnz ? a.value[nz0 + k] : static_cast<V>(0);
   }
-  const int32_t row = threadIdx.x / g;
-  const int lane = threadIdx.x % g;
-  Acc s = 0;
-  if (row < nrows) {
+  const bool has_row = t < nrows;
+  int32_t rb = 0, re = 0;
+  typename Epi::Pre pre{};
+  if (has_row) {
+    rb = a.start[r0 + t] - nz0;
+    re = a.start[r0 + t + 1] - nz0;
+    pre = epi.prefetch(r0 + t, 0);
+  }
+  // ---- the gather reads the previous launch's output
+  pdl_wait();
+  pdl_launch();
+  Acc xv[kPerThread];
+#pragma unroll
+  for (int q = 0; q < kPerThread; ++q)
+    xv[q] = col[q] >= 0 ? static_cast<Acc>(x[col[q]]) : static_cast<Acc>(0);
+#pragma unroll
+  for (int q = 0; q < kPerThread; ++q)
+    if (col[q] >= 0) prod[q * kRowThreads + t] = mul(static_cast<Acc>(val[q]), xv[q]);
+  __syncthreads();
+  const bool is_long = has_row && re - rb > kSerialRow;
+  if (has_row && !is_long) {
+    Acc s = 0;
+    for (int32_t k = rb; k < re; ++k) s = add(s, prod[k]);
+    rowsum[t] = s;
+  }
+  const int warp = t / 32;
+  const int lane = t % 32;
+  const unsigned ballot = __ballot_sync(0xffffffffu, is_long);
+  if (lane == 0) warp_long[warp] = __popc(ballot);
+  __syncthreads();
+  int32_t before = 0, nlong = 0;
+#pragma unroll
+  for (int w = 0; w < kWarps; ++w) {
+    const int32_t c = warp_long[w];
+    if (w < warp) before += c;
+    nlong += c;
+  }
+  if (is_long) long_rows[before + __popc(ballot & ((1u << lane) - 1u))] = t;
+  __syncthreads();
+  for (int32_t i = warp; i < nlong; i += kWarps) {
+    const int32_t row = long_rows[i];
     const int32_t b = a.start[r0 + row] - nz0;
     const int32_t e = a.start[r0 + row + 1] - nz0;
-    for (int32_t k = b + lane; k < e; k += g) s = add(s, prod[k]);
+    Acc s = 0;
+    for (int32_t k = b + lane; k < e; k += 32) s = add(s, prod[k]);
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) s = add(s, __shfl_down_sync(0xffffffffu, s, off));
+    if (lane == 0) rowsum[row] = s;
   }
-  for (int off = g >> 1; off > 0; off >>= 1) s = add(s, __shfl_down_sync(0xffffffffu, s, off));
-  if (lane == 0 && row < nrows) rowsum[row] = s;
   __syncthreads();
-  for (int32_t t = threadIdx.x; t < nrows; t += kThreads) epi(r0 + t, 0, rowsum[t]);
-}
-
-// ---------------------------------------------------------- cases_kernel
-
-// L lanes per row group (power of two, <= 32); CPL cases per lane.
-template <class V, class X, class Acc, class Epi, int L, int CPL>
-__global__ void __launch_bounds__(kThreads) cases_kernel(CsrView<V> a, const X* __restrict__ x,
-                                                          int32_t K, Epi epi) {
-  constexpr int kGroups = kThreads / L;
-  const int group = threadIdx.x / L;
-  const int lane = threadIdx.x % L;
-  for (int32_t row = blockIdx.x * kGroups + group; row < a.rows; row += gridDim.x * kGroups) {
-    Acc acc[CPL];
-#pragma unroll
-    for (int c = 0; c < CPL; ++c) acc[c] = 0;
-    const int32_t b = a.start[row];
-    const int32_t e = a.start[row + 1];
-    for (int32_t k = b; k < e; ++k) {
-      const int32_t col = a.index[k];
-      const Acc v = static_cast<Acc>(a.value[k]);
-      const X* xc = x + (size_t)col * K;
-#pragma unroll
-      for (int c = 0; c < CPL; ++c) {
-        const int32_t cs = lane + c * L;
-        if (cs < K) acc[c] = madd(acc[c], v, static_cast<Acc>(xc[cs]));
-      }
-    }
-#pragma unroll
-    for (int c = 0; c < CPL; ++c) {
-      const int32_t cs = lane + c * L;
-      if (cs < K) epi(row, cs, acc[c]);
-    }
-  }
+  if (has_row) epi.finish(r0 + t, 0, rowsum[t], pre);
 }
 
 // ------------------------------------------------------------ seg_kernel

@@ -34,7 +34,17 @@ void product(Exec& p, const Mat& a, const X* x, int K, const Epi& epi, bool pdl 
   if (a.rows == 0) return;
   cudaStream_t s = p.stream;
   if (K == 1) {
-    rows_kernel<V, X, Acc, Epi><<<a.num_blocks, kThreads, 0, s>>>(a.template view<V>(), x, epi);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(a.num_blocks);
+    cfg.blockDim = dim3(kRowThreads);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = pdl ? 1 : 0;
+    cuda_check(cudaLaunchKernelEx(&cfg, rows_kernel<V, X, Acc, Epi>, a.template view<V>(), x, epi),
+               "rows_kernel launch");
   } else {
 #define ANU_CASES(L_, CPL_)                                                              \
   do {                                                                                   \

@@ -10,7 +10,17 @@ on the device; `e2e` is the same metric through the C ABI from host arrays
 (create + solve + download inside the timed region).
 
     python bench.py [--gpus N --steps K --warmup W] [--impl reference]
-                    [--workload stack|large]
+                    [--workload stack|spmv]
+
+Two side measurements ride on the stack line:
+  * `spmv`: the single-LP iteration (the two fused SpMV kernels) on the
+    200,000 x 300,000 power-law LP (2.4M nonzeros), FP32 and FP64, timed over
+    a fixed number of iterations with CUDA events - per-iteration time,
+    iterations/s and algorithmic GB/s against the measured HBM peak.
+    `--workload spmv` runs this leg alone (for profiling).
+  * `fp64_single_case`: the same 60 cases solved one at a time by the
+    engine's plain FP64 mode - the plain FP64 single-case GPU PDHG the batched
+    mixed-precision run is compared with.
 
 Under torchrun every rank solves its own copy of the stack (weak scaling, no
 collective on the data path); rank 0 prints one JSON line. `--impl reference`
@@ -125,6 +135,52 @@ def flush_l2(torch, buf):
     buf.zero_()
 
 
+def spmv_leg(iterations, device, peak):
+    """Per-iteration time of the single-LP path on the power-law LP: two fused
+    SpMV + step kernels per iteration, graph-captured, timed by the engine's
+    CUDA events around every iteration chunk (`profile`)."""
+    from anukulan_b200 import lpgen, pdhg
+    from anukulan_b200.abi import PRECISION_FP32, PRECISION_FP64, make_options
+    lp, _ = lpgen.power_law_lp()
+    m, n, nnz = lp.num_rows, lp.num_cols, lp.k.nnz
+    out = {"workload": "powerlaw_lp", "rows": m, "cols": n, "nnz": nnz,
+           "row_length_max": int(lp.k.row_lengths().max()), "iterations": iterations,
+           "peak_GBps": peak,
+           "note": "algorithmic bytes = 2 nnz (s_a + 4) + 4 (m + n + 2) + s_x (8n + 7m); "
+                   "each gathered x or y element also moves a 32-byte sector through L1"}
+    for name, prec, size in (("fp32", PRECISION_FP32, 4), ("fp64", PRECISION_FP64, 8)):
+        opts = make_options(tolerance=1e-12, precision=prec, max_iterations=iterations,
+                            profile=1, polish_feasibility=0, polish_on_exit=0, device=device)
+        r = pdhg.solve_pdhg(lp, opts)
+        per_it = r.device_iteration_seconds / max(r.device_iterations, 1)
+        b = algorithmic_bytes_per_iteration(nnz, m, n, 1, size, size)
+        out[name] = {"us_per_iteration": per_it * 1e6, "iterations_per_second": 1.0 / per_it,
+                     "algorithmic_bytes_per_iteration": b,
+                     "achieved_GBps": b / per_it / 1e9, "frac": b / per_it / 1e9 / peak,
+                     "kernel_launches": int(r.kernel_launches)}
+    return out
+
+
+def fp64_single_case(st, device):
+    """The stack's cases solved one after another by the engine's plain FP64
+    single-case mode (host arrays in, results out, like a solve_pdhg call)."""
+    from anukulan_b200 import pdhg
+    from anukulan_b200.abi import OPTIMAL, PRECISION_FP64, make_options
+    opts = make_options(tolerance=TOL, precision=PRECISION_FP64, device=device)
+    pdhg.solve_pdhg(st.case(0), opts)  # warm-up: context, module load
+    t0 = time.perf_counter()
+    ok = 0
+    iters = 0
+    for k in range(st.num_cases):
+        r = pdhg.solve_pdhg(st.case(k), opts)
+        ok += int(r.status == OPTIMAL)
+        iters += r.iterations
+    dt = time.perf_counter() - t0
+    return {"value": ok / dt, "unit": "solves/s", "cases": st.num_cases, "optimal": ok,
+            "seconds": dt, "iterations_per_second": iters / dt,
+            "mode": "engine FP64, one case per solve, no batching"}
+
+
 # -------------------------------------------------------------- our arm
 
 def run_engine(args, rank, world, local_rank):
@@ -155,6 +211,7 @@ def run_engine(args, rank, world, local_rank):
     clocks = ClockSampler(local_rank)
     clocks.start()
     step_ms = []
+    phases = []
     dev_iter_s = 0.0
     dev_iters = 0
     launches = 0
@@ -171,6 +228,7 @@ def run_engine(args, rank, world, local_rank):
         e1.record()
         torch.cuda.synchronize()
         step_ms.append(e0.elapsed_time(e1))
+        phases.append(res[0].phases)
         solved += sum(1 for r in res if r.status == OPTIMAL)
         dev_iter_s += res[0].device_iteration_seconds
         dev_iters += res[0].device_iterations
@@ -233,17 +291,23 @@ def run_engine(args, rank, world, local_rank):
             "cases_optimal": solved_all,
             "cases_attempted": cases_all,
             "iterations_per_solve": total_iterations / args.steps,
+            "step_ms": [round(v, 2) for v in step_ms],
+            "phases_ms_median": {k: round(1e3 * float(np.median([ph[k] for ph in phases])), 2)
+                                 for k in phases[0]},
             "e2e": {"value": solved_all / (total_e2e / 1e3), "unit": "solves/s",
                     "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None, "traffic": None,
                          "peak_source": peak_kind,
-                         "kernel": "cases_kernel (fused SpMM + primal/dual step), mean per launch",
+                         "kernel": "seg_kernel (fused case-stack SpMM + primal/dual step), mean per launch",
                          "algorithmic_bytes_per_launch": bytes_it / 2.0,
                          "launch_seconds": per_launch_s},
             "clocks": clk,
         }
+        if args.side:
+            out["spmv"] = spmv_leg(args.spmv_iterations, local_rank, peak)
+            out["fp64_single_case"] = fp64_single_case(st, local_rank)
         if args.cpu_baseline:
             out["cpu_baseline"] = cpu_baseline(st, seconds=args.cpu_seconds)
     if dist is not None:
@@ -325,12 +389,24 @@ def main(argv=None):
     ap.add_argument("--ref-seconds", type=float, default=10.0)
     ap.add_argument("--no-e2e", dest="e2e", action="store_false",
                     help="skip the end-to-end pass (profiling runs)")
+    ap.add_argument("--workload", default="stack", choices=["stack", "spmv"])
+    ap.add_argument("--spmv-iterations", type=int, default=2000)
+    ap.add_argument("--no-side", dest="side", action="store_false",
+                    help="skip the spmv and fp64 single-case side measurements")
     args = ap.parse_args(argv)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         out = run_reference(args, rank, world)
+    elif args.workload == "spmv":
+        out = None
+        if rank == 0:
+            import torch
+            torch.cuda.set_device(local_rank)
+            peak, kind = hbm_peak()
+            out = spmv_leg(args.spmv_iterations, local_rank, peak)
+            out["peak_source"] = kind
     else:
         out = run_engine(args, rank, world, local_rank)
     if rank == 0 and out is not None:
