@@ -111,7 +111,74 @@ CsrView<float> DevCsr::view<float>() const {
 }
 
 Problem::~Problem() {
+  // The pool, destroyed after this body, frees its blocks on this device.
+  cudaSetDevice(device);
+  if (stream) cudaStreamSynchronize(stream);
   if (owns_stream && stream) cudaStreamDestroy(stream);
+}
+
+namespace {
+thread_local MemoryPool* t_pool = nullptr;
+// Most bytes a pool keeps cached per kind; blocks beyond it are freed.
+constexpr size_t kPoolCap[2] = {size_t(4) << 30, size_t(256) << 20};
+
+size_t size_class(size_t bytes) {
+  size_t c = 256;
+  while (c < bytes) c <<= 1;
+  return c;
+}
+}  // namespace
+
+MemoryPool* current_pool() { return t_pool; }
+
+PoolScope::PoolScope(MemoryPool* pool, cudaStream_t stream) : previous_(t_pool), stream_(stream) {
+  t_pool = pool;
+}
+
+PoolScope::~PoolScope() {
+  if (stream_) cudaStreamSynchronize(stream_);
+  t_pool = previous_;
+}
+
+void* MemoryPool::get(bool pinned, size_t bytes, size_t* rounded) {
+  const size_t c = size_class(bytes);
+  *rounded = c;
+  {
+    std::lock_guard<std::mutex> g(lock_);
+    auto it = free_[pinned].find(c);
+    if (it != free_[pinned].end()) {
+      void* p = it->second;
+      free_[pinned].erase(it);
+      cached_[pinned] -= c;
+      return p;
+    }
+  }
+  void* p = nullptr;
+  const cudaError_t e = pinned ? cudaMallocHost(&p, c) : cudaMalloc(&p, c);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    throw Error(ANU_ERR_MEMORY, std::string(pinned ? "cudaMallocHost: " : "cudaMalloc: ") +
+                                    cudaGetErrorString(e));
+  }
+  return p;
+}
+
+void MemoryPool::put(bool pinned, void* p, size_t rounded) {
+  {
+    std::lock_guard<std::mutex> g(lock_);
+    if (cached_[pinned] + rounded <= kPoolCap[pinned]) {
+      free_[pinned].emplace(rounded, p);
+      cached_[pinned] += rounded;
+      return;
+    }
+  }
+  if (pinned) cudaFreeHost(p);
+  else cudaFree(p);
+}
+
+MemoryPool::~MemoryPool() {
+  for (auto& b : free_[0]) cudaFree(b.second);
+  for (auto& b : free_[1]) cudaFreeHost(b.second);
 }
 
 // ------------------------------------------------------------- launches
@@ -370,11 +437,21 @@ template <class T>
 struct Pinned {
   T* p = nullptr;
   size_t n = 0;
+  MemoryPool* pool = nullptr;
+  size_t bytes = 0;
   explicit Pinned(size_t count) : n(count) {
-    if (count) ANU_CUDA(cudaMallocHost(reinterpret_cast<void**>(&p), sizeof(T) * count));
+    if (!count) return;
+    if (MemoryPool* mp = current_pool()) {
+      p = static_cast<T*>(mp->get(true, sizeof(T) * count, &bytes));
+      pool = mp;
+      return;
+    }
+    ANU_CUDA(cudaMallocHost(reinterpret_cast<void**>(&p), sizeof(T) * count));
   }
   ~Pinned() {
-    if (p) cudaFreeHost(p);
+    if (!p) return;
+    if (pool) pool->put(true, p, bytes);
+    else cudaFreeHost(p);
   }
   Pinned(const Pinned&) = delete;
   Pinned& operator=(const Pinned&) = delete;
@@ -1656,6 +1733,7 @@ void run_cases(Problem& problem, const std::vector<const CaseData*>& cases,
                const std::vector<const std::vector<double>*>& warm_y,
                std::vector<CaseResult>* results, double start_time) {
   ANU_CUDA(cudaSetDevice(problem.device));
+  PoolScope scope(&problem.pool, problem.stream);
   if (problem.precision == ANU_PRECISION_FP32)
     run_cases_t<float>(problem, cases, options, warm_x, warm_y, results, start_time,
                        problem.unit_scaling);

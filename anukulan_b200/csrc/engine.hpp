@@ -4,7 +4,9 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -27,23 +29,75 @@ void cuda_check(cudaError_t status, const char* what);
 void set_last_error(int code, const std::string& message);
 void clear_last_error();
 
-// Device memory owned by RAII.
+// Device and pinned host blocks kept for reuse by one problem handle. A
+// solve allocates its working vectors, host staging buffers and polishing
+// sub-stacks again and again; without the pool each of those is a
+// cudaMalloc/cudaFree (or cudaMallocHost/cudaFreeHost) pair, and a free
+// waits for the whole device. Blocks are sized in powers of two. The pool
+// is consulted only inside a PoolScope, whose work all runs on the
+// problem's one stream, so a block handed from one allocation to the next
+// is ordered by that stream; the scope synchronises the stream when it
+// ends, so no copy from a pinned block is still pending when the host
+// writes into it again.
+class MemoryPool {
+ public:
+  MemoryPool() = default;
+  MemoryPool(const MemoryPool&) = delete;
+  MemoryPool& operator=(const MemoryPool&) = delete;
+  ~MemoryPool();
+  // A block of at least `bytes`; *rounded receives its size class.
+  void* get(bool pinned, size_t bytes, size_t* rounded);
+  void put(bool pinned, void* p, size_t rounded);
+
+ private:
+  std::mutex lock_;
+  std::multimap<size_t, void*> free_[2];
+  size_t cached_[2] = {0, 0};
+};
+
+// The pool of the innermost PoolScope on this thread, or null.
+MemoryPool* current_pool();
+
+class PoolScope {
+ public:
+  PoolScope(MemoryPool* pool, cudaStream_t stream);
+  ~PoolScope();
+  PoolScope(const PoolScope&) = delete;
+  PoolScope& operator=(const PoolScope&) = delete;
+
+ private:
+  MemoryPool* previous_;
+  cudaStream_t stream_;
+};
+
+// Device memory owned by RAII; from the current pool when there is one.
 template <class T>
 struct DevBuf {
   T* p = nullptr;
   size_t n = 0;
+  MemoryPool* pool = nullptr;
+  size_t bytes = 0;  // size class of a pooled block
   DevBuf() = default;
   explicit DevBuf(size_t count) { alloc(count); }
   DevBuf(const DevBuf&) = delete;
   DevBuf& operator=(const DevBuf&) = delete;
-  DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+  DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n), pool(o.pool), bytes(o.bytes) {
+    o.p = nullptr;
+    o.n = 0;
+    o.pool = nullptr;
+    o.bytes = 0;
+  }
   DevBuf& operator=(DevBuf&& o) noexcept {
     if (this != &o) {
       release();
       p = o.p;
       n = o.n;
+      pool = o.pool;
+      bytes = o.bytes;
       o.p = nullptr;
       o.n = 0;
+      o.pool = nullptr;
+      o.bytes = 0;
     }
     return *this;
   }
@@ -52,16 +106,27 @@ struct DevBuf {
     release();
     n = count;
     if (count == 0) return;
+    if (MemoryPool* mp = current_pool()) {
+      p = static_cast<T*>(mp->get(false, sizeof(T) * count, &bytes));
+      pool = mp;
+      return;
+    }
     cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&p), sizeof(T) * count);
     if (e != cudaSuccess) {
       p = nullptr;
+      n = 0;
       throw Error(ANU_ERR_MEMORY, std::string("cudaMalloc: ") + cudaGetErrorString(e));
     }
   }
   void release() {
-    if (p) cudaFree(p);
+    if (p) {
+      if (pool) pool->put(false, p, bytes);
+      else cudaFree(p);
+    }
     p = nullptr;
     n = 0;
+    pool = nullptr;
+    bytes = 0;
   }
   T* get() const { return p; }
 };
@@ -85,6 +150,7 @@ struct DevCsr {
 // Everything that depends on the matrix alone: the scaled matrix and its
 // transpose (host and device), the scaling, ||K~||, the stream.
 struct Problem : Exec {
+  MemoryPool pool;  // declared first: outlives every other member
   int32_t m = 0, n = 0, num_eq = 0;
   int precision = ANU_PRECISION_FP64;
   HostCsr k;   // scaled K~

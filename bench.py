@@ -238,6 +238,7 @@ def run_engine(args, rank, world, local_rank):
     solver.close()
     # e2e: from host arrays through the C ABI, every step
     e2e_ms = []
+    e2e_parts = []
     for i in range(args.warmup + args.steps if args.e2e else 0):
         flush_l2(torch, flush)
         barrier()
@@ -245,13 +246,18 @@ def run_engine(args, rank, world, local_rank):
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record()
+        h0 = time.perf_counter()
         s2 = pdhg.CaseStackSolver(st.base, st.c, st.q, st.lower, st.upper, opts)
+        h1 = time.perf_counter()
         r2 = s2.solve()
+        h2 = time.perf_counter()
         s2.close()
+        h3 = time.perf_counter()
         e1.record()
         torch.cuda.synchronize()
         if i >= args.warmup:
             e2e_ms.append(e0.elapsed_time(e1))
+            e2e_parts.append((h1 - h0, h2 - h1, h3 - h2))
     total_ms = float(np.sum(step_ms))
     total_e2e = float(np.sum(e2e_ms)) if e2e_ms else float("nan")
     if dist is not None:
@@ -295,7 +301,10 @@ def run_engine(args, rank, world, local_rank):
             "phases_ms_median": {k: round(1e3 * float(np.median([ph[k] for ph in phases])), 2)
                                  for k in phases[0]},
             "e2e": {"value": solved_all / (total_e2e / 1e3), "unit": "solves/s",
-                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                    "parts_ms_median": ({k: round(1e3 * float(np.median([p[i] for p in e2e_parts])), 2)
+                                         for i, k in enumerate(("create", "solve", "close"))}
+                                        if e2e_parts else None)},
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None, "traffic": None,
