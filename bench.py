@@ -46,6 +46,10 @@ sys.path.insert(0, ROOT)
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM = 6650.0
 TOL = 1e-6
+# DRAM bytes (read + write) per fused seg_kernel launch on this workload, mean
+# of the primal and dual kernels, from one cold-cache ncu capture
+# (profiles/seg_kernel_refinery_stack.md): 5.68 MB and 5.27 MB.
+SEG_KERNEL_TRAFFIC = 5.475e6
 
 
 def hbm_peak():
@@ -307,7 +311,10 @@ def run_engine(args, rank, world, local_rank):
                                         if e2e_parts else None)},
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": (achieved / peak) if achieved else None, "traffic": None,
+                         "frac": (achieved / peak) if achieved else None,
+                         "traffic": SEG_KERNEL_TRAFFIC,
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, "
+                                           "cold cache, profiles/seg_kernel_refinery_stack.md",
                          "peak_source": peak_kind,
                          "kernel": "seg_kernel (fused case-stack SpMM + primal/dual step), mean per launch",
                          "algorithmic_bytes_per_launch": bytes_it / 2.0,
