@@ -346,6 +346,33 @@ def refinery_stack(periods: int = 24, seed: int = BASE_SEED + 2) -> CaseStack:
                      np.stack(his))
 
 
+def sparse_random_lp(m: int, n: int, per_col: int = 8,
+                     seed: int = BASE_SEED) -> Tuple[StandardLp, float]:
+    """The construction of :func:`random_lp` (per column `per_col` distinct
+    uniformly random rows, N(0,1) values, planted optimum) with a sampler
+    whose cost is linear in the nonzeros: draw every slot at random, then
+    redraw the slots that repeat a row of their column until none do."""
+    rng = np.random.default_rng(seed)
+    per_col = min(per_col, m)
+    rows = rng.integers(0, m, size=(n, per_col))
+    while True:
+        srt = np.sort(rows, axis=1)
+        dup_cols = np.nonzero((srt[:, 1:] == srt[:, :-1]).any(axis=1))[0]
+        if dup_cols.size == 0:
+            break
+        sub = rows[dup_cols]
+        first = np.ones_like(sub, dtype=bool)
+        for s in range(1, per_col):
+            first[:, s] = ~(sub[:, :s] == sub[:, s:s + 1]).any(axis=1)
+        redraw = ~first
+        sub[redraw] = rng.integers(0, m, size=int(redraw.sum()))
+        rows[dup_cols] = sub
+    vals = rng.standard_normal((n, per_col))
+    cols = np.repeat(np.arange(n, dtype=np.int64), per_col)
+    a = Csr.from_triplets(m, n, rows.reshape(-1), cols, vals.reshape(-1))
+    return _kkt_lp(a, rng, f"sparse_random_{m}x{n}")
+
+
 def packed_batch(count: int = 256, seed: int = BASE_SEED + 3,
                  min_rows: int = 500, max_rows: int = 50_000) -> List[Tuple[StandardLp, float]]:
     """`count` independent known-optimum LPs, rows log-uniform in
@@ -354,7 +381,7 @@ def packed_batch(count: int = 256, seed: int = BASE_SEED + 3,
     rows = np.exp(rng.uniform(np.log(min_rows), np.log(max_rows), count)).astype(np.int64)
     out = []
     for i, mi in enumerate(rows.tolist()):
-        out.append(random_lp(int(mi), int(round(1.5 * mi)), 8, seed * 1000 + i))
+        out.append(sparse_random_lp(int(mi), int(round(1.5 * mi)), 8, seed * 1000 + i))
     return out
 
 

@@ -37,6 +37,8 @@ EXPORTS = (
     "anu_backend_step_size_terms", "anu_backend_convergence_terms",
     "anu_backend_convergence_terms_noalloc",
     "anu_pdhg_batch_create", "anu_pdhg_batch_solve", "anu_pdhg_batch_destroy",
+    "anu_pdhg_packed_create", "anu_pdhg_packed_solve", "anu_pdhg_packed_workers",
+    "anu_pdhg_packed_destroy",
 )
 
 
@@ -82,6 +84,12 @@ def lib():
     d("anu_pdhg_batch_solve", C.c_int, [C.c_void_p, _P(C.c_double), _P(C.c_double),
                                         _P(anu_pdhg_result)])
     d("anu_pdhg_batch_destroy", None, [C.c_void_p])
+    d("anu_pdhg_packed_create", C.c_int, [C.c_int32, _P(anu_lp), _P(anu_pdhg_options),
+                                          C.c_int32, _P(C.c_void_p)])
+    d("anu_pdhg_packed_solve", C.c_int, [C.c_void_p, _P(_P(C.c_double)), _P(_P(C.c_double)),
+                                         _P(anu_pdhg_result)])
+    d("anu_pdhg_packed_workers", C.c_int32, [C.c_void_p])
+    d("anu_pdhg_packed_destroy", None, [C.c_void_p])
     vp = C.c_void_p
     i64 = C.c_int64
     dbl = C.c_double
@@ -250,6 +258,56 @@ class CaseStackSolver:
 def solve_case_stack(stack, options: Optional[anu_pdhg_options] = None, **kw):
     """Solves an :class:`anukulan_b200.lpgen.CaseStack` on the engine."""
     s = CaseStackSolver(stack.base, stack.c, stack.q, stack.lower, stack.upper, options, **kw)
+    try:
+        return s.solve()
+    finally:
+        s.close()
+
+
+class PackedBatchSolver:
+    """Independent LPs of different shapes solved together
+    (``anu_pdhg_packed_*``). `workers` = 0 lets the engine autotune the
+    number of LPs in flight."""
+
+    def __init__(self, lps, options: Optional[anu_pdhg_options] = None, workers: int = 0, **kw):
+        self._cls = [CLp(lp) for lp in lps]
+        arr = (anu_lp * len(self._cls))(*[c.struct for c in self._cls])
+        self._arr = arr
+        self.options = _options(options, kw)
+        self._h = C.c_void_p()
+        check(lib().anu_pdhg_packed_create(len(self._cls), arr, C.byref(self.options),
+                                           int(workers), C.byref(self._h)))
+
+    @property
+    def workers(self) -> int:
+        return int(lib().anu_pdhg_packed_workers(self._h))
+
+    def solve(self):
+        """Returns a list of PdhgResult, one per LP, in input order."""
+        N = len(self._cls)
+        xs = [np.zeros(c.n) for c in self._cls]
+        ys = [np.zeros(c.m) for c in self._cls]
+        px = (C.POINTER(C.c_double) * N)(*[f64_ptr(v) for v in xs])
+        py = (C.POINTER(C.c_double) * N)(*[f64_ptr(v) for v in ys])
+        res = (anu_pdhg_result * N)()
+        check(lib().anu_pdhg_packed_solve(self._h, px, py, res))
+        return [PdhgResult.from_c(res[i], xs[i], ys[i]) for i in range(N)]
+
+    def close(self):
+        if self._h:
+            lib().anu_pdhg_packed_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def solve_packed(lps, options: Optional[anu_pdhg_options] = None, workers: int = 0, **kw):
+    """Solves independent LPs as one packed batch; one PdhgResult per LP."""
+    s = PackedBatchSolver(lps, options, workers, **kw)
     try:
         return s.solve()
     finally:

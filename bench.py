@@ -10,7 +10,7 @@ on the device; `e2e` is the same metric through the C ABI from host arrays
 (create + solve + download inside the timed region).
 
     python bench.py [--gpus N --steps K --warmup W] [--impl reference]
-                    [--workload stack|spmv]
+                    [--workload stack|spmv|packed]
 
 Two side measurements ride on the stack line:
   * `spmv`: the single-LP iteration (the two fused SpMV kernels) on the
@@ -18,6 +18,8 @@ Two side measurements ride on the stack line:
     a fixed number of iterations with CUDA events - per-iteration time,
     iterations/s and algorithmic GB/s against the measured HBM peak.
     `--workload spmv` runs this leg alone (for profiling).
+  `--workload packed` instead times the packed batch of 256 unequal LPs
+  (its own JSON line).
   * `fp64_single_case`: the same 60 cases solved one at a time by the
     engine's plain FP64 mode - the plain FP64 single-case GPU PDHG the batched
     mixed-precision run is compared with.
@@ -162,6 +164,81 @@ def spmv_leg(iterations, device, peak):
                      "algorithmic_bytes_per_iteration": b,
                      "achieved_GBps": b / per_it / 1e9, "frac": b / per_it / 1e9 / peak,
                      "kernel_launches": int(r.kernel_launches)}
+    return out
+
+
+def run_packed(args, rank, world, local_rank):
+    """The packed batch: 256 independent LPs, rows log-uniform in
+    [500, 50,000], 1.5x as many columns, 8 nonzeros per column, FP32 with
+    FP64 checks and refinement to relative KKT 1e-6. A step solves the whole
+    batch. Rank 0 only (the batch does not shard here)."""
+    if rank != 0:
+        return None
+    import torch
+    import oracle
+    from concurrent.futures import ThreadPoolExecutor
+    from anukulan_b200 import lpgen, pdhg
+    from anukulan_b200.abi import OPTIMAL, PRECISION_FP32, make_options
+    torch.cuda.set_device(local_rank)
+    batch = lpgen.packed_batch()
+    lps = [lp for lp, _ in batch]
+    opts = make_options(tolerance=TOL, precision=PRECISION_FP32, device=local_rank)
+    t0 = time.perf_counter()
+    solver = pdhg.PackedBatchSolver(lps, opts, workers=args.packed_workers)
+    create_s = time.perf_counter() - t0
+    for _ in range(args.warmup):
+        solver.solve()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    step_ms, solved, iters = [], 0, 0
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        res = solver.solve()
+        e1.record()
+        torch.cuda.synchronize()
+        step_ms.append(e0.elapsed_time(e1))
+        solved += sum(int(r.status == OPTIMAL) for r in res)
+        iters += sum(r.iterations for r in res)
+    clk = clocks.stop()
+    workers = solver.workers
+    solver.close()
+    total = float(np.sum(step_ms))
+    nnz = sum(lp.k.nnz for lp in lps)
+    out = {
+        "metric": "LP solves/s to relative KKT 1e-6 (packed batch of unequal LPs, FP32 + FP64 checks)",
+        "value": solved / (total / 1e3), "unit": "solves/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded generator, 256 LPs of the random known-optimum construction)",
+        "config": {"workload": "packed_batch", "lps": len(lps),
+                   "rows_total": int(sum(lp.num_rows for lp in lps)), "nnz_total": int(nnz),
+                   "rows_range": [int(min(lp.num_rows for lp in lps)),
+                                  int(max(lp.num_rows for lp in lps))],
+                   "tolerance": TOL, "workers": workers},
+        "cases_optimal": solved, "cases_attempted": len(lps) * args.steps,
+        "iterations_per_second": iters / (total / 1e3),
+        "step_ms": [round(v, 1) for v in step_ms], "create_seconds": create_s, "clocks": clk,
+    }
+    if args.cpu_baseline:
+        # The reference's CPU PDHG on a uniform random sample of the batch,
+        # one LP per host thread.
+        rng = np.random.default_rng(0)
+        sample = [lps[i] for i in rng.choice(len(lps), size=min(32, len(lps)), replace=False)]
+        threads = os.cpu_count() or 1
+        use_ref = oracle.have_reference()
+        fn = (lambda lp: oracle.ref_solve(lp, tolerance=TOL)) if use_ref else \
+            (lambda lp: oracle.oracle_solve(lp, tolerance=TOL))
+        t0 = time.perf_counter()
+        with ThreadPoolExecutor(max_workers=threads) as ex:
+            ok = sum(int(r.status == OPTIMAL) for r in ex.map(fn, sample))
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": ok / dt, "unit": "solves/s", "cores": threads,
+                               "kind": "reference" if use_ref else "port",
+                               "sample": f"{len(sample)} LPs drawn uniformly from the batch, "
+                                         f"one per host thread (cpu_backend), {dt:.1f} s"}
     return out
 
 
@@ -405,7 +482,9 @@ def main(argv=None):
     ap.add_argument("--ref-seconds", type=float, default=10.0)
     ap.add_argument("--no-e2e", dest="e2e", action="store_false",
                     help="skip the end-to-end pass (profiling runs)")
-    ap.add_argument("--workload", default="stack", choices=["stack", "spmv"])
+    ap.add_argument("--workload", default="stack", choices=["stack", "spmv", "packed"])
+    ap.add_argument("--packed-workers", type=int, default=0,
+                    help="LPs in flight for --workload packed (0: autotune)")
     ap.add_argument("--spmv-iterations", type=int, default=2000)
     ap.add_argument("--no-side", dest="side", action="store_false",
                     help="skip the spmv and fp64 single-case side measurements")
@@ -415,6 +494,8 @@ def main(argv=None):
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         out = run_reference(args, rank, world)
+    elif args.workload == "packed":
+        out = run_packed(args, rank, world, local_rank)
     elif args.workload == "spmv":
         out = None
         if rank == 0:

@@ -368,6 +368,29 @@ int anu_pdhg_batch_solve(anu_pdhg_batch* handle, double* x, double* y,
                          anu_pdhg_result* results);
 void anu_pdhg_batch_destroy(anu_pdhg_batch* handle);
 
+/* ------------------------------------------------------ packed batches
+ * Independent LPs of different shapes solved together on one GPU. No
+ * counterpart in the reference, whose callers loop solve_pdhg over such a
+ * set. Every LP is solved exactly as anu_pdhg_solve solves it (same
+ * iterates, same result); what the batch adds is concurrency: W host
+ * workers take LPs from one queue, largest first, each on its own stream,
+ * and a worker that retires an LP admits the next one at once.
+ *
+ * workers: 0 = choose W by a short autotuning run at creation (each
+ * candidate W runs W LPs drawn evenly from the batch for a few check
+ * periods; the most nonzero-iterations per second wins), else W itself. */
+typedef struct anu_pdhg_packed anu_pdhg_packed;
+int anu_pdhg_packed_create(int32_t num_lps, const anu_lp* lps,
+                           const anu_pdhg_options* options, int32_t workers,
+                           anu_pdhg_packed** handle);
+/* x[i] (n_i entries) and y[i] (m_i entries) receive LP i's answer (a NULL
+ * array or entry skips it); results has num_lps entries. */
+int anu_pdhg_packed_solve(anu_pdhg_packed* handle, double* const* x,
+                          double* const* y, anu_pdhg_result* results);
+/* The worker count in use (the autotuner's choice when it ran). */
+int32_t anu_pdhg_packed_workers(const anu_pdhg_packed* handle);
+void anu_pdhg_packed_destroy(anu_pdhg_packed* handle);
+
 #ifdef __cplusplus
 }  /* extern "C" */
 #endif
