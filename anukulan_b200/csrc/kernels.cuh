@@ -164,7 +164,7 @@ struct PrimalEpi {
     T x, c, lo, hi, anchor, sum;
   };
   __device__ __forceinline__ Pre prefetch(int32_t j, int32_t k) const {
-    Pre r;
+    Pre r{};
     const StepParams& P = p[k];
     if (!P.active) return r;
     const size_t e = (size_t)j * K + k;
@@ -235,7 +235,7 @@ struct DualEpi {
     T y, q, kx, anchor_y, anchor_kx, floor_v, sum;
   };
   __device__ __forceinline__ Pre prefetch(int32_t i, int32_t k) const {
-    Pre r;
+    Pre r{};
     const StepParams& P = p[k];
     if (!P.active) return r;
     const size_t e = (size_t)i * K + k;
