@@ -39,6 +39,8 @@ EXPORTS = (
     "anu_pdhg_batch_create", "anu_pdhg_batch_solve", "anu_pdhg_batch_destroy",
     "anu_pdhg_packed_create", "anu_pdhg_packed_solve", "anu_pdhg_packed_workers",
     "anu_pdhg_packed_destroy",
+    "anu_pdhg_unrolled_create", "anu_pdhg_unrolled_step_sizes", "anu_pdhg_forward_unrolled",
+    "anu_pdhg_backward", "anu_pdhg_unrolled_destroy",
 )
 
 
@@ -90,6 +92,12 @@ def lib():
                                          _P(anu_pdhg_result)])
     d("anu_pdhg_packed_workers", C.c_int32, [C.c_void_p])
     d("anu_pdhg_packed_destroy", None, [C.c_void_p])
+    d("anu_pdhg_unrolled_create", C.c_int, [_P(anu_lp), C.c_int32] + [_P(C.c_double)] * 4
+      + [_P(anu_pdhg_options), C.c_int32, C.c_int32, _P(C.c_void_p)])
+    d("anu_pdhg_unrolled_step_sizes", C.c_int, [C.c_void_p, _P(C.c_double), _P(C.c_double)])
+    d("anu_pdhg_forward_unrolled", C.c_int, [C.c_void_p, _P(C.c_double), _P(C.c_double)])
+    d("anu_pdhg_backward", C.c_int, [C.c_void_p] + [_P(C.c_double)] * 4)
+    d("anu_pdhg_unrolled_destroy", None, [C.c_void_p])
     vp = C.c_void_p
     i64 = C.c_int64
     dbl = C.c_double
@@ -312,3 +320,62 @@ def solve_packed(lps, options: Optional[anu_pdhg_options] = None, workers: int =
         return s.solve()
     finally:
         s.close()
+
+
+class UnrolledPdhg:
+    """Truncated, unrolled PDHG over a case stack and its adjoint
+    (``anu_pdhg_unrolled_*``): forward() gives x_T, y_T; backward(dL/dx_T,
+    dL/dy_T) gives dL/dc, dL/dq, all unscaled and case-major."""
+
+    def __init__(self, base: StandardLp, c=None, q=None, lower=None, upper=None,
+                 iterations: int = 2000, checkpoint_every: int = 100,
+                 options: Optional[anu_pdhg_options] = None, **kw):
+        arrays = [c, q, lower, upper]
+        counts = {np.atleast_2d(a).shape[0] for a in arrays if a is not None}
+        if len(counts) > 1:
+            raise ValueError("case arrays must share their first dimension")
+        self.num_cases = counts.pop() if counts else 1
+        self._keep = [None if a is None else np.ascontiguousarray(np.atleast_2d(a), np.float64)
+                      for a in arrays]
+        self._cl = CLp(base)
+        self.options = _options(options, kw)
+        self._h = C.c_void_p()
+        check(lib().anu_pdhg_unrolled_create(self._cl.ref(), self.num_cases,
+                                             *[f64_ptr(a) for a in self._keep],
+                                             C.byref(self.options), int(iterations),
+                                             int(checkpoint_every), C.byref(self._h)))
+
+    def step_sizes(self):
+        tau = np.zeros(self.num_cases)
+        sigma = np.zeros(self.num_cases)
+        check(lib().anu_pdhg_unrolled_step_sizes(self._h, f64_ptr(tau), f64_ptr(sigma)))
+        return tau, sigma
+
+    def forward(self):
+        K, n, m = self.num_cases, self._cl.n, self._cl.m
+        x = np.zeros((K, n))
+        y = np.zeros((K, m))
+        check(lib().anu_pdhg_forward_unrolled(self._h, f64_ptr(x), f64_ptr(y)))
+        return x, y
+
+    def backward(self, dloss_dx, dloss_dy=None):
+        K, n, m = self.num_cases, self._cl.n, self._cl.m
+        dx = np.ascontiguousarray(np.broadcast_to(dloss_dx, (K, n)), np.float64)
+        dy = None if dloss_dy is None else np.ascontiguousarray(
+            np.broadcast_to(dloss_dy, (K, m)), np.float64)
+        gc = np.zeros((K, n))
+        gq = np.zeros((K, m))
+        check(lib().anu_pdhg_backward(self._h, f64_ptr(dx), f64_ptr(dy), f64_ptr(gc),
+                                      f64_ptr(gq)))
+        return gc, gq
+
+    def close(self):
+        if self._h:
+            lib().anu_pdhg_unrolled_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

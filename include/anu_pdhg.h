@@ -391,6 +391,41 @@ int anu_pdhg_packed_solve(anu_pdhg_packed* handle, double* const* x,
 int32_t anu_pdhg_packed_workers(const anu_pdhg_packed* handle);
 void anu_pdhg_packed_destroy(anu_pdhg_packed* handle);
 
+/* ------------------------------------------------------ unrolled adjoint
+ * d(loss)/d(c, q) through a truncated, unrolled PDHG. No counterpart in the
+ * reference. The unrolled program is `iterations` steps of reflected
+ * Halpern PDHG (reflection 1) on the scaled problem, step sizes fixed at the
+ * values solve_pdhg starts from (or options.initial_step_size /
+ * initial_primal_weight), the Halpern anchor restarted at the new iterate
+ * every `checkpoint_every` steps, from solve_pdhg's cold start. It is
+ * piecewise linear in (c, q); the adjoint is exact wherever no projection
+ * sits on its kink.
+ *
+ * Cases as in anu_pdhg_batch_create (case-major arrays, NULL = base), at
+ * most 64. The forward pass keeps the iterate every `checkpoint_every`
+ * steps; the backward pass recomputes each segment from its checkpoint,
+ * recording the projection masks, and reverses it with hand-written
+ * kernels (two fused SpMV launches per step); gradients accumulate in FP64.
+ * options.precision selects FP32 or FP64 iterates. */
+typedef struct anu_pdhg_unrolled anu_pdhg_unrolled;
+int anu_pdhg_unrolled_create(const anu_lp* base, int32_t num_cases,
+                             const double* c, const double* q,
+                             const double* lower, const double* upper,
+                             const anu_pdhg_options* options, int32_t iterations,
+                             int32_t checkpoint_every, anu_pdhg_unrolled** handle);
+/* The fixed primal and dual step sizes of each case (num_cases each). */
+int anu_pdhg_unrolled_step_sizes(const anu_pdhg_unrolled* handle, double* tau,
+                                 double* sigma);
+/* x_T (num_cases*n) and y_T (num_cases*m), unscaled, case-major; either
+ * may be NULL. */
+int anu_pdhg_forward_unrolled(anu_pdhg_unrolled* handle, double* x, double* y);
+/* Given dloss/dx_T (num_cases*n) and dloss/dy_T (num_cases*m, NULL = 0),
+ * writes dloss/dc (num_cases*n) and dloss/dq (num_cases*m). A loss that
+ * depends on c directly (such as c'x_T) adds that term itself. */
+int anu_pdhg_backward(anu_pdhg_unrolled* handle, const double* dloss_dx,
+                      const double* dloss_dy, double* grad_c, double* grad_q);
+void anu_pdhg_unrolled_destroy(anu_pdhg_unrolled* handle);
+
 #ifdef __cplusplus
 }  /* extern "C" */
 #endif
