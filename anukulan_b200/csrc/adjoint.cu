@@ -243,6 +243,11 @@ int grid_elems(int64_t n) { return grid_for(n, 256, 148 * 8); }
 
 }  // namespace
 
+namespace {
+template <class T>
+struct UnrollState;
+}  // namespace
+
 // The unrolled program of one case stack, held on the device.
 struct Unrolled {
   std::unique_ptr<Problem> problem;
@@ -251,8 +256,12 @@ struct Unrolled {
   int32_t iterations = 0, period = 0;
   int precision = ANU_PRECISION_FP64;
   std::vector<double> tau, sigma;
-  bool have_forward = false;
   double scaling_seconds = 0.0, norm_seconds = 0.0;
+  // The last forward pass's state and checkpoints (declared after the
+  // problem, so released into its memory pool before the pool goes).
+  std::unique_ptr<UnrollState<float>> state32;
+  std::unique_ptr<UnrollState<double>> state64;
+  ~Unrolled();
 };
 
 namespace {
@@ -290,6 +299,15 @@ struct UnrollState {
   DevBuf<T> ckpt;  // checkpoints: per segment x, y, ax, ay
   size_t nk = 0, mk = 0;
 };
+
+}  // namespace
+
+Unrolled::~Unrolled() {
+  state32.reset();
+  state64.reset();
+}
+
+namespace {
 
 template <class T>
 void setup_state(Unrolled& u, UnrollState<T>& s) {
@@ -543,17 +561,17 @@ int anu_pdhg_unrolled_step_sizes(const anu_pdhg_unrolled* h, double* tau, double
 int anu_pdhg_forward_unrolled(anu_pdhg_unrolled* h, double* x, double* y) {
   return anu::guarded_unrolled([&] {
     if (h == nullptr) throw Error(ANU_ERR_INVALID, "null argument");
-    anu::Problem& p = *h->u.problem;
+    anu::Unrolled& u = h->u;
+    anu::Problem& p = *u.problem;
     ANU_CUDA(cudaSetDevice(p.device));
     anu::PoolScope scope(&p.pool, p.stream);
-    if (h->u.precision == ANU_PRECISION_FP32) {
-      anu::UnrollState<float> s;
-      anu::forward_t<float>(h->u, s, x, y);
+    if (u.precision == ANU_PRECISION_FP32) {
+      u.state32 = std::make_unique<anu::UnrollState<float>>();
+      anu::forward_t<float>(u, *u.state32, x, y);
     } else {
-      anu::UnrollState<double> s;
-      anu::forward_t<double>(h->u, s, x, y);
+      u.state64 = std::make_unique<anu::UnrollState<double>>();
+      anu::forward_t<double>(u, *u.state64, x, y);
     }
-    h->u.have_forward = true;
   });
 }
 
@@ -561,19 +579,24 @@ int anu_pdhg_backward(anu_pdhg_unrolled* h, const double* dloss_dx, const double
                       double* grad_c, double* grad_q) {
   return anu::guarded_unrolled([&] {
     if (h == nullptr) throw Error(ANU_ERR_INVALID, "null argument");
-    anu::Problem& p = *h->u.problem;
+    anu::Unrolled& u = h->u;
+    anu::Problem& p = *u.problem;
     ANU_CUDA(cudaSetDevice(p.device));
     anu::PoolScope scope(&p.pool, p.stream);
-    // The forward pass is run again to lay down the checkpoints, then
-    // reversed segment by segment.
-    if (h->u.precision == ANU_PRECISION_FP32) {
-      anu::UnrollState<float> s;
-      anu::forward_t<float>(h->u, s, nullptr, nullptr);
-      anu::backward_t<float>(h->u, s, dloss_dx, dloss_dy, grad_c, grad_q);
+    // The checkpoints of the last forward pass; without one, a forward pass
+    // lays them down first.
+    if (u.precision == ANU_PRECISION_FP32) {
+      if (!u.state32) {
+        u.state32 = std::make_unique<anu::UnrollState<float>>();
+        anu::forward_t<float>(u, *u.state32, nullptr, nullptr);
+      }
+      anu::backward_t<float>(u, *u.state32, dloss_dx, dloss_dy, grad_c, grad_q);
     } else {
-      anu::UnrollState<double> s;
-      anu::forward_t<double>(h->u, s, nullptr, nullptr);
-      anu::backward_t<double>(h->u, s, dloss_dx, dloss_dy, grad_c, grad_q);
+      if (!u.state64) {
+        u.state64 = std::make_unique<anu::UnrollState<double>>();
+        anu::forward_t<double>(u, *u.state64, nullptr, nullptr);
+      }
+      anu::backward_t<double>(u, *u.state64, dloss_dx, dloss_dy, grad_c, grad_q);
     }
   });
 }

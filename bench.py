@@ -10,7 +10,7 @@ on the device; `e2e` is the same metric through the C ABI from host arrays
 (create + solve + download inside the timed region).
 
     python bench.py [--gpus N --steps K --warmup W] [--impl reference]
-                    [--workload stack|spmv|packed]
+                    [--workload stack|spmv|packed|adjoint]
 
 Two side measurements ride on the stack line:
   * `spmv`: the single-LP iteration (the two fused SpMV kernels) on the
@@ -18,11 +18,13 @@ Two side measurements ride on the stack line:
     a fixed number of iterations with CUDA events - per-iteration time,
     iterations/s and algorithmic GB/s against the measured HBM peak.
     `--workload spmv` runs this leg alone (for profiling).
-  `--workload packed` instead times the packed batch of 256 unequal LPs
-  (its own JSON line).
   * `fp64_single_case`: the same 60 cases solved one at a time by the
     engine's plain FP64 mode - the plain FP64 single-case GPU PDHG the batched
     mixed-precision run is compared with.
+
+`--workload packed` times the packed batch of 256 unequal LPs instead, and
+`--workload adjoint` the unrolled-PDHG sensitivities of the 60-case stack;
+each prints its own JSON line.
 
 Under torchrun every rank solves its own copy of the stack (weak scaling, no
 collective on the data path); rank 0 prints one JSON line. `--impl reference`
@@ -175,8 +177,6 @@ def run_packed(args, rank, world, local_rank):
     if rank != 0:
         return None
     import torch
-    import oracle
-    from concurrent.futures import ThreadPoolExecutor
     from anukulan_b200 import lpgen, pdhg
     from anukulan_b200.abi import OPTIMAL, PRECISION_FP32, make_options
     torch.cuda.set_device(local_rank)
@@ -225,6 +225,8 @@ def run_packed(args, rank, world, local_rank):
     if args.cpu_baseline:
         # The reference's CPU PDHG on a uniform random sample of the batch,
         # one LP per host thread.
+        import oracle
+        from concurrent.futures import ThreadPoolExecutor
         rng = np.random.default_rng(0)
         sample = [lps[i] for i in rng.choice(len(lps), size=min(32, len(lps)), replace=False)]
         threads = os.cpu_count() or 1
@@ -239,6 +241,70 @@ def run_packed(args, rank, world, local_rank):
                                "kind": "reference" if use_ref else "port",
                                "sample": f"{len(sample)} LPs drawn uniformly from the batch, "
                                          f"one per host thread (cpu_backend), {dt:.1f} s"}
+    return out
+
+
+def run_adjoint(args, rank, world, local_rank):
+    """Sensitivities through the unrolled program: the 60-case refinery stack,
+    2,000 FP32 iterations with checkpoints every 100, loss c_hat'x_T per
+    case with c_hat = c (1 + 0.05 N(0,1)). A step is one forward pass (x_T
+    and the losses) and one backward pass (dL/dc, dL/dq for every case)."""
+    if rank != 0:
+        return None
+    import torch
+    from anukulan_b200 import lpgen, pdhg
+    from anukulan_b200.abi import PRECISION_FP32, make_options
+    torch.cuda.set_device(local_rank)
+    stack, c_hat = lpgen.adjoint_case()
+    ratio = c_hat / np.where(stack.base.c != 0, stack.base.c, 1.0)
+    loss = stack.c * ratio
+    T, R = 2000, 100
+    opts = make_options(precision=PRECISION_FP32, device=local_rank)
+    u = pdhg.UnrolledPdhg(stack.base, stack.c, stack.q, stack.lower, stack.upper,
+                          iterations=T, checkpoint_every=R, options=opts)
+    for _ in range(args.warmup):
+        x, _ = u.forward()
+        u.backward(loss)
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    step_ms = []
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        x, _ = u.forward()
+        gc, gq = u.backward(loss)
+        e1.record()
+        torch.cuda.synchronize()
+        step_ms.append(e0.elapsed_time(e1))
+    clk = clocks.stop()
+    tau, sigma = u.step_sizes()
+    u.close()
+    total = float(np.sum(step_ms))
+    K = stack.num_cases
+    out = {
+        "metric": "unrolled-PDHG sensitivities/s (dL/dc, dL/dq per case, 2,000 FP32 iterations)",
+        "value": K * args.steps / (total / 1e3), "unit": "case gradients/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded generator, refinery-shaped 60-case stack)",
+        "config": {"workload": "unrolled_adjoint", "cases": K, "iterations": T,
+                   "checkpoint_every": R, "rows": stack.base.num_rows,
+                   "cols": stack.base.num_cols},
+        "step_ms": [round(v, 2) for v in step_ms], "clocks": clk,
+    }
+    if args.cpu_baseline:
+        # The float64 numpy restatement of the same program and reverse mode,
+        # one case on one host thread.
+        from oracle import unrolled as U
+        slp = U.ScaledLp(stack.case(0))
+        t0 = time.perf_counter()
+        U.adjoint(slp, stack.c[0], stack.q[0], loss[0], tau[0], sigma[0], T, R)
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": 1.0 / dt, "unit": "case gradients/s", "cores": 1,
+                               "kind": "port",
+                               "sample": f"case 0, forward + reverse in numpy/scipy FP64, {dt:.2f} s"}
     return out
 
 
@@ -482,7 +548,8 @@ def main(argv=None):
     ap.add_argument("--ref-seconds", type=float, default=10.0)
     ap.add_argument("--no-e2e", dest="e2e", action="store_false",
                     help="skip the end-to-end pass (profiling runs)")
-    ap.add_argument("--workload", default="stack", choices=["stack", "spmv", "packed"])
+    ap.add_argument("--workload", default="stack",
+                    choices=["stack", "spmv", "packed", "adjoint"])
     ap.add_argument("--packed-workers", type=int, default=0,
                     help="LPs in flight for --workload packed (0: autotune)")
     ap.add_argument("--spmv-iterations", type=int, default=2000)
@@ -496,6 +563,8 @@ def main(argv=None):
         out = run_reference(args, rank, world)
     elif args.workload == "packed":
         out = run_packed(args, rank, world, local_rank)
+    elif args.workload == "adjoint":
+        out = run_adjoint(args, rank, world, local_rank)
     elif args.workload == "spmv":
         out = None
         if rank == 0:
