@@ -19,7 +19,8 @@
 //
 // Forward: the steps run as the engine's fused SpMV launches over the case
 // stack (case-interleaved vectors, every nonzero read serving all cases),
-// with the state saved every `checkpoint_every` steps.
+// with the state saved every `checkpoint_every` steps; a segment's launches
+// are one CUDA graph, replayed segment after segment.
 //
 // Backward (reverse mode): segment by segment from the last, the segment is
 // recomputed from its checkpoint with the projection masks recorded
@@ -376,15 +377,61 @@ void checkpoint(Problem& p, UnrollState<T>& s, int seg, bool save) {
                              sizeof(T) * len[i], cudaMemcpyDeviceToDevice, p.stream));
 }
 
+// A segment's launches as one CUDA graph: captured on first use, replayed
+// for every later full segment (the launches and their arguments repeat
+// from segment to segment; only the checkpoint copies between differ).
+struct SegmentGraph {
+  cudaGraphExec_t exec = nullptr;
+  int64_t launches = 0;
+  SegmentGraph() = default;
+  SegmentGraph(const SegmentGraph&) = delete;
+  SegmentGraph& operator=(const SegmentGraph&) = delete;
+  ~SegmentGraph() {
+    if (exec) cudaGraphExecDestroy(exec);
+  }
+};
+
+template <class F>
+void replay(Problem& p, SegmentGraph& g, F&& body) {
+  if (g.exec == nullptr) {
+    const int64_t before = p.launches;
+    ANU_CUDA(cudaStreamBeginCapture(p.stream, cudaStreamCaptureModeThreadLocal));
+    try {
+      body();
+    } catch (...) {
+      cudaGraph_t broken = nullptr;
+      cudaStreamEndCapture(p.stream, &broken);
+      if (broken) cudaGraphDestroy(broken);
+      throw;
+    }
+    cudaGraph_t graph = nullptr;
+    ANU_CUDA(cudaStreamEndCapture(p.stream, &graph));
+    const cudaError_t e = cudaGraphInstantiate(&g.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    ANU_CUDA(e);
+    g.launches = p.launches - before;
+    p.launches = before;
+  }
+  ANU_CUDA(cudaGraphLaunch(g.exec, p.stream));
+  p.launches += g.launches;
+}
+
 template <class T>
 void forward_t(Unrolled& u, UnrollState<T>& s, double* x_out, double* y_out) {
   Problem& p = *u.problem;
   const int segments = (u.iterations + u.period - 1) / u.period;
   setup_state(u, s);
   s.ckpt.alloc(static_cast<size_t>(std::max(segments, 1)) * 2 * (s.nk + s.mk));
-  for (int t = 0; t < u.iterations; ++t) {
-    if (t % u.period == 0) checkpoint(p, s, t / u.period, true);
-    forward_step(p, u.K, s, t, u.period, nullptr, nullptr);
+  SegmentGraph graph;
+  for (int seg = 0; seg < segments; ++seg) {
+    const int s0 = seg * u.period;
+    const int len = std::min(u.iterations - s0, u.period);
+    checkpoint(p, s, seg, true);
+    auto body = [&]() {
+      for (int j = 0; j < len; ++j) forward_step(p, u.K, s, j, u.period, nullptr, nullptr);
+    };
+    if (len == u.period) replay(p, graph, body);
+    else body();
   }
   if (x_out) download_cases(p.stream, s.x, p.n, u.K, &p.scaling.col_scale, x_out);
   if (y_out) download_cases(p.stream, s.y, p.m, u.K, &p.scaling.row_scale, y_out);
@@ -425,33 +472,45 @@ void backward_t(Unrolled& u, UnrollState<T>& s, const double* dx, const double* 
   ANU_CUDA(cudaMemsetAsync(gc.p, 0, sizeof(double) * s.nk, st));
   ANU_CUDA(cudaMemsetAsync(gq.p, 0, sizeof(double) * s.mk, st));
   DevBuf<uint8_t> mx(static_cast<size_t>(R) * s.nk), my(static_cast<size_t>(R) * s.mk);
+  SegmentGraph recompute_graph, reverse_graph;
   for (int seg = segments - 1; seg >= 0; --seg) {
     const int s0 = seg * R;
     const int s1 = std::min(u.iterations, s0 + R);
+    const int len = s1 - s0;
     // Recompute the segment from its checkpoint, recording the masks.
     checkpoint(p, s, seg, false);
-    for (int t = s0; t < s1; ++t)
-      forward_step(p, K, s, t, R, mx.p + static_cast<size_t>(t - s0) * s.nk,
-                   my.p + static_cast<size_t>(t - s0) * s.mk);
-    // The dual half of reversing the segment's last step.
-    {
-      const StepSchedule sc = schedule(s1 - 1, R);
+    auto recompute = [&]() {
+      for (int j = 0; j < len; ++j)
+        forward_step(p, K, s, j, R, mx.p + static_cast<size_t>(j) * s.nk,
+                     my.p + static_cast<size_t>(j) * s.mk);
+    };
+    // Then reverse it: the dual half of its last step, then step by step.
+    auto reverse = [&]() {
+      const StepSchedule sc = schedule(len - 1, R);
       dual_reverse_kernel<T><<<grid_elems(s.mk), 256, 0, st>>>(
           static_cast<int64_t>(s.mk), K, s.sigma.p, sc.restart ? 1 : 0, sc.a,
-          my.p + static_cast<size_t>(s1 - 1 - s0) * s.mk, yh.p, ayh.p, z.p, gq.p);
+          my.p + static_cast<size_t>(len - 1) * s.mk, yh.p, ayh.p, z.p, gq.p);
       ANU_CUDA(cudaGetLastError());
-    }
-    for (int t = s1 - 1; t >= s0; --t) {
-      const StepSchedule sc = schedule(t, R);
-      product<T, T, T>(p, p.dkt, z.p, K,
-                       RevPrimal<T>{K, s.tau.p, sc.restart ? 1 : 0, sc.a, xh.p, axh.p,
-                                    mx.p + static_cast<size_t>(t - s0) * s.nk, uh.p, gc.p});
-      const bool more = t > s0;
-      const StepSchedule sp = more ? schedule(t - 1, R) : StepSchedule{false, 0.0};
-      product<T, T, T>(p, p.dk, uh.p, K,
-                       RevDual<T>{K, s.tau.p, s.sigma.p, yh.p, ayh.p, z.p, gq.p,
-                                  more ? my.p + static_cast<size_t>(t - 1 - s0) * s.mk : nullptr,
-                                  sp.restart ? 1 : 0, sp.a});
+      ++p.launches;
+      for (int j = len - 1; j >= 0; --j) {
+        const StepSchedule sj = schedule(j, R);
+        product<T, T, T>(p, p.dkt, z.p, K,
+                         RevPrimal<T>{K, s.tau.p, sj.restart ? 1 : 0, sj.a, xh.p, axh.p,
+                                      mx.p + static_cast<size_t>(j) * s.nk, uh.p, gc.p});
+        const bool more = j > 0;
+        const StepSchedule sp = more ? schedule(j - 1, R) : StepSchedule{false, 0.0};
+        product<T, T, T>(p, p.dk, uh.p, K,
+                         RevDual<T>{K, s.tau.p, s.sigma.p, yh.p, ayh.p, z.p, gq.p,
+                                    more ? my.p + static_cast<size_t>(j - 1) * s.mk : nullptr,
+                                    sp.restart ? 1 : 0, sp.a});
+      }
+    };
+    if (len == R) {
+      replay(p, recompute_graph, recompute);
+      replay(p, reverse_graph, reverse);
+    } else {
+      recompute();
+      reverse();
     }
   }
   // Back to the unscaled data: c~ = D2 c, q~ = D1 q.
