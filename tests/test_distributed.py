@@ -1,0 +1,76 @@
+"""The multi-GPU case sharding on CPU: two gloo ranks, a stand-in solver.
+
+Each rank solves its slice of the case stack; the all-gather must hand every
+rank every case's result exactly once, in case order. The stand-in records
+which rank solved which case, so the test also checks the partition.
+"""
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+from anukulan_b200 import distributed as D
+from anukulan_b200.lpgen import CaseStack
+from anukulan_b200.model import Csr, StandardLp
+
+
+def _stack(num_cases):
+    a = Csr.from_triplets(2, 3, [0, 0, 1], [0, 2, 1], [1.0, 2.0, 3.0])
+    base = StandardLp(a, np.ones(3), np.ones(2), np.zeros(3), np.full(3, 5.0), 1, 1.0, 0.0,
+                      np.arange(2, dtype=np.int32), np.ones(2), "tiny")
+    c = np.tile(base.c, (num_cases, 1)) + np.arange(num_cases)[:, None]
+    return CaseStack(base, [f"case{k}" for k in range(num_cases)], c,
+                     np.tile(base.q, (num_cases, 1)), np.tile(base.lower, (num_cases, 1)),
+                     np.tile(base.upper, (num_cases, 1)))
+
+
+def _worker(rank, world, port, num_cases, out):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        stack = _stack(num_cases)
+        res = D.solve_stack_sharded(
+            stack, solve=lambda s: [(rank, float(c[0])) for c in s.c])
+        out.put((rank, res))
+    finally:
+        dist.destroy_process_group()
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+@pytest.mark.parametrize("num_cases", [60, 7, 1])
+def test_sharded_stack_two_ranks(num_cases):
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, num_cases, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = dict(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for rank in (0, 1):
+        res = got[rank]
+        assert [c for _, c in res] == [1.0 + k for k in range(num_cases)]
+        owners = [r for r, _ in res]
+        assert owners == sorted(owners)
+        for r in (0, 1):
+            assert owners.count(r) == len(D.case_shard(num_cases, r, 2))
+
+
+def test_case_shard_partition():
+    for n in (0, 1, 5, 60, 61):
+        for w in (1, 2, 3, 8):
+            covered = [k for r in range(w) for k in D.case_shard(n, r, w)]
+            assert covered == list(range(n))
+    with pytest.raises(ValueError):
+        D.case_shard(4, 2, 2)
