@@ -613,13 +613,42 @@ void download_all(cudaStream_t s, const DevBuf<T>& src, int32_t len, int K,
       (*out)[k][i] = static_cast<double>(staging[static_cast<size_t>(i) * K + k]);
 }
 
+// A rolling case stack: the cases waiting for a slot and where the results
+// of finished cases go. A slot whose case retires at a termination check is
+// refilled there with the next waiting case (admission in place).
+struct AdmissionQueue {
+  std::vector<const CaseData*> pending;  // in admission order
+  std::vector<int32_t> pending_index;    // their positions in the caller's list
+  size_t next = 0;
+  std::vector<int32_t> slot_index;       // the caller's position of each slot's case, -1: none
+  std::vector<CaseResult>* out = nullptr;  // results by the caller's position
+};
+
+// One case's column of a case-interleaved device array (element (row, k) at
+// row*K + k), written from host data.
+template <class T>
+void upload_slot(cudaStream_t s, T* dst, int32_t len, int K, int k, const std::vector<double>& src,
+                 std::vector<std::vector<T>>* staging) {
+  if (len == 0) return;
+  staging->emplace_back(src.begin(), src.begin() + len);
+  ANU_CUDA(cudaMemcpy2DAsync(dst + k, sizeof(T) * K, staging->back().data(), sizeof(T), sizeof(T),
+                             len, cudaMemcpyHostToDevice, s));
+}
+
+template <class T>
+void zero_slot(cudaStream_t s, T* dst, int32_t len, int K, int k) {
+  if (len == 0 || dst == nullptr) return;
+  ANU_CUDA(cudaMemset2DAsync(dst + k, sizeof(T) * K, 0, sizeof(T), len, s));
+}
+
 template <class T>
 void run_cases_t(Problem& p, const std::vector<const CaseData*>& cases,
                  const anu_pdhg_options& o, const std::vector<const std::vector<double>*>& warm_x,
                  const std::vector<const std::vector<double>*>& warm_y,
                  std::vector<CaseResult>* results, double start_time, bool unit,
                  const std::vector<double>* init_eta = nullptr,
-                 const std::vector<double>* init_omega = nullptr);
+                 const std::vector<double>* init_omega = nullptr,
+                 AdmissionQueue* queue = nullptr);
 
 // Feasibility polishing of a set of cases (pdhg.cpp:666-751): a primal
 // sub-stack (c = 0) warm started from the seeds' x, then a dual sub-stack
@@ -726,11 +755,14 @@ void run_polish(Problem& p, bool unit, const std::vector<const CaseData*>& paren
 }
 
 template <class T>
-void run_cases_t(Problem& p, const std::vector<const CaseData*>& cases,
+void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
                  const anu_pdhg_options& o, const std::vector<const std::vector<double>*>& warm_x,
                  const std::vector<const std::vector<double>*>& warm_y,
                  std::vector<CaseResult>* results, double start_time, bool unit,
-                 const std::vector<double>* init_eta, const std::vector<double>* init_omega) {
+                 const std::vector<double>* init_eta, const std::vector<double>* init_omega,
+                 AdmissionQueue* queue) {
+  // The case in each slot; a rolling stack replaces retired ones.
+  std::vector<const CaseData*> cases(initial_cases);
   const int K = static_cast<int>(cases.size());
   const int32_t n = p.n, m = p.m;
   results->assign(K, CaseResult{});
@@ -750,6 +782,9 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& cases,
                    host_norminf(cases[k]->c)};
     S[k].next_polish_iteration = o.polish_first_iteration;
   }
+  // The stack iteration at which each slot's case started (0 unless admitted
+  // into a rolling stack); a case's own iteration count is measured from it.
+  std::vector<int32_t> origin(K, 0);
   const double tolerance = o.tolerance;
   const double gap_tolerance = o.gap_tolerance > 0.0 ? o.gap_tolerance : tolerance;
   const bool inf_norm = o.require_inf_norm_termination != 0;
@@ -1234,13 +1269,240 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& cases,
     return false;
   };
 
-  while (iteration < o.max_iterations && any_active()) {
+  // Results (pdhg.cpp:1205-1285) of the cases in slots `ks`: the final
+  // iterate (or the polished point), its FP64 residual, exit polishing, the
+  // objective. A rolling stack hands them to the queue and frees the slots.
+  auto finalize = [&](const std::vector<int>& ks) {
+    if (ks.empty()) return;
+    std::vector<std::vector<double>> fx, fy;
+    download_all(st, w.x, n, K, &fx);
+    download_all(st, w.y, m, K, &fy);
+    if (refine) {
+      // The answer is base + offset.
+      std::vector<std::vector<double>> bx, by;
+      download_all(st, w.xb, n, K, &bx);
+      download_all(st, w.yb, m, K, &by);
+      for (int k : ks) {
+        for (int32_t j = 0; j < n; ++j) fx[k][j] += bx[k][j];
+        for (int32_t i = 0; i < m; ++i) fy[k][i] += by[k][i];
+      }
+    }
+    std::vector<double> fterms;
+    {
+      std::vector<const CaseData*> ec;
+      std::vector<std::vector<double>> ex, ey;
+      for (int k : ks) {
+        ec.push_back(cases[k]);
+        ex.push_back(fx[k]);
+        ey.push_back(fy[k]);
+      }
+      eval_points_terms(p, unit, static_cast<int>(ks.size()), ec, ex, ey, &fterms);
+    }
+    std::vector<int> pos(K, -1);
+    for (size_t i = 0; i < ks.size(); ++i) pos[ks[i]] = static_cast<int>(i);
+    std::vector<int> exit_polish;
+    for (int k : ks) {
+      CaseState& c = S[k];
+      CaseResult& cr = R[k];
+      if (c.have_polished) {
+        cr.x = c.polished_x;
+        cr.y = c.polished_y;
+        cr.r.residual = c.polished_residual;
+        continue;
+      }
+      cr.xs = fx[k];
+      cr.ys = fy[k];
+      cr.x.resize(n);
+      cr.y.resize(m);
+      for (int32_t j = 0; j < n; ++j) cr.x[j] = unit ? fx[k][j] : p.scaling.col_scale[j] * fx[k][j];
+      for (int32_t i = 0; i < m; ++i) cr.y[i] = unit ? fy[k][i] : p.scaling.row_scale[i] * fy[k][i];
+      cr.r.residual = residual_from_terms(&fterms[static_cast<size_t>(pos[k]) * kCheckTerms],
+                                          &fterms[static_cast<size_t>(pos[k]) * kCheckTerms + kRowTerms],
+                                          c.scales);
+      const bool worth = polish_on && o.polish_on_exit &&
+                         o.termination == ANU_TERMINATION_FULL && c.status != ANU_PDHG_OPTIMAL &&
+                         c.status != ANU_PDHG_PRIMAL_INFEASIBLE &&
+                         c.status != ANU_PDHG_NUMERICAL_ERROR &&
+                         std::isfinite(cr.r.residual.primal_residual) &&
+                         std::isfinite(cr.r.residual.dual_residual) &&
+                         now_seconds() - start_time < o.time_limit_seconds;
+      if (worth && polish_budget(o, c.final_iteration) > 0) exit_polish.push_back(k);
+    }
+    // Exit polishing, one sub-stack per budget (cases that stopped at the
+    // same iteration count share one).
+    std::map<int32_t, std::vector<int>> exit_groups;
+    for (int k : exit_polish) exit_groups[polish_budget(o, S[k].final_iteration)].push_back(k);
+    for (const auto& group : exit_groups) {
+      const std::vector<int>& exits = group.second;
+      std::vector<std::vector<double>> sx, sy;
+      for (int k : exits) {
+        sx.push_back(fx[k]);
+        sy.push_back(fy[k]);
+      }
+      std::vector<std::vector<double>> pxs, pys, px, py;
+      std::vector<anu_pdhg_residual> pr;
+      std::vector<int32_t> spent;
+      run_polish<T>(p, unit, cases, exits, sx, sy, group.first, S, o, start_time, &pxs, &pys, &px,
+                    &py, &pr, &spent);
+      t_polish += phase_end();
+      for (size_t i = 0; i < exits.size(); ++i) {
+        const int k = exits[i];
+        CaseResult& cr = R[k];
+        ++cr.r.polish_attempts;
+        cr.r.polish_iterations += spent[i];
+        const anu_pdhg_residual& cur = cr.r.residual;
+        const anu_pdhg_residual& tr = pr[i];
+        const double gap_ceiling = std::fmax(gap_tolerance, cur.relative_gap);
+        const bool improved = tr.relative_primal <= cur.relative_primal &&
+                              tr.relative_dual <= cur.relative_dual &&
+                              (tr.relative_primal < cur.relative_primal ||
+                               tr.relative_dual < cur.relative_dual);
+        if (improved && tr.relative_gap <= gap_ceiling) {
+          cr.x = px[i];
+          cr.y = py[i];
+          cr.xs = pxs[i];
+          cr.ys = pys[i];
+          cr.r.residual = tr;
+          cr.r.polished = 1;
+          if (converged(tr, tolerance, o.absolute_tolerance, inf_norm, gap_tolerance)) {
+            S[k].status = ANU_PDHG_OPTIMAL;
+            set_message(&cr.r, "converged after feasibility polishing");
+          } else if (cr.r.message[0] == '\0') {
+            set_message(&cr.r, "feasibility polished");
+          } else {
+            set_message(&cr.r, std::string(cr.r.message) + ", feasibility polished");
+          }
+        }
+      }
+    }
+    t_checks += phase_end();
+    for (int k : ks) {
+      CaseResult& cr = R[k];
+      double cx = 0.0;
+      for (int32_t j = 0; j < n; ++j) cx += cases[k]->c[j] * cr.x[j];
+      cr.r.objective = cases[k]->objective_scale * cx + cases[k]->objective_offset;
+      cr.r.iterations = S[k].final_iteration;
+      cr.r.status = S[k].status;
+      cr.r.final_step_size = S[k].eta;
+      cr.r.final_primal_weight = S[k].omega;
+      cr.r.solve_seconds = now_seconds() - start_time;
+      cr.r.phases.setup = t_setup;
+      cr.r.phases.iterating = t_iter;
+      cr.r.phases.checks = t_checks;
+      cr.r.phases.polishing = t_polish;
+      cr.r.kernel_launches = static_cast<int32_t>(p.launches - launches0);
+      cr.r.device_iteration_seconds = device_iter_s;
+      cr.r.device_iterations = device_iters;
+      if (queue != nullptr) {
+        (*queue->out)[queue->slot_index[k]] = std::move(cr);
+        cr = CaseResult{};
+        queue->slot_index[k] = -1;
+      }
+    }
+  };
+
+  // Admission of `d` (the caller's case `index`) into the free slot k of a
+  // rolling stack, at a termination check: the slot's host state and every
+  // case-interleaved device array start over as at the start of a solve.
+  auto admit = [&](int k, int32_t index, const CaseData* d) {
+    cases[k] = d;
+    queue->slot_index[k] = index;
+    origin[k] = iteration;
+    S[k] = CaseState{};
+    S[k].scales = {host_norm2(d->q), host_norm2(d->c), host_norminf(d->q), host_norminf(d->c)};
+    S[k].next_polish_iteration = o.polish_first_iteration;
+    double eta = 0.9 / p.matrix_norm;
+    if (o.constant_step_size) eta = o.constant_step_scale / p.matrix_norm;
+    double omega = 1.0;
+    if (o.primal_weight_updates) {
+      const double cn = host_norm2(d->cs);
+      const double qn = host_norm2(d->qs);
+      if (cn > 1e-12 && qn > 1e-12) omega = cn / qn;
+    }
+    if (o.initial_step_size > 0.0) eta = o.initial_step_size;
+    if (o.initial_primal_weight > 0.0) omega = o.initial_primal_weight;
+    S[k].eta = eta;
+    S[k].omega = omega;
+    R[k] = CaseResult{};
+    R[k].r.matrix_norm_estimate = p.matrix_norm;
+    vc[k] = &d->cs;
+    vl[k] = &d->ls;
+    vu[k] = &d->us;
+    vq[k] = &d->qs;
+    oc[k] = &d->c;
+    ol[k] = &d->lower;
+    ou[k] = &d->upper;
+    oq[k] = &d->q;
+    std::vector<double> x0(n, 0.0);
+    for (int32_t j = 0; j < n; ++j) {
+      double v = 0.0;
+      const double lo = d->ls[j], hi = d->us[j];
+      if (v < lo) v = std::isfinite(lo) ? lo : 0.0;
+      if (v > hi) v = std::isfinite(hi) ? hi : 0.0;
+      x0[j] = v;
+    }
+    std::vector<std::vector<T>> staged;
+    std::vector<std::vector<double>> staged64;
+    upload_slot<T>(st, w.x.p, n, K, k, x0, &staged);
+    zero_slot<T>(st, w.y.p, m, K, k);
+    upload_slot<T>(st, w.c.p, n, K, k, d->cs, &staged);
+    upload_slot<T>(st, w.lo.p, n, K, k, d->ls, &staged);
+    upload_slot<T>(st, w.hi.p, n, K, k, d->us, &staged);
+    upload_slot<T>(st, w.q.p, m, K, k, d->qs, &staged);
+    upload_slot<double>(st, w.c0.p, n, K, k, d->c, &staged64);
+    upload_slot<double>(st, w.lo0.p, n, K, k, d->lower, &staged64);
+    upload_slot<double>(st, w.hi0.p, n, K, k, d->upper, &staged64);
+    upload_slot<double>(st, w.q0.p, m, K, k, d->q, &staged64);
+    if (o.detect_infeasibility) {
+      upload_slot<double>(st, w.los.p, n, K, k, d->ls, &staged64);
+      upload_slot<double>(st, w.his.p, n, K, k, d->us, &staged64);
+      upload_slot<double>(st, w.qs.p, m, K, k, d->qs, &staged64);
+    }
+    zero_slot<T>(st, w.ylo.p, m, K, k);
+    zero_slot<T>(st, w.anchor_x.p, n, K, k);
+    zero_slot<T>(st, w.anchor_y.p, m, K, k);
+    zero_slot<T>(st, w.anchor_kx.p, m, K, k);
+    zero_slot<T>(st, w.dx.p, n, K, k);
+    zero_slot<T>(st, w.dy.p, m, K, k);
+    upload_slot<T>(st, w.x_restart.p, n, K, k, x0, &staged);
+    zero_slot<T>(st, w.y_restart.p, m, K, k);
+    if (!o.pid_primal_weight) {
+      upload_slot<T>(st, w.x_prev.p, n, K, k, x0, &staged);
+      zero_slot<T>(st, w.y_prev.p, m, K, k);
+    }
+    zero_slot<T>(st, w.sum_x.p, n, K, k);
+    zero_slot<T>(st, w.sum_y.p, m, K, k);
+    if (refine) {
+      zero_slot<double>(st, w.xb.p, n, K, k);
+      zero_slot<double>(st, w.yb.p, m, K, k);
+      upload_slot<double>(st, w.c0s.p, n, K, k, d->cs, &staged64);
+      upload_slot<double>(st, w.q0s.p, m, K, k, d->qs, &staged64);
+      upload_slot<double>(st, w.l0s.p, n, K, k, d->ls, &staged64);
+      upload_slot<double>(st, w.u0s.p, n, K, k, d->us, &staged64);
+    }
+    // K x0 for this slot alone (pdhg.cpp:593).
+    product<double, T, double>(p, p.dk, w.x.p, K, StoreEpi<double>{K, w.kx64.p});
+    std::vector<int32_t> only(K, 0);
+    only[k] = 1;
+    set_mask(only);
+    masked_copy<T, double>(p, m, K, w.mask.p, w.kx64.p, w.kx.p);
+    if (o.restarts && !o.restart_on_fixed_point) {
+      kkt_terms(w.x.p, w.y.p, w.kkt.p);
+      ANU_CUDA(cudaMemcpy(h_kkt.p, w.kkt.p, sizeof(double) * kKktTerms * K, cudaMemcpyDeviceToHost));
+      S[k].kkt_at_restart = kkt_value(&h_kkt.p[static_cast<size_t>(k) * kKktTerms], S[k].omega);
+    }
+    // The staged host columns stay alive until the copies are done.
+    ANU_CUDA(cudaStreamSynchronize(st));
+  };
+
+  while ((queue != nullptr || iteration < o.max_iterations) && any_active()) {
     int32_t last;
     bool is_check;
     int len;
     if (!slow) {
       const int32_t next_check = (iteration / F + 1) * F - 1;
-      last = std::min(next_check, o.max_iterations - 1);
+      // A rolling stack checks every case's own limit at the checks.
+      last = queue != nullptr ? next_check : std::min(next_check, o.max_iterations - 1);
       is_check = (last == next_check);
       len = last - iteration + 1;
       upload_params(len);
@@ -1359,6 +1621,8 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& cases,
 
     // ------------------------------------------------------------- check
     const int32_t it_idx = last;
+    std::vector<char> was_active(K);
+    for (int k = 0; k < K; ++k) was_active[k] = S[k].active ? 1 : 0;
     bool any_avg = false;
     for (int k = 0; k < K; ++k) any_avg = any_avg || (S[k].active && averaging && S[k].sum_weight > 0.0);
     const bool fresh_kx = !fp64 || !o.reuse_products;
@@ -1399,7 +1663,7 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& cases,
         if (!bad && (tc[8] - tc[kRowTerms + 7]) / scale > o.infeasibility_tolerance) {
           c.status = ANU_PDHG_PRIMAL_INFEASIBLE;
           set_message(&R[k].r, "Farkas certificate found in the dual iterate difference");
-          c.final_iteration = it_idx + 1;
+          c.final_iteration = it_idx + 1 - origin[k];
           c.active = false;
           continue;
         }
@@ -1422,22 +1686,23 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& cases,
       if (!std::isfinite(r.primal_residual) || !std::isfinite(r.dual_residual)) {
         c.status = ANU_PDHG_NUMERICAL_ERROR;
         set_message(&R[k].r, "iterates stopped being finite");
-        c.final_iteration = it_idx + 1;
+        c.final_iteration = it_idx + 1 - origin[k];
         adopt_mask[k] = c.use_average;
         c.active = false;
         continue;
       }
       if (passes(r)) {
         c.status = ANU_PDHG_OPTIMAL;
-        c.final_iteration = it_idx + 1;
+        c.final_iteration = it_idx + 1 - origin[k];
         adopt_mask[k] = c.use_average;
         c.active = false;
         continue;
       }
+      const int32_t done = it_idx + 1 - origin[k];
       if (polish_on && o.termination == ANU_TERMINATION_FULL &&
-          it_idx + 1 >= c.next_polish_iteration) {
-        while (c.next_polish_iteration <= it_idx + 1) c.next_polish_iteration *= 2;
-        const int32_t budget = polish_budget(o, it_idx);
+          done >= c.next_polish_iteration) {
+        while (c.next_polish_iteration <= done) c.next_polish_iteration *= 2;
+        const int32_t budget = polish_budget(o, done - 1);
         if (r.relative_gap <= gap_tolerance && budget > 0) polish_cases.push_back(k);
       }
     }
@@ -1466,16 +1731,39 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& cases,
           }
         }
       }
-      std::vector<std::vector<double>> sx, sy;
-      for (int k : polish_cases) {
-        sx.push_back(S[k].use_average ? avg_x[k] : cur_x[k]);
-        sy.push_back(S[k].use_average ? avg_y[k] : cur_y[k]);
+      // One primal and one dual sub-stack per budget (the cases of a stack
+      // started together share one; a rolling stack's may differ).
+      const size_t P = polish_cases.size();
+      std::vector<std::vector<double>> pxs(P), pys(P), px(P), py(P);
+      std::vector<anu_pdhg_residual> pr(P);
+      std::vector<int32_t> spent(P);
+      std::map<int32_t, std::vector<size_t>> groups;
+      for (size_t i = 0; i < P; ++i)
+        groups[polish_budget(o, it_idx - origin[polish_cases[i]])].push_back(i);
+      for (const auto& group : groups) {
+        std::vector<int> which;
+        std::vector<std::vector<double>> sx, sy;
+        for (size_t i : group.second) {
+          const int k = polish_cases[i];
+          which.push_back(k);
+          sx.push_back(S[k].use_average ? avg_x[k] : cur_x[k]);
+          sy.push_back(S[k].use_average ? avg_y[k] : cur_y[k]);
+        }
+        std::vector<std::vector<double>> gxs, gys, gx, gy;
+        std::vector<anu_pdhg_residual> gr;
+        std::vector<int32_t> gs;
+        run_polish<T>(p, unit, cases, which, sx, sy, group.first, S, o, start_time, &gxs, &gys,
+                      &gx, &gy, &gr, &gs);
+        for (size_t g = 0; g < group.second.size(); ++g) {
+          const size_t i = group.second[g];
+          pxs[i] = std::move(gxs[g]);
+          pys[i] = std::move(gys[g]);
+          px[i] = std::move(gx[g]);
+          py[i] = std::move(gy[g]);
+          pr[i] = gr[g];
+          spent[i] = gs[g];
+        }
       }
-      std::vector<std::vector<double>> pxs, pys, px, py;
-      std::vector<anu_pdhg_residual> pr;
-      std::vector<int32_t> spent;
-      run_polish<T>(p, unit, cases, polish_cases, sx, sy, polish_budget(o, it_idx), S, o,
-                    start_time, &pxs, &pys, &px, &py, &pr, &spent);
       t_polish += phase_end();
       for (size_t i = 0; i < polish_cases.size(); ++i) {
         const int k = polish_cases[i];
@@ -1492,7 +1780,7 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& cases,
           R[k].r.polished = 1;
           c.status = ANU_PDHG_OPTIMAL;
           set_message(&R[k].r, "converged after feasibility polishing");
-          c.final_iteration = it_idx + 1;
+          c.final_iteration = it_idx + 1 - origin[k];
           c.active = false;
         }
       }
@@ -1511,7 +1799,7 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& cases,
       for (int k = 0; k < K; ++k) {
         if (!S[k].active) continue;
         S[k].status = ANU_PDHG_TIME_LIMIT;
-        S[k].final_iteration = it_idx + 1;
+        S[k].final_iteration = it_idx + 1 - origin[k];
         adopt_mask[k] = S[k].use_average;
         S[k].active = false;
       }
@@ -1533,7 +1821,7 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& cases,
       const bool sufficient = measure <= 0.2 * at_restart;
       const bool necessary = measure <= 0.8 * at_restart && measure > previous;
       const bool too_long = static_cast<double>(c.iterations_since_restart) >=
-                            0.36 * static_cast<double>(it_idx + 1);
+                            0.36 * static_cast<double>(it_idx + 1 - origin[k]);
       c.last_candidate_kkt = candidate_kkt[k];
       c.last_residual = residual;
       if (!(sufficient || necessary || too_long)) continue;
@@ -1599,120 +1887,40 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& cases,
       ANU_CUDA(cudaStreamSynchronize(st));
     }
     recenter();
+    if (queue != nullptr) {
+      // Every case's own iteration limit; then the slots freed at this check
+      // hand their results over and take the next waiting cases.
+      for (int k = 0; k < K; ++k)
+        if (S[k].active && it_idx + 1 - origin[k] >= o.max_iterations) {
+          S[k].status = ANU_PDHG_ITERATION_LIMIT;
+          S[k].final_iteration = it_idx + 1 - origin[k];
+          S[k].active = false;
+        }
+      std::vector<int> retired;
+      for (int k = 0; k < K; ++k)
+        if (was_active[k] && !S[k].active && queue->slot_index[k] >= 0) retired.push_back(k);
+      if (!retired.empty()) {
+        t_checks += phase_end();
+        finalize(retired);
+        for (int k : retired) {
+          if (queue->next >= queue->pending.size()) break;
+          admit(k, queue->pending_index[queue->next], queue->pending[queue->next]);
+          ++queue->next;
+        }
+      }
+    }
     t_checks += phase_end();
   }
   for (int k = 0; k < K; ++k)
     if (S[k].active) {
-      S[k].final_iteration = iteration;
+      S[k].final_iteration = iteration - origin[k];
       S[k].status = ANU_PDHG_ITERATION_LIMIT;
     }
 
-  // Results (pdhg.cpp:1205-1285).
-  std::vector<std::vector<double>> fx, fy;
-  download_all(st, w.x, n, K, &fx);
-  download_all(st, w.y, m, K, &fy);
-  if (refine) {
-    // The answer is base + offset.
-    std::vector<std::vector<double>> bx, by;
-    download_all(st, w.xb, n, K, &bx);
-    download_all(st, w.yb, m, K, &by);
-    for (int k = 0; k < K; ++k) {
-      for (int32_t j = 0; j < n; ++j) fx[k][j] += bx[k][j];
-      for (int32_t i = 0; i < m; ++i) fy[k][i] += by[k][i];
-    }
-  }
-  std::vector<double> fterms;
-  eval_points_terms(p, unit, K, cases, fx, fy, &fterms);
-  std::vector<int> exit_polish;
-  for (int k = 0; k < K; ++k) {
-    CaseState& c = S[k];
-    CaseResult& cr = R[k];
-    if (c.have_polished) {
-      cr.x = c.polished_x;
-      cr.y = c.polished_y;
-      cr.r.residual = c.polished_residual;
-      continue;
-    }
-    cr.xs = fx[k];
-    cr.ys = fy[k];
-    cr.x.resize(n);
-    cr.y.resize(m);
-    for (int32_t j = 0; j < n; ++j) cr.x[j] = unit ? fx[k][j] : p.scaling.col_scale[j] * fx[k][j];
-    for (int32_t i = 0; i < m; ++i) cr.y[i] = unit ? fy[k][i] : p.scaling.row_scale[i] * fy[k][i];
-    cr.r.residual = residual_from_terms(&fterms[static_cast<size_t>(k) * kCheckTerms],
-                                        &fterms[static_cast<size_t>(k) * kCheckTerms + kRowTerms],
-                                        c.scales);
-    const bool worth = polish_on && o.polish_on_exit &&
-                       o.termination == ANU_TERMINATION_FULL && c.status != ANU_PDHG_OPTIMAL &&
-                       c.status != ANU_PDHG_PRIMAL_INFEASIBLE &&
-                       c.status != ANU_PDHG_NUMERICAL_ERROR &&
-                       std::isfinite(cr.r.residual.primal_residual) &&
-                       std::isfinite(cr.r.residual.dual_residual) &&
-                       now_seconds() - start_time < o.time_limit_seconds;
-    if (worth && polish_budget(o, c.final_iteration) > 0) exit_polish.push_back(k);
-  }
-  if (!exit_polish.empty()) {
-    // All cases that reach here stopped at the same iteration count.
-    std::vector<std::vector<double>> sx, sy;
-    for (int k : exit_polish) {
-      sx.push_back(fx[k]);
-      sy.push_back(fy[k]);
-    }
-    std::vector<std::vector<double>> pxs, pys, px, py;
-    std::vector<anu_pdhg_residual> pr;
-    std::vector<int32_t> spent;
-    run_polish<T>(p, unit, cases, exit_polish, sx, sy, polish_budget(o, S[exit_polish[0]].final_iteration),
-                  S, o, start_time, &pxs, &pys, &px, &py, &pr, &spent);
-    t_polish += phase_end();
-    for (size_t i = 0; i < exit_polish.size(); ++i) {
-      const int k = exit_polish[i];
-      CaseResult& cr = R[k];
-      ++cr.r.polish_attempts;
-      cr.r.polish_iterations += spent[i];
-      const anu_pdhg_residual& cur = cr.r.residual;
-      const anu_pdhg_residual& tr = pr[i];
-      const double gap_ceiling = std::fmax(gap_tolerance, cur.relative_gap);
-      const bool improved = tr.relative_primal <= cur.relative_primal &&
-                            tr.relative_dual <= cur.relative_dual &&
-                            (tr.relative_primal < cur.relative_primal ||
-                             tr.relative_dual < cur.relative_dual);
-      if (improved && tr.relative_gap <= gap_ceiling) {
-        cr.x = px[i];
-        cr.y = py[i];
-        cr.xs = pxs[i];
-        cr.ys = pys[i];
-        cr.r.residual = tr;
-        cr.r.polished = 1;
-        if (converged(tr, tolerance, o.absolute_tolerance, inf_norm, gap_tolerance)) {
-          S[k].status = ANU_PDHG_OPTIMAL;
-          set_message(&cr.r, "converged after feasibility polishing");
-        } else if (cr.r.message[0] == '\0') {
-          set_message(&cr.r, "feasibility polished");
-        } else {
-          set_message(&cr.r, std::string(cr.r.message) + ", feasibility polished");
-        }
-      }
-    }
-  }
-  t_checks += phase_end();
-  for (int k = 0; k < K; ++k) {
-    CaseResult& cr = R[k];
-    double cx = 0.0;
-    for (int32_t j = 0; j < n; ++j) cx += cases[k]->c[j] * cr.x[j];
-    cr.r.objective = cases[k]->objective_scale * cx + cases[k]->objective_offset;
-    cr.r.iterations = S[k].final_iteration;
-    cr.r.status = S[k].status;
-    cr.r.final_step_size = S[k].eta;
-    cr.r.final_primal_weight = S[k].omega;
-    cr.r.solve_seconds = now_seconds() - start_time;
-    cr.r.phases.setup = t_setup;
-    cr.r.phases.iterating = t_iter;
-    cr.r.phases.checks = t_checks;
-    cr.r.phases.polishing = t_polish;
-    cr.r.kernel_launches = static_cast<int32_t>(p.launches - launches0);
-    cr.r.device_iteration_seconds = device_iter_s;
-    cr.r.device_iterations = device_iters;
-  }
+  std::vector<int> remaining;
+  for (int k = 0; k < K; ++k)
+    if (queue == nullptr || queue->slot_index[k] >= 0) remaining.push_back(k);
+  finalize(remaining);
 }
 
 }  // namespace
@@ -1740,6 +1948,41 @@ void run_cases(Problem& problem, const std::vector<const CaseData*>& cases,
   else
     run_cases_t<double>(problem, cases, options, warm_x, warm_y, results, start_time,
                         problem.unit_scaling);
+}
+
+void run_cases_rolling(Problem& problem, const std::vector<const CaseData*>& cases, int slots,
+                       const anu_pdhg_options& options, std::vector<CaseResult>* results,
+                       double start_time) {
+  ANU_CUDA(cudaSetDevice(problem.device));
+  PoolScope scope(&problem.pool, problem.stream);
+  const int total = static_cast<int>(cases.size());
+  const int K = std::max(1, std::min(slots, total));
+  results->assign(total, CaseResult{});
+  AdmissionQueue queue;
+  queue.out = results;
+  std::vector<const CaseData*> first(cases.begin(), cases.begin() + K);
+  for (int k = 0; k < K; ++k) queue.slot_index.push_back(k);
+  for (int i = K; i < total; ++i) {
+    queue.pending.push_back(cases[i]);
+    queue.pending_index.push_back(i);
+  }
+  std::vector<CaseResult> slot_results;
+  std::vector<const std::vector<double>*> none(K, nullptr);
+  if (problem.precision == ANU_PRECISION_FP32)
+    run_cases_t<float>(problem, first, options, none, none, &slot_results, start_time,
+                       problem.unit_scaling, nullptr, nullptr, &queue);
+  else
+    run_cases_t<double>(problem, first, options, none, none, &slot_results, start_time,
+                        problem.unit_scaling, nullptr, nullptr, &queue);
+  // Cases the time limit (or a stop request) kept from ever starting.
+  for (size_t i = queue.next; i < queue.pending.size(); ++i) {
+    CaseResult& r = (*results)[queue.pending_index[i]];
+    r.r.status = ANU_PDHG_TIME_LIMIT;
+    set_message(&r.r, "not started: the time limit ended the stack first");
+    r.x.assign(problem.n, 0.0);
+    r.y.assign(problem.m, 0.0);
+    r.r.matrix_norm_estimate = problem.matrix_norm;
+  }
 }
 
 }  // namespace anu
@@ -1993,20 +2236,22 @@ int anu_pdhg_batch_solve(anu_pdhg_batch* h, double* x, double* y, anu_pdhg_resul
     if (h == nullptr || results == nullptr) throw Error(ANU_ERR_INVALID, "null argument");
     const int32_t n = h->problem->n, m = h->problem->m;
     const int total = static_cast<int>(h->cases.size());
-    // Stacks larger than one run's capacity go through in slices.
-    for (int base = 0; base < total; base += anu::kMaxCasesPerRun) {
-      const int count = std::min(anu::kMaxCasesPerRun, total - base);
-      const double start = anu::now_seconds();
-      std::vector<const anu::CaseData*> cs(count);
-      for (int k = 0; k < count; ++k) cs[k] = &h->cases[base + k];
-      std::vector<const std::vector<double>*> none(count, nullptr);
-      std::vector<anu::CaseResult> res;
+    const double start = anu::now_seconds();
+    std::vector<const anu::CaseData*> cs(total);
+    for (int k = 0; k < total; ++k) cs[k] = &h->cases[k];
+    std::vector<anu::CaseResult> res;
+    if (total <= anu::kMaxCasesPerRun) {
+      std::vector<const std::vector<double>*> none(total, nullptr);
       anu::run_cases(*h->problem, cs, h->options, none, none, &res, start);
-      for (int k = 0; k < count; ++k) {
-        fill_result(*h->problem, res[k], h->scaling_seconds, h->norm_seconds, &results[base + k]);
-        if (x) std::copy(res[k].x.begin(), res[k].x.end(), x + static_cast<size_t>(base + k) * n);
-        if (y) std::copy(res[k].y.begin(), res[k].y.end(), y + static_cast<size_t>(base + k) * m);
-      }
+    } else {
+      // More cases than one run carries: a rolling stack of that many slots,
+      // each slot taking the next waiting case as soon as its case retires.
+      anu::run_cases_rolling(*h->problem, cs, anu::kMaxCasesPerRun, h->options, &res, start);
+    }
+    for (int k = 0; k < total; ++k) {
+      fill_result(*h->problem, res[k], h->scaling_seconds, h->norm_seconds, &results[k]);
+      if (x) std::copy(res[k].x.begin(), res[k].x.end(), x + static_cast<size_t>(k) * n);
+      if (y) std::copy(res[k].y.begin(), res[k].y.end(), y + static_cast<size_t>(k) * m);
     }
   });
 }

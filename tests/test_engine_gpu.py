@@ -235,6 +235,36 @@ def test_case_stack_fp32_reaches_tolerance(engine, stack):
             assert abs(r.objective - ref_obj) <= 1e-5 * abs(ref_obj)
 
 
+def _rolling(stack, idx):
+    return lpgen.CaseStack(stack.base, [stack.names[i] for i in idx], stack.c[idx], stack.q[idx],
+                           stack.lower[idx], stack.upper[idx])
+
+
+def test_rolling_stack_fp64_matches_lockstep(engine, stack):
+    # 90 cases (the 60 and the first 30 again) exceed one run's 64 slots: the
+    # stack rolls, each freed slot admitting the next case at a check. Every
+    # case runs its own iteration from its admission, so it must end as in
+    # the 60-case lockstep stack.
+    idx = list(range(60)) + list(range(30))
+    res = engine.solve_case_stack(_rolling(stack, idx), tolerance=1e-6)
+    ref = engine.solve_case_stack(stack, tolerance=1e-6)
+    assert len(res) == 90
+    for i, k in enumerate(idx):
+        assert res[i].status == ref[k].status == OPTIMAL, (i, k)
+        assert abs(res[i].iterations - ref[k].iterations) <= 80, (i, k)
+        assert abs(res[i].objective - ref[k].objective) <= 1e-8 * abs(ref[k].objective), (i, k)
+
+
+def test_rolling_stack_fp32_admitted_cases_converge(engine, stack):
+    idx = list(range(60)) + [16, 33, 45, 55, 0, 7, 21]
+    res = engine.solve_case_stack(_rolling(stack, idx), tolerance=1e-6, precision=PRECISION_FP32)
+    for i in range(60, len(idx)):
+        k = idx[i]
+        assert res[i].status == OPTIMAL, (i, res[i].message)
+        r = oracle.oracle_residual(stack.case(k), res[i].x, res[i].y)
+        assert r.converged(1e-6), (k, r)
+
+
 def test_case_stack_equals_single_solves(engine, stack):
     sub = lpgen.CaseStack(stack.base, stack.names[:5], stack.c[:5], stack.q[:5],
                           stack.lower[:5], stack.upper[:5])
