@@ -1018,7 +1018,11 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
   Pinned<double> h_w(static_cast<size_t>(std::max(F, 1)) * K);
   Pinned<double> h_terms(static_cast<size_t>(kCheckTerms) * K * 2);
   Pinned<double> h_kkt(static_cast<size_t>(kKktTerms) * K * 2);
-  Pinned<int32_t> h_mask(K);
+  // Case masks go up through a ring of pinned staging slots, so a new mask
+  // never waits for the copy of the previous one.
+  constexpr int kMaskSlots = 4;
+  Pinned<int32_t> h_mask(static_cast<size_t>(K) * kMaskSlots);
+  int mask_slot = 0;
   Pinned<double> h_weights(K);
 
 
@@ -1132,16 +1136,25 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
       if (b) cudaEventDestroy(b);
     }
   } event_guard{ev_begin, ev_end};
+  // With profiling, the chunk's events are read once the stream has passed
+  // them (at the next read-back), so timing adds no wait of its own.
+  int pending_timed = 0;
+  auto collect_chunk_time = [&]() {
+    if (!o.profile || pending_timed == 0) return;
+    ANU_CUDA(cudaEventSynchronize(ev_end));
+    float ms = 0.0f;
+    ANU_CUDA(cudaEventElapsedTime(&ms, ev_begin, ev_end));
+    device_iter_s += 1e-3 * ms;
+    device_iters += pending_timed;
+    pending_timed = 0;
+  };
   auto run_chunk = [&](int len, bool check_at_end) {
+    collect_chunk_time();
     if (o.profile) ANU_CUDA(cudaEventRecord(ev_begin, st));
     run_chunk_body(len, check_at_end);
     if (o.profile) {
       ANU_CUDA(cudaEventRecord(ev_end, st));
-      ANU_CUDA(cudaEventSynchronize(ev_end));
-      float ms = 0.0f;
-      ANU_CUDA(cudaEventElapsedTime(&ms, ev_begin, ev_end));
-      device_iter_s += 1e-3 * ms;
-      device_iters += len;
+      pending_timed = len;
     }
   };
 
@@ -1194,10 +1207,13 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
   };
 
   auto set_mask = [&](const std::vector<int32_t>& mk) {
-    // The pinned staging buffer may still feed an earlier copy.
-    ANU_CUDA(cudaStreamSynchronize(st));
-    for (int k = 0; k < K; ++k) h_mask.p[k] = mk[k];
-    ANU_CUDA(cudaMemcpyAsync(w.mask.p, h_mask.p, sizeof(int32_t) * K, cudaMemcpyHostToDevice, st));
+    // Wrapping around the ring, the slot about to be refilled may still feed
+    // a copy: drain the stream first.
+    mask_slot = (mask_slot + 1) % kMaskSlots;
+    if (mask_slot == 0) ANU_CUDA(cudaStreamSynchronize(st));
+    int32_t* h = h_mask.p + static_cast<size_t>(mask_slot) * K;
+    for (int k = 0; k < K; ++k) h[k] = mk[k];
+    ANU_CUDA(cudaMemcpyAsync(w.mask.p, h, sizeof(int32_t) * K, cudaMemcpyHostToDevice, st));
   };
 
   // Adopting the averaged candidate moves it on the device (pdhg.cpp:981-987).
@@ -1208,7 +1224,6 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
     set_mask(mk);
     masked_copy<T, T>(p, n, K, w.mask.p, w.avg_x.p, w.x.p);
     masked_copy<T, T>(p, m, K, w.mask.p, w.avg_y.p, w.y.p);
-    ANU_CUDA(cudaStreamSynchronize(st));
   };
 
   std::vector<CaseResult>* R_ptr = results;
@@ -1647,6 +1662,7 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
       ANU_CUDA(cudaMemcpyAsync(h_kkt.p, w.kkt.p, sizeof(double) * kKktTerms * K * (any_avg ? 2 : 1),
                                cudaMemcpyDeviceToHost, st));
     ANU_CUDA(cudaStreamSynchronize(st));
+    collect_chunk_time();
 
     std::vector<int32_t> adopt_mask(K, 0);
     std::vector<anu_pdhg_residual> rr(K);
@@ -1884,7 +1900,6 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
         masked_fill<T>(p, n, K, w.mask.p, static_cast<T>(0), w.sum_x.p);
         masked_fill<T>(p, m, K, w.mask.p, static_cast<T>(0), w.sum_y.p);
       }
-      ANU_CUDA(cudaStreamSynchronize(st));
     }
     recenter();
     if (queue != nullptr) {
@@ -1917,6 +1932,7 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
       S[k].status = ANU_PDHG_ITERATION_LIMIT;
     }
 
+  collect_chunk_time();
   std::vector<int> remaining;
   for (int k = 0; k < K; ++k)
     if (queue == nullptr || queue->slot_index[k] >= 0) remaining.push_back(k);

@@ -21,6 +21,8 @@ Two side measurements ride on the stack line:
   * `fp64_single_case`: the same 60 cases solved one at a time by the
     engine's plain FP64 mode - the plain FP64 single-case GPU PDHG the batched
     mixed-precision run is compared with.
+  * `stream`: 240 cases (the 60, four times) through a rolling stack of 64
+    slots, each freed slot admitting the next case in place.
 
 `--workload packed` times the packed batch of 256 unequal LPs instead, and
 `--workload adjoint` the unrolled-PDHG sensitivities of the 60-case stack;
@@ -308,6 +310,31 @@ def run_adjoint(args, rank, world, local_rank):
     return out
 
 
+def stream_leg(st, opts, copies=4):
+    """A stack of copies x 60 cases (more than one run's 64 slots), solved as a
+    rolling stack: a slot freed by a converged case admits the next waiting
+    case at once. Timed after one warm-up solve; device-resident handle."""
+    import torch
+    from anukulan_b200 import pdhg
+    from anukulan_b200.abi import OPTIMAL
+    c = np.concatenate([st.c] * copies)
+    q = np.concatenate([st.q] * copies)
+    lo = np.concatenate([st.lower] * copies)
+    hi = np.concatenate([st.upper] * copies)
+    solver = pdhg.CaseStackSolver(st.base, c, q, lo, hi, opts)
+    solver.solve()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    res = solver.solve()
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    solver.close()
+    ok = sum(int(r.status == OPTIMAL) for r in res)
+    return {"cases": len(res), "slots": 64, "optimal": ok, "seconds": dt, "value": ok / dt,
+            "unit": "solves/s",
+            "mode": "rolling stack: retired slots admit waiting cases at termination checks"}
+
+
 def fp64_single_case(st, device):
     """The stack's cases solved one after another by the engine's plain FP64
     single-case mode (host arrays in, results out, like a solve_pdhg call)."""
@@ -467,6 +494,7 @@ def run_engine(args, rank, world, local_rank):
         if args.side:
             out["spmv"] = spmv_leg(args.spmv_iterations, local_rank, peak)
             out["fp64_single_case"] = fp64_single_case(st, local_rank)
+            out["stream"] = stream_leg(st, opts)
         if args.cpu_baseline:
             out["cpu_baseline"] = cpu_baseline(st, seconds=args.cpu_seconds)
     if dist is not None:
