@@ -550,7 +550,7 @@ def run_reference(args, rank, world):
             per_step.append(r)
             solved += 1
     value = float(np.mean([r["value"] for r in per_step]))
-    return {
+    out = {
         "impl": "reference",
         "metric": "LP solves/s to relative KKT 1e-6 (batched FP32 PDHG, FP64 checks)",
         "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
@@ -563,6 +563,30 @@ def run_reference(args, rank, world):
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
+    if args.gpu_reference and oracle.have_reference_cuda():
+        out["gpu_reference"] = reference_gpu_leg(st)
+    return out
+
+
+def reference_gpu_leg(st, cases=None):
+    """The reference's own FP64 GPU PDHG (its cuda_backend.cu, built for
+    sm_100a into oracle/_ref) solving the stack's cases one at a time: the
+    plain FP64 single-case GPU PDHG."""
+    import oracle
+    from anukulan_b200.abi import OPTIMAL
+    ks = range(st.num_cases) if cases is None else cases
+    oracle.ref_cuda_solve(st.case(0), tolerance=TOL)  # context and module load
+    t0 = time.perf_counter()
+    ok = 0
+    iters = 0
+    for k in ks:
+        r = oracle.ref_cuda_solve(st.case(k), tolerance=TOL)
+        ok += int(r.status == OPTIMAL)
+        iters += r.iterations
+    dt = time.perf_counter() - t0
+    return {"value": ok / dt, "unit": "solves/s", "cases": len(ks), "optimal": ok,
+            "seconds": dt, "iterations_per_second": iters / dt,
+            "mode": "reference solve_pdhg on its cuda_backend, FP64, one case per call"}
 
 
 def main(argv=None):
@@ -574,6 +598,8 @@ def main(argv=None):
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--ref-seconds", type=float, default=10.0)
+    ap.add_argument("--no-gpu-reference", dest="gpu_reference", action="store_false",
+                    help="reference arm: skip the reference's own CUDA backend leg")
     ap.add_argument("--no-e2e", dest="e2e", action="store_false",
                     help="skip the end-to-end pass (profiling runs)")
     ap.add_argument("--workload", default="stack",

@@ -2,6 +2,8 @@
 
 * :func:`oracle_lib` - ``liboracle.so``, the C restatement of the reference
   PDHG path (pdhg_oracle.c). Always present once built.
+* :func:`ref_cuda_lib` - ``_ref/libanuref_cuda.so``, the same with the
+  reference's own CUDA backend (the plain FP64 single-case GPU PDHG).
 * :func:`ref_lib` - ``_ref/libanuref.so``, the reference's own sources compiled
   by oracle/Makefile, present where the reference tree was available at build
   time (the built file travels with the working tree).
@@ -26,23 +28,25 @@ from anukulan_b200.model import StandardLp
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libanuref.so")
+REF_CUDA_SO = os.path.join(HERE, "_ref", "libanuref_cuda.so")
 REF_SRC = "/root/reference/src/anukulan/pdhg.cpp"
 
 _oracle = None
 _ref = None
+_ref_cuda = None
 
 _P = C.POINTER
 
 
 def build(with_reference: Optional[bool] = None) -> None:
-    """Builds liboracle.so, and _ref/libanuref.so when the reference sources
-    are present (or `with_reference` is True)."""
+    """Builds liboracle.so, and _ref/libanuref.so and _ref/libanuref_cuda.so
+    when the reference sources are present (or `with_reference` is True)."""
     import subprocess
     subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
     if with_reference is None:
         with_reference = os.path.exists(REF_SRC)
     if with_reference:
-        subprocess.run(["make", "-s", "-j8", "-C", HERE, "ref"], check=True)
+        subprocess.run(["make", "-s", "-j8", "-C", HERE, "ref", "ref_cuda"], check=True)
 
 
 def _declare(lib, name, restype, argtypes):
@@ -125,6 +129,39 @@ def oracle_solve(lp: StandardLp, options=None, warm_x=None, warm_y=None, **kw) -
     wy = None if warm_y is None else np.ascontiguousarray(warm_y, np.float64)
     oracle_lib().oracle_pdhg_solve(cl.ref(), C.byref(o), f64_ptr(wx), f64_ptr(wy),
                                    f64_ptr(x), f64_ptr(y), C.byref(r))
+    return PdhgResult.from_c(r, x, y)
+
+
+def have_reference_cuda() -> bool:
+    return os.path.exists(REF_CUDA_SO)
+
+
+def ref_cuda_lib():
+    """_ref/libanuref_cuda.so: the reference with its own CUDA backend."""
+    global _ref_cuda
+    if _ref_cuda is None:
+        if not os.path.exists(REF_CUDA_SO):
+            raise FileNotFoundError("oracle/_ref/libanuref_cuda.so is not built")
+        lib = C.CDLL(REF_CUDA_SO)
+        _declare(lib, "ref_pdhg_solve", C.c_int,
+                 [C.c_void_p, _P(anu_pdhg_options), C.c_int, _P(C.c_double),
+                  _P(C.c_double), _P(C.c_double), _P(C.c_double), _P(anu_pdhg_result)])
+        _ref_cuda = lib
+    return _ref_cuda
+
+
+def ref_cuda_solve(lp: StandardLp, options=None, **kw) -> PdhgResult:
+    """The reference's own solve_pdhg on its CUDA backend (cuda_backend.cu,
+    FP64, one LP per call)."""
+    cl = CLp(lp)
+    o = _opts(options, **kw)
+    x = np.zeros(cl.n)
+    y = np.zeros(cl.m)
+    r = anu_pdhg_result()
+    rc = ref_cuda_lib().ref_pdhg_solve(cl.ref(), C.byref(o), -2, None, None, f64_ptr(x),
+                                       f64_ptr(y), C.byref(r))
+    if rc != 0:
+        raise RuntimeError(r.message.decode())
     return PdhgResult.from_c(r, x, y)
 
 

@@ -12,6 +12,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <stdexcept>
 #include <string>
 #include <vector>
 
@@ -139,9 +140,18 @@ int ref_pdhg_solve(const anu_lp* lp_in, const anu_pdhg_options* opt_in,
   try {
     const anukulan::StandardLp lp = to_lp(*lp_in);
     anukulan::PdhgOptions options = to_options(*opt_in);
-    if (threads < 0) threads = anukulan::default_thread_count();
-    options.backend = threads <= 1 ? &anukulan::cpu_backend()
-                                   : &anukulan::threaded_cpu_backend(threads);
+    if (threads == -2) {
+#ifdef ANUKULAN_WITH_CUDA
+      // The reference's own GPU backend (src/anukulan/cuda_backend.cu).
+      options.backend = &anukulan::cuda_backend();
+#else
+      throw std::runtime_error("this build of the reference has no CUDA backend");
+#endif
+    } else {
+      if (threads < 0) threads = anukulan::default_thread_count();
+      options.backend = threads <= 1 ? &anukulan::cpu_backend()
+                                     : &anukulan::threaded_cpu_backend(threads);
+    }
     std::vector<double> wx, wy;
     if (warm_x != nullptr && warm_y != nullptr) {
       wx.assign(warm_x, warm_x + lp_in->k.cols);
