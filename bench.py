@@ -10,7 +10,7 @@ on the device; `e2e` is the same metric through the C ABI from host arrays
 (create + solve + download inside the timed region).
 
     python bench.py [--gpus N --steps K --warmup W] [--impl reference]
-                    [--workload stack|spmv|packed|adjoint]
+                    [--workload stack|spmv|packed|adjoint|powerlaw]
 
 Two side measurements ride on the stack line:
   * `spmv`: the single-LP iteration (the two fused SpMV kernels) on the
@@ -24,9 +24,10 @@ Two side measurements ride on the stack line:
   * `stream`: 240 cases (the 60, four times) through a rolling stack of 64
     slots, each freed slot admitting the next case in place.
 
-`--workload packed` times the packed batch of 256 unequal LPs instead, and
-`--workload adjoint` the unrolled-PDHG sensitivities of the 60-case stack;
-each prints its own JSON line.
+`--workload packed` times the packed batch of 256 unequal LPs instead,
+`--workload adjoint` the unrolled-PDHG sensitivities of the 60-case stack, and
+`--workload powerlaw --tolerance T` whole solves of the power-law LP in FP32
+(with refinement) and FP64; each prints its own JSON line.
 
 Under torchrun every rank solves its own copy of the stack (weak scaling, no
 collective on the data path); rank 0 prints one JSON line. `--impl reference`
@@ -335,6 +336,41 @@ def stream_leg(st, opts, copies=4):
             "mode": "rolling stack: retired slots admit waiting cases at termination checks"}
 
 
+def run_powerlaw(args, rank, world, local_rank):
+    """Whole solves of the 200,000 x 300,000 power-law LP to --tolerance: FP64
+    iterates against FP32 iterates with FP64 checks and refinement. A step
+    is one solve in each precision (no warm-up: each solve is long)."""
+    if rank != 0:
+        return None
+    import torch
+    from anukulan_b200 import lpgen, pdhg
+    from anukulan_b200.abi import PRECISION_FP32, PRECISION_FP64, make_options
+    torch.cuda.set_device(local_rank)
+    lp, objective = lpgen.power_law_lp()
+    out = {"metric": f"power-law LP solve to relative KKT {args.tolerance:g}",
+           "unit": "seconds", "higher_is_better": False, "n_gpus": 1,
+           "config": {"workload": "powerlaw_lp", "rows": lp.num_rows, "cols": lp.num_cols,
+                      "nnz": lp.k.nnz, "tolerance": args.tolerance},
+           "data": "synthetic (seeded generator, planted optimum c'x0)"}
+    for name, prec in (("fp32", PRECISION_FP32), ("fp64", PRECISION_FP64)):
+        opts = make_options(tolerance=args.tolerance, precision=prec, device=local_rank,
+                            max_iterations=5_000_000, time_limit_seconds=args.time_limit,
+                            profile=1)
+        t0 = time.perf_counter()
+        r = pdhg.solve_pdhg(lp, opts)
+        dt = time.perf_counter() - t0
+        out[name] = {"status": r.status, "iterations": r.iterations, "seconds": dt,
+                     "restarts": r.restarts, "polished": bool(r.polished),
+                     "relative_primal": r.residual.relative_primal,
+                     "relative_dual": r.residual.relative_dual,
+                     "relative_gap": r.residual.relative_gap,
+                     "objective_error": abs(r.objective - objective) / abs(objective),
+                     "us_per_iteration_device": 1e6 * r.device_iteration_seconds
+                     / max(r.device_iterations, 1)}
+    out["value"] = out["fp32"]["seconds"]
+    return out
+
+
 def fp64_single_case(st, device):
     """The stack's cases solved one after another by the engine's plain FP64
     single-case mode (host arrays in, results out, like a solve_pdhg call)."""
@@ -603,7 +639,11 @@ def main(argv=None):
     ap.add_argument("--no-e2e", dest="e2e", action="store_false",
                     help="skip the end-to-end pass (profiling runs)")
     ap.add_argument("--workload", default="stack",
-                    choices=["stack", "spmv", "packed", "adjoint"])
+                    choices=["stack", "spmv", "packed", "adjoint", "powerlaw"])
+    ap.add_argument("--tolerance", type=float, default=1e-6,
+                    help="--workload powerlaw: relative KKT tolerance")
+    ap.add_argument("--time-limit", type=float, default=300.0,
+                    help="--workload powerlaw: seconds per solve")
     ap.add_argument("--packed-workers", type=int, default=0,
                     help="LPs in flight for --workload packed (0: autotune)")
     ap.add_argument("--spmv-iterations", type=int, default=2000)
@@ -619,6 +659,8 @@ def main(argv=None):
         out = run_packed(args, rank, world, local_rank)
     elif args.workload == "adjoint":
         out = run_adjoint(args, rank, world, local_rank)
+    elif args.workload == "powerlaw":
+        out = run_powerlaw(args, rank, world, local_rank)
     elif args.workload == "spmv":
         out = None
         if rank == 0:
