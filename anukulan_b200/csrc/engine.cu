@@ -16,6 +16,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <thread>
 #include <utility>
 
 #include "engine.hpp"
@@ -346,6 +347,37 @@ std::unique_ptr<Problem> make_problem(const anu_lp& lp, const anu_pdhg_options& 
   p->matrix_norm = o.known_matrix_norm > 0.0 ? o.known_matrix_norm
                                               : device_matrix_norm(*p, 200, 1e-8);
   if (norm_seconds) *norm_seconds = now_seconds() - t0;
+  return p;
+}
+
+std::unique_ptr<Problem> clone_problem(const Problem& src) {
+  ANU_CUDA(cudaSetDevice(src.device));
+  auto p = std::make_unique<Problem>();
+  p->device = src.device;
+  ANU_CUDA(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
+  p->owns_stream = true;
+  p->m = src.m;
+  p->n = src.n;
+  p->num_eq = src.num_eq;
+  p->precision = src.precision;
+  p->k = src.k;
+  p->kt = src.kt;
+  p->scaling = src.scaling;
+  p->sweeps = src.sweeps;
+  p->unit_scaling = src.unit_scaling;
+  p->matrix_norm = src.matrix_norm;
+  const bool fp32 = p->precision == ANU_PRECISION_FP32;
+  p->dk.upload(p->k, fp32, p->stream);
+  p->dkt.upload(p->kt, fp32, p->stream);
+  p->row_scale.alloc(std::max(p->m, 1));
+  p->col_scale.alloc(std::max(p->n, 1));
+  if (p->m > 0)
+    ANU_CUDA(cudaMemcpyAsync(p->row_scale.p, p->scaling.row_scale.data(), sizeof(double) * p->m,
+                             cudaMemcpyHostToDevice, p->stream));
+  if (p->n > 0)
+    ANU_CUDA(cudaMemcpyAsync(p->col_scale.p, p->scaling.col_scale.data(), sizeof(double) * p->n,
+                             cudaMemcpyHostToDevice, p->stream));
+  ANU_CUDA(cudaStreamSynchronize(p->stream));
   return p;
 }
 
@@ -2051,6 +2083,9 @@ struct anu_pdhg {
 
 struct anu_pdhg_batch {
   std::unique_ptr<anu::Problem> problem;
+  // A second problem on its own stream (same scaled matrix): larger stacks
+  // run as two half-stacks at once, one per problem.
+  std::unique_ptr<anu::Problem> twin;
   std::vector<anu::CaseData> cases;
   anu_pdhg_options options;
   double scaling_seconds = 0.0;
@@ -2234,6 +2269,7 @@ int anu_pdhg_batch_create(const anu_lp* base, int32_t num_cases, const double* c
     auto h = std::make_unique<anu_pdhg_batch>();
     h->options = *options;
     h->problem = anu::make_problem(*base, *options, &h->scaling_seconds, &h->norm_seconds);
+    if (num_cases >= anu::kSplitStack) h->twin = anu::clone_problem(*h->problem);
     h->cases.reserve(num_cases);
     for (int32_t k = 0; k < num_cases; ++k) {
       h->cases.push_back(anu::make_case(
@@ -2253,16 +2289,54 @@ int anu_pdhg_batch_solve(anu_pdhg_batch* h, double* x, double* y, anu_pdhg_resul
     const int32_t n = h->problem->n, m = h->problem->m;
     const int total = static_cast<int>(h->cases.size());
     const double start = anu::now_seconds();
-    std::vector<const anu::CaseData*> cs(total);
-    for (int k = 0; k < total; ++k) cs[k] = &h->cases[k];
-    std::vector<anu::CaseResult> res;
-    if (total <= anu::kMaxCasesPerRun) {
-      std::vector<const std::vector<double>*> none(total, nullptr);
-      anu::run_cases(*h->problem, cs, h->options, none, none, &res, start);
+    // One stack of the given cases on one problem: lockstep up to one run's
+    // capacity, rolling beyond it.
+    auto solve_part = [&](anu::Problem& prob, const std::vector<int>& idx,
+                          std::vector<anu::CaseResult>* out) {
+      std::vector<const anu::CaseData*> cs;
+      for (int k : idx) cs.push_back(&h->cases[k]);
+      if (static_cast<int>(cs.size()) <= anu::kMaxCasesPerRun) {
+        std::vector<const std::vector<double>*> none(cs.size(), nullptr);
+        anu::run_cases(prob, cs, h->options, none, none, out, start);
+      } else {
+        anu::run_cases_rolling(prob, cs, anu::kMaxCasesPerRun, h->options, out, start);
+      }
+    };
+    std::vector<anu::CaseResult> res(total);
+    if (h->twin == nullptr) {
+      std::vector<int> all(total);
+      for (int k = 0; k < total; ++k) all[k] = k;
+      solve_part(*h->problem, all, &res);
     } else {
-      // More cases than one run carries: a rolling stack of that many slots,
-      // each slot taking the next waiting case as soon as its case retires.
-      anu::run_cases_rolling(*h->problem, cs, anu::kMaxCasesPerRun, h->options, &res, start);
+      // Two half-stacks (alternate cases) at once, each on its own problem,
+      // stream and host thread: every iteration kernel is latency-bound, so
+      // two streams of them overlap.
+      std::vector<int> part[2];
+      for (int k = 0; k < total; ++k) part[k % 2].push_back(k);
+      std::vector<anu::CaseResult> out[2];
+      int code = 0;
+      std::string message;
+      std::thread other([&]() {
+        try {
+          solve_part(*h->twin, part[1], &out[1]);
+        } catch (const Error& e) {
+          code = e.code;
+          message = e.what();
+        } catch (const std::exception& e) {
+          code = ANU_ERR_INTERNAL;
+          message = e.what();
+        }
+      });
+      try {
+        solve_part(*h->problem, part[0], &out[0]);
+      } catch (...) {
+        other.join();
+        throw;
+      }
+      other.join();
+      if (code != 0) throw Error(code, message);
+      for (int s = 0; s < 2; ++s)
+        for (size_t i = 0; i < part[s].size(); ++i) res[part[s][i]] = std::move(out[s][i]);
     }
     for (int k = 0; k < total; ++k) {
       fill_result(*h->problem, res[k], h->scaling_seconds, h->norm_seconds, &results[k]);

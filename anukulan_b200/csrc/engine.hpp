@@ -188,6 +188,14 @@ struct CaseResult {
 // estimates ||K~|| unless known_matrix_norm is given.
 std::unique_ptr<Problem> make_problem(const anu_lp& lp, const anu_pdhg_options& o,
                                       double* scaling_seconds, double* norm_seconds);
+// A second problem on its own stream and memory pool with the same scaled
+// matrix (host and device copies), scaling and norm, made without scaling or
+// power iteration again.
+std::unique_ptr<Problem> clone_problem(const Problem& src);
+
+// Case stacks of at least this many cases run as two half-stacks at once.
+constexpr int kSplitStack = 16;
+
 CaseData make_case(const Problem& p, const double* c, const double* q, const double* lower,
                    const double* upper, double objective_scale, double objective_offset);
 

@@ -484,7 +484,11 @@ def run_engine(args, rank, world, local_rank):
     if rank == 0:
         peak, peak_kind = hbm_peak()
         nnz, m, n = st.base.k.nnz, st.base.num_rows, st.base.num_cols
-        bytes_it = algorithmic_bytes_per_iteration(nnz, m, n, st.num_cases, 4, 4)
+        # The engine runs a stack of 16 or more cases as two half-stacks at
+        # once (two streams): a launch carries half the cases, and two are in
+        # flight at a time.
+        per_launch_cases = (st.num_cases + 1) // 2 if st.num_cases >= 16 else st.num_cases
+        bytes_it = algorithmic_bytes_per_iteration(nnz, m, n, per_launch_cases, 4, 4)
         per_launch_s = dev_iter_s / max(dev_iters, 1) / 2.0
         achieved = (bytes_it / 2.0) / per_launch_s / 1e9 if dev_iters else None
         h2d = (st.base.k.nnz * 12 + (st.base.num_rows + 1) * 4
@@ -524,6 +528,8 @@ def run_engine(args, rank, world, local_rank):
                          "peak_source": peak_kind,
                          "kernel": "seg_kernel (fused case-stack SpMM + primal/dual step), mean per launch",
                          "algorithmic_bytes_per_launch": bytes_it / 2.0,
+                         "cases_per_launch": per_launch_cases,
+                         "launches_in_flight": 2 if per_launch_cases < st.num_cases else 1,
                          "launch_seconds": per_launch_s},
             "clocks": clk,
         }
