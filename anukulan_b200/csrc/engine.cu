@@ -651,6 +651,8 @@ void download_all(cudaStream_t s, const DevBuf<T>& src, int32_t len, int K,
 struct AdmissionQueue {
   std::vector<const CaseData*> pending;  // in admission order
   std::vector<int32_t> pending_index;    // their positions in the caller's list
+  // Their warm starts (scaled space, as solve_pdhg takes them), null: cold.
+  std::vector<const std::vector<double>*> pending_warm_x, pending_warm_y;
   size_t next = 0;
   std::vector<int32_t> slot_index;       // the caller's position of each slot's case, -1: none
   std::vector<CaseResult>* out = nullptr;  // results by the caller's position
@@ -1451,7 +1453,8 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
   // Admission of `d` (the caller's case `index`) into the free slot k of a
   // rolling stack, at a termination check: the slot's host state and every
   // case-interleaved device array start over as at the start of a solve.
-  auto admit = [&](int k, int32_t index, const CaseData* d) {
+  auto admit = [&](int k, int32_t index, const CaseData* d, const std::vector<double>* wx,
+                   const std::vector<double>* wy) {
     cases[k] = d;
     queue->slot_index[k] = index;
     origin[k] = iteration;
@@ -1480,9 +1483,18 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
     ol[k] = &d->lower;
     ou[k] = &d->upper;
     oq[k] = &d->q;
-    std::vector<double> x0(n, 0.0);
+    // The starting point as at the start of a solve (pdhg.cpp:481-503).
+    const bool warm = wx != nullptr && wy != nullptr && wx->size() == static_cast<size_t>(n) &&
+                      wy->size() == static_cast<size_t>(m);
+    std::vector<double> x0(n, 0.0), y0(m, 0.0);
+    if (warm) {
+      y0 = *wy;
+      for (int32_t i = p.num_eq; i < m; ++i)
+        if (!(y0[i] > 0.0)) y0[i] = 0.0;
+    }
     for (int32_t j = 0; j < n; ++j) {
-      double v = 0.0;
+      double v = warm ? (*wx)[j] : 0.0;
+      if (!std::isfinite(v)) v = 0.0;
       const double lo = d->ls[j], hi = d->us[j];
       if (v < lo) v = std::isfinite(lo) ? lo : 0.0;
       if (v > hi) v = std::isfinite(hi) ? hi : 0.0;
@@ -1491,7 +1503,7 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
     std::vector<std::vector<T>> staged;
     std::vector<std::vector<double>> staged64;
     upload_slot<T>(st, w.x.p, n, K, k, x0, &staged);
-    zero_slot<T>(st, w.y.p, m, K, k);
+    upload_slot<T>(st, w.y.p, m, K, k, y0, &staged);
     upload_slot<T>(st, w.c.p, n, K, k, d->cs, &staged);
     upload_slot<T>(st, w.lo.p, n, K, k, d->ls, &staged);
     upload_slot<T>(st, w.hi.p, n, K, k, d->us, &staged);
@@ -1512,10 +1524,10 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
     zero_slot<T>(st, w.dx.p, n, K, k);
     zero_slot<T>(st, w.dy.p, m, K, k);
     upload_slot<T>(st, w.x_restart.p, n, K, k, x0, &staged);
-    zero_slot<T>(st, w.y_restart.p, m, K, k);
+    upload_slot<T>(st, w.y_restart.p, m, K, k, y0, &staged);
     if (!o.pid_primal_weight) {
       upload_slot<T>(st, w.x_prev.p, n, K, k, x0, &staged);
-      zero_slot<T>(st, w.y_prev.p, m, K, k);
+      upload_slot<T>(st, w.y_prev.p, m, K, k, y0, &staged);
     }
     zero_slot<T>(st, w.sum_x.p, n, K, k);
     zero_slot<T>(st, w.sum_y.p, m, K, k);
@@ -1951,7 +1963,10 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
         finalize(retired);
         for (int k : retired) {
           if (queue->next >= queue->pending.size()) break;
-          admit(k, queue->pending_index[queue->next], queue->pending[queue->next]);
+          const size_t q = queue->next;
+          admit(k, queue->pending_index[q], queue->pending[q],
+                q < queue->pending_warm_x.size() ? queue->pending_warm_x[q] : nullptr,
+                q < queue->pending_warm_y.size() ? queue->pending_warm_y[q] : nullptr);
           ++queue->next;
         }
       }
@@ -1999,8 +2014,10 @@ void run_cases(Problem& problem, const std::vector<const CaseData*>& cases,
 }
 
 void run_cases_rolling(Problem& problem, const std::vector<const CaseData*>& cases, int slots,
-                       const anu_pdhg_options& options, std::vector<CaseResult>* results,
-                       double start_time) {
+                       const anu_pdhg_options& options,
+                       const std::vector<const std::vector<double>*>& warm_x,
+                       const std::vector<const std::vector<double>*>& warm_y,
+                       std::vector<CaseResult>* results, double start_time) {
   ANU_CUDA(cudaSetDevice(problem.device));
   PoolScope scope(&problem.pool, problem.stream);
   const int total = static_cast<int>(cases.size());
@@ -2010,17 +2027,26 @@ void run_cases_rolling(Problem& problem, const std::vector<const CaseData*>& cas
   queue.out = results;
   std::vector<const CaseData*> first(cases.begin(), cases.begin() + K);
   for (int k = 0; k < K; ++k) queue.slot_index.push_back(k);
+  auto warm_of = [](const std::vector<const std::vector<double>*>& v, int i) {
+    return i < static_cast<int>(v.size()) ? v[i] : nullptr;
+  };
+  std::vector<const std::vector<double>*> first_x(K), first_y(K);
+  for (int k = 0; k < K; ++k) {
+    first_x[k] = warm_of(warm_x, k);
+    first_y[k] = warm_of(warm_y, k);
+  }
   for (int i = K; i < total; ++i) {
     queue.pending.push_back(cases[i]);
     queue.pending_index.push_back(i);
+    queue.pending_warm_x.push_back(warm_of(warm_x, i));
+    queue.pending_warm_y.push_back(warm_of(warm_y, i));
   }
   std::vector<CaseResult> slot_results;
-  std::vector<const std::vector<double>*> none(K, nullptr);
   if (problem.precision == ANU_PRECISION_FP32)
-    run_cases_t<float>(problem, first, options, none, none, &slot_results, start_time,
+    run_cases_t<float>(problem, first, options, first_x, first_y, &slot_results, start_time,
                        problem.unit_scaling, nullptr, nullptr, &queue);
   else
-    run_cases_t<double>(problem, first, options, none, none, &slot_results, start_time,
+    run_cases_t<double>(problem, first, options, first_x, first_y, &slot_results, start_time,
                         problem.unit_scaling, nullptr, nullptr, &queue);
   // Cases the time limit (or a stop request) kept from ever starting.
   for (size_t i = queue.next; i < queue.pending.size(); ++i) {
@@ -2284,6 +2310,11 @@ int anu_pdhg_batch_create(const anu_lp* base, int32_t num_cases, const double* c
 }
 
 int anu_pdhg_batch_solve(anu_pdhg_batch* h, double* x, double* y, anu_pdhg_result* results) {
+  return anu_pdhg_batch_solve_warm(h, nullptr, nullptr, x, y, results);
+}
+
+int anu_pdhg_batch_solve_warm(anu_pdhg_batch* h, const double* warm_x, const double* warm_y,
+                              double* x, double* y, anu_pdhg_result* results) {
   return guarded([&] {
     if (h == nullptr || results == nullptr) throw Error(ANU_ERR_INVALID, "null argument");
     const int32_t n = h->problem->n, m = h->problem->m;
@@ -2291,16 +2322,26 @@ int anu_pdhg_batch_solve(anu_pdhg_batch* h, double* x, double* y, anu_pdhg_resul
     const double start = anu::now_seconds();
     // One stack of the given cases on one problem: lockstep up to one run's
     // capacity, rolling beyond it.
+    // Warm starts, case-major, both or neither.
+    const bool warm = warm_x != nullptr && warm_y != nullptr;
+    std::vector<std::vector<double>> wx(warm ? total : 0), wy(warm ? total : 0);
+    for (int k = 0; warm && k < total; ++k) {
+      wx[k].assign(warm_x + static_cast<size_t>(k) * n, warm_x + static_cast<size_t>(k + 1) * n);
+      wy[k].assign(warm_y + static_cast<size_t>(k) * m, warm_y + static_cast<size_t>(k + 1) * m);
+    }
     auto solve_part = [&](anu::Problem& prob, const std::vector<int>& idx,
                           std::vector<anu::CaseResult>* out) {
       std::vector<const anu::CaseData*> cs;
-      for (int k : idx) cs.push_back(&h->cases[k]);
-      if (static_cast<int>(cs.size()) <= anu::kMaxCasesPerRun) {
-        std::vector<const std::vector<double>*> none(cs.size(), nullptr);
-        anu::run_cases(prob, cs, h->options, none, none, out, start);
-      } else {
-        anu::run_cases_rolling(prob, cs, anu::kMaxCasesPerRun, h->options, out, start);
+      std::vector<const std::vector<double>*> vx, vy;
+      for (int k : idx) {
+        cs.push_back(&h->cases[k]);
+        vx.push_back(warm ? &wx[k] : nullptr);
+        vy.push_back(warm ? &wy[k] : nullptr);
       }
+      if (static_cast<int>(cs.size()) <= anu::kMaxCasesPerRun)
+        anu::run_cases(prob, cs, h->options, vx, vy, out, start);
+      else
+        anu::run_cases_rolling(prob, cs, anu::kMaxCasesPerRun, h->options, vx, vy, out, start);
     };
     std::vector<anu::CaseResult> res(total);
     if (h->twin == nullptr) {

@@ -212,8 +212,10 @@ void run_cases(Problem& problem, const std::vector<const CaseData*>& cases,
 // results[i] is case i's result. Each case runs the iteration it would run
 // in a stack of its own (its iteration count starts at its admission).
 void run_cases_rolling(Problem& problem, const std::vector<const CaseData*>& cases, int slots,
-                       const anu_pdhg_options& options, std::vector<CaseResult>* results,
-                       double start_time);
+                       const anu_pdhg_options& options,
+                       const std::vector<const std::vector<double>*>& warm_x,
+                       const std::vector<const std::vector<double>*>& warm_y,
+                       std::vector<CaseResult>* results, double start_time);
 
 // ||K~|| by power iteration on the device, FP64 (pdhg.cpp:223-282).
 double device_matrix_norm(Problem& p, int iterations, double tolerance);

@@ -36,7 +36,8 @@ EXPORTS = (
     "anu_backend_accumulate", "anu_backend_scale_into", "anu_backend_weighted_norm_squared",
     "anu_backend_step_size_terms", "anu_backend_convergence_terms",
     "anu_backend_convergence_terms_noalloc",
-    "anu_pdhg_batch_create", "anu_pdhg_batch_solve", "anu_pdhg_batch_destroy",
+    "anu_pdhg_batch_create", "anu_pdhg_batch_solve", "anu_pdhg_batch_solve_warm",
+    "anu_pdhg_batch_destroy",
     "anu_pdhg_packed_create", "anu_pdhg_packed_solve", "anu_pdhg_packed_workers",
     "anu_pdhg_packed_destroy",
     "anu_pdhg_unrolled_create", "anu_pdhg_unrolled_step_sizes", "anu_pdhg_forward_unrolled",
@@ -85,6 +86,9 @@ def lib():
                                          _P(anu_pdhg_options), _P(C.c_void_p)])
     d("anu_pdhg_batch_solve", C.c_int, [C.c_void_p, _P(C.c_double), _P(C.c_double),
                                         _P(anu_pdhg_result)])
+    d("anu_pdhg_batch_solve_warm", C.c_int, [C.c_void_p, _P(C.c_double), _P(C.c_double),
+                                             _P(C.c_double), _P(C.c_double),
+                                             _P(anu_pdhg_result)])
     d("anu_pdhg_batch_destroy", None, [C.c_void_p])
     d("anu_pdhg_packed_create", C.c_int, [C.c_int32, _P(anu_lp), _P(anu_pdhg_options),
                                           C.c_int32, _P(C.c_void_p)])
@@ -242,13 +246,20 @@ class CaseStackSolver:
                                           *[f64_ptr(a) for a in self._keep],
                                           C.byref(self.options), C.byref(self._h)))
 
-    def solve(self):
-        """Returns a list of PdhgResult, one per case."""
+    def solve(self, warm_x=None, warm_y=None):
+        """Returns a list of PdhgResult, one per case. warm_x (K x n) and
+        warm_y (K x m) warm start every case, as solve_pdhg's warm start."""
         K, n, m = self.num_cases, self._cl.n, self._cl.m
         x = np.zeros((K, n))
         y = np.zeros((K, m))
         res = (anu_pdhg_result * K)()
-        check(lib().anu_pdhg_batch_solve(self._h, f64_ptr(x), f64_ptr(y), res))
+        if warm_x is None or warm_y is None:
+            check(lib().anu_pdhg_batch_solve(self._h, f64_ptr(x), f64_ptr(y), res))
+        else:
+            wx = np.ascontiguousarray(warm_x, np.float64).reshape(K, n)
+            wy = np.ascontiguousarray(warm_y, np.float64).reshape(K, m)
+            check(lib().anu_pdhg_batch_solve_warm(self._h, f64_ptr(wx), f64_ptr(wy), f64_ptr(x),
+                                                  f64_ptr(y), res))
         return [PdhgResult.from_c(res[k], x[k], y[k]) for k in range(K)]
 
     def close(self):

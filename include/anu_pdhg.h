@@ -366,6 +366,12 @@ int anu_pdhg_batch_create(const anu_lp* base, int32_t num_cases,
  * num_cases entries. */
 int anu_pdhg_batch_solve(anu_pdhg_batch* handle, double* x, double* y,
                          anu_pdhg_result* results);
+/* The same, each case warm started as solve_pdhg takes a warm start
+ * (PdhgOptions::warm_x / warm_y, src/anukulan/pdhg.cpp:478-502): warm_x is
+ * num_cases*n, warm_y num_cases*m, case-major; both or neither. */
+int anu_pdhg_batch_solve_warm(anu_pdhg_batch* handle, const double* warm_x,
+                              const double* warm_y, double* x, double* y,
+                              anu_pdhg_result* results);
 void anu_pdhg_batch_destroy(anu_pdhg_batch* handle);
 
 /* ------------------------------------------------------ packed batches

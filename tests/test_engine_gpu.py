@@ -265,6 +265,26 @@ def test_rolling_stack_fp32_admitted_cases_converge(engine, stack):
         assert r.converged(1e-6), (k, r)
 
 
+@pytest.mark.parametrize("count", [6, 20])
+def test_case_stack_warm_start_matches_single(engine, stack, count):
+    # Warm starts go to every case as solve_pdhg takes them; 20 cases also
+    # exercise the two half-stacks.
+    sub = _rolling(stack, list(range(count)))
+    cold = engine.solve_case_stack(sub, tolerance=1e-6)
+    wx = np.stack([r.x for r in cold])
+    wy = np.stack([r.y for r in cold])
+    solver = engine.CaseStackSolver(sub.base, sub.c, sub.q, sub.lower, sub.upper, tolerance=1e-6)
+    try:
+        warm = solver.solve(wx, wy)
+    finally:
+        solver.close()
+    for k in (0, count // 2, count - 1):
+        single = engine.solve_pdhg(sub.case(k), warm_x=wx[k], warm_y=wy[k], tolerance=1e-6)
+        assert warm[k].status == single.status == OPTIMAL, k
+        assert abs(warm[k].iterations - single.iterations) <= 40, k
+        assert abs(warm[k].objective - single.objective) <= 1e-8 * abs(single.objective), k
+
+
 def test_case_stack_equals_single_solves(engine, stack):
     sub = lpgen.CaseStack(stack.base, stack.names[:5], stack.c[:5], stack.q[:5],
                           stack.lower[:5], stack.upper[:5])
