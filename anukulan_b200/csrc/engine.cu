@@ -2169,6 +2169,7 @@ void anu_pdhg_default_options(anu_pdhg_options* o) {
   o->device = 0;
   o->use_graphs = 1;
   o->profile = 0;
+  o->split_stacks = 1;
 }
 
 int anu_last_error(char* buf, int32_t size) { return anu::copy_last_error(buf, size); }
@@ -2295,7 +2296,8 @@ int anu_pdhg_batch_create(const anu_lp* base, int32_t num_cases, const double* c
     auto h = std::make_unique<anu_pdhg_batch>();
     h->options = *options;
     h->problem = anu::make_problem(*base, *options, &h->scaling_seconds, &h->norm_seconds);
-    if (num_cases >= anu::kSplitStack) h->twin = anu::clone_problem(*h->problem);
+    if (options->split_stacks && num_cases >= anu::kSplitStack)
+      h->twin = anu::clone_problem(*h->problem);
     h->cases.reserve(num_cases);
     for (int32_t k = 0; k < num_cases; ++k) {
       h->cases.push_back(anu::make_case(

@@ -406,7 +406,8 @@ def run_engine(args, rank, world, local_rank):
         dist.init_process_group("nccl", timeout=timedelta(seconds=600),
                                 device_id=torch.device("cuda", local_rank))
     st, cfg = stack_workload()
-    opts = make_options(tolerance=TOL, precision=PRECISION_FP32, device=local_rank, profile=1)
+    opts = make_options(tolerance=TOL, precision=PRECISION_FP32, device=local_rank, profile=1,
+                        split_stacks=0 if args.no_split else 1)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
 
     def barrier():
@@ -487,7 +488,8 @@ def run_engine(args, rank, world, local_rank):
         # The engine runs a stack of 16 or more cases as two half-stacks at
         # once (two streams): a launch carries half the cases, and two are in
         # flight at a time.
-        per_launch_cases = (st.num_cases + 1) // 2 if st.num_cases >= 16 else st.num_cases
+        split = st.num_cases >= 16 and not args.no_split
+        per_launch_cases = (st.num_cases + 1) // 2 if split else st.num_cases
         bytes_it = algorithmic_bytes_per_iteration(nnz, m, n, per_launch_cases, 4, 4)
         per_launch_s = dev_iter_s / max(dev_iters, 1) / 2.0
         achieved = (bytes_it / 2.0) / per_launch_s / 1e9 if dev_iters else None
@@ -644,6 +646,8 @@ def main(argv=None):
                     help="reference arm: skip the reference's own CUDA backend leg")
     ap.add_argument("--no-e2e", dest="e2e", action="store_false",
                     help="skip the end-to-end pass (profiling runs)")
+    ap.add_argument("--no-split", action="store_true",
+                    help="run the stack as one stack on one stream (profiling)")
     ap.add_argument("--workload", default="stack",
                     choices=["stack", "spmv", "packed", "adjoint", "powerlaw"])
     ap.add_argument("--tolerance", type=float, default=1e-6,

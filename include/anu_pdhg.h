@@ -159,6 +159,9 @@ typedef struct anu_pdhg_options {
    * and report their total in anu_pdhg_result::device_iteration_seconds.
    * Events do not serialise the stream. 0 = off. */
   int32_t profile;
+  /* Case stacks of 16 or more cases run as two half-stacks at once, each on
+   * its own stream and host thread. 0 = one stack on one stream. 1 */
+  int32_t split_stacks;
 } anu_pdhg_options;
 
 /* PdhgResidual, src/anukulan/pdhg.hpp:429-496. */
