@@ -141,6 +141,71 @@ PoolScope::~PoolScope() {
   t_pool = previous_;
 }
 
+// Idle blocks of destroyed pools, by (device, size class); pinned host
+// blocks under device -1. Created on first use and never destroyed: at
+// process exit the CUDA runtime may already be gone, and the driver
+// reclaims the memory.
+class BlockCache {
+ public:
+  void* take(int device, size_t cls) {
+    std::lock_guard<std::mutex> g(lock_);
+    auto it = free_.find({device, cls});
+    if (it == free_.end()) return nullptr;
+    void* p = it->second;
+    free_.erase(it);
+    bytes_[device < 0] -= cls;
+    return p;
+  }
+  bool keep(int device, void* p, size_t cls) {
+    std::lock_guard<std::mutex> g(lock_);
+    if (bytes_[device < 0] + cls > kGlobalCap[device < 0]) return false;
+    free_.emplace(std::make_pair(device, cls), p);
+    bytes_[device < 0] += cls;
+    return true;
+  }
+  size_t release() {
+    std::multimap<std::pair<int, size_t>, void*> blocks;
+    {
+      std::lock_guard<std::mutex> g(lock_);
+      blocks.swap(free_);
+      bytes_[0] = bytes_[1] = 0;
+    }
+    int current = 0;
+    cudaGetDevice(&current);
+    size_t freed = 0;
+    for (auto& b : blocks) {
+      if (b.first.first < 0) {
+        cudaFreeHost(b.second);
+      } else {
+        cudaSetDevice(b.first.first);
+        cudaFree(b.second);
+      }
+      freed += b.first.second;
+    }
+    cudaSetDevice(current);
+    return freed;
+  }
+
+ private:
+  // Most bytes kept: device blocks (all devices together), pinned blocks.
+  static constexpr size_t kGlobalCap[2] = {size_t(16) << 30, size_t(1) << 30};
+  std::mutex lock_;
+  std::multimap<std::pair<int, size_t>, void*> free_;
+  size_t bytes_[2] = {0, 0};
+};
+
+BlockCache& block_cache() {
+  static BlockCache* cache = new BlockCache();
+  return *cache;
+}
+
+size_t release_cached_blocks() { return block_cache().release(); }
+
+std::mutex& cooperative_mutex(int device) {
+  static std::mutex locks[64];
+  return locks[static_cast<unsigned>(device) % 64u];
+}
+
 void* MemoryPool::get(bool pinned, size_t bytes, size_t* rounded) {
   const size_t c = size_class(bytes);
   *rounded = c;
@@ -154,8 +219,24 @@ void* MemoryPool::get(bool pinned, size_t bytes, size_t* rounded) {
       return p;
     }
   }
+  int device = -1;
+  if (!pinned) {
+    ANU_CUDA(cudaGetDevice(&device));
+    std::lock_guard<std::mutex> g(lock_);
+    if (device_ < 0) device_ = device;
+    if (device_ != device)
+      throw Error(ANU_ERR_INTERNAL, "memory pool used on two devices");
+  }
+  if (void* p = block_cache().take(device, c)) return p;
   void* p = nullptr;
-  const cudaError_t e = pinned ? cudaMallocHost(&p, c) : cudaMalloc(&p, c);
+  cudaError_t e = pinned ? cudaMallocHost(&p, c) : cudaMalloc(&p, c);
+  if (e == cudaErrorMemoryAllocation) {
+    // Cached blocks of other sizes may be what fills the device: free them
+    // and try once more.
+    cudaGetLastError();
+    block_cache().release();
+    e = pinned ? cudaMallocHost(&p, c) : cudaMalloc(&p, c);
+  }
   if (e != cudaSuccess) {
     cudaGetLastError();
     throw Error(ANU_ERR_MEMORY, std::string(pinned ? "cudaMallocHost: " : "cudaMalloc: ") +
@@ -173,13 +254,30 @@ void MemoryPool::put(bool pinned, void* p, size_t rounded) {
       return;
     }
   }
+  // Over this pool's cap: freed at once (this pool's stream may still use
+  // the block, and cudaFree waits for the device; the shared cache does not).
   if (pinned) cudaFreeHost(p);
   else cudaFree(p);
 }
 
 MemoryPool::~MemoryPool() {
-  for (auto& b : free_[0]) cudaFree(b.second);
-  for (auto& b : free_[1]) cudaFreeHost(b.second);
+  if (free_[0].empty() && free_[1].empty()) return;
+  // All work that could read these blocks ends before any other pool may
+  // receive them.
+  int current = 0;
+  cudaGetDevice(&current);
+  if (device_ >= 0) {
+    cudaSetDevice(device_);
+    cudaDeviceSynchronize();
+  } else {
+    cudaDeviceSynchronize();
+  }
+  BlockCache& cache = block_cache();
+  for (auto& b : free_[0])
+    if (!cache.keep(device_, b.second, b.first)) cudaFree(b.second);
+  for (auto& b : free_[1])
+    if (!cache.keep(-1, b.second, b.first)) cudaFreeHost(b.second);
+  cudaSetDevice(current);
 }
 
 // ------------------------------------------------------------- launches
@@ -322,6 +420,9 @@ std::unique_ptr<Problem> make_problem(const anu_lp& lp, const anu_pdhg_options& 
   p->device = o.device;
   ANU_CUDA(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
   p->owns_stream = true;
+  // The matrices and the norm estimate's vectors come from the problem's
+  // pool too, so they return to the shared cache with it.
+  PoolScope scope(&p->pool, p->stream);
   p->m = lp.k.rows;
   p->n = lp.k.cols;
   p->num_eq = lp.num_equalities;
@@ -350,12 +451,21 @@ std::unique_ptr<Problem> make_problem(const anu_lp& lp, const anu_pdhg_options& 
   return p;
 }
 
+bool stack_runs_persistent(const Problem& p, int K, const anu_pdhg_options& o) {
+  const bool slow = (o.adaptive_step_size && !o.constant_step_size) || o.halpern_restart;
+  if (!o.persistent_chunks || !o.use_graphs || slow) return false;
+  ANU_CUDA(cudaSetDevice(p.device));
+  return p.precision == ANU_PRECISION_FP32 ? chunk_fits<float>(p.dkt, p.dk, K)
+                                           : chunk_fits<double>(p.dkt, p.dk, K);
+}
+
 std::unique_ptr<Problem> clone_problem(const Problem& src) {
   ANU_CUDA(cudaSetDevice(src.device));
   auto p = std::make_unique<Problem>();
   p->device = src.device;
   ANU_CUDA(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
   p->owns_stream = true;
+  PoolScope scope(&p->pool, p->stream);
   p->m = src.m;
   p->n = src.n;
   p->num_eq = src.num_eq;
@@ -1131,8 +1241,48 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
     product<T, T, T>(p, p.dk, w.x_bar.p, K, de, true);
   };
 
+  // Persistent chunks: one cooperative launch per chunk (chunk_kernel). At
+  // most one runs per device at a time from this process: the lock is taken
+  // before a launch and let go once the stream has been synchronised after
+  // it, so two stacks never hold part of the device each while waiting for
+  // the rest.
+  const bool persistent = o.persistent_chunks != 0 && !slow && o.use_graphs &&
+                          chunk_fits<T>(p.dkt, p.dk, K);
+  DevBuf<uint32_t> sync_arrived;
+  DevBuf<int32_t> sync_status;
+  Pinned<int32_t> h_sync_status(persistent ? 1 : 0);
+  std::unique_lock<std::mutex> coop_lock(cooperative_mutex(p.device), std::defer_lock);
+  if (persistent) {
+    sync_arrived.alloc(1);
+    sync_status.alloc(1);
+    ANU_CUDA(cudaMemsetAsync(sync_status.p, 0, sizeof(int32_t), st));
+    h_sync_status.p[0] = 0;
+  }
+  // After a synchronisation of the stream: the chunks before it are done.
+  auto chunks_done = [&]() {
+    if (!persistent) return;
+    if (coop_lock.owns_lock()) coop_lock.unlock();
+    if (h_sync_status.p[0] != 0)
+      throw Error(ANU_ERR_INTERNAL,
+                  "chunk_kernel: a grid barrier wait gave up (the grid was not co-resident)");
+  };
+
   auto run_chunk_body = [&](int len, bool check_at_end) {
     const uint32_t base_flags = averaging ? kAccumulate : 0u;
+    if (persistent) {
+      if (!coop_lock.owns_lock()) coop_lock.lock();
+      PrimalEpi<T> pe{K, 0, 0u, w.params.p, w.w_table.p, w.x.p, w.x.p, w.c.p, w.lo.p, w.hi.p,
+                      w.x_bar.p, w.anchor_x.p, w.dx.p, w.sum_x.p};
+      DualEpi<T> de{K, 0, 0u, p.num_eq, w.params.p, w.w_table.p, w.y.p, w.y.p, w.q.p, w.kx.p,
+                    w.kx.p, w.anchor_y.p, w.anchor_kx.p, w.dy.p, nullptr, w.sum_y.p, ylo_ptr};
+      ANU_CUDA(cudaMemsetAsync(sync_arrived.p, 0, sizeof(uint32_t), st));
+      launch_chunk<T>(p, p.dkt, p.dk, w.y.p, w.x_bar.p, K, len, base_flags,
+                      base_flags | (check_at_end ? kWriteDelta : 0u), pe, de,
+                      GridSync{sync_arrived.p, reinterpret_cast<int*>(sync_status.p)});
+      ANU_CUDA(cudaMemcpyAsync(h_sync_status.p, sync_status.p, sizeof(int32_t),
+                               cudaMemcpyDeviceToHost, st));
+      return;
+    }
     if (o.use_graphs) {
       const auto key = std::make_pair(len, check_at_end ? 1 : 0);
       auto found = w.graphs.find(key);
@@ -1676,6 +1826,7 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
     iteration = last + 1;
     if (!is_check) continue;
     ANU_CUDA(cudaStreamSynchronize(st));
+    chunks_done();
     t_iter += phase_end();
 
     // ------------------------------------------------------------- check
@@ -1973,6 +2124,10 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
     }
     t_checks += phase_end();
   }
+  if (persistent) {
+    ANU_CUDA(cudaStreamSynchronize(st));
+    chunks_done();
+  }
   for (int k = 0; k < K; ++k)
     if (S[k].active) {
       S[k].final_iteration = iteration - origin[k];
@@ -2170,9 +2325,14 @@ void anu_pdhg_default_options(anu_pdhg_options* o) {
   o->use_graphs = 1;
   o->profile = 0;
   o->split_stacks = 1;
+  o->persistent_chunks = 0;
 }
 
 int anu_last_error(char* buf, int32_t size) { return anu::copy_last_error(buf, size); }
+
+int64_t anu_release_cached_memory(void) {
+  return static_cast<int64_t>(anu::release_cached_blocks());
+}
 
 int32_t anu_device_count(void) {
   int count = 0;
@@ -2296,7 +2456,11 @@ int anu_pdhg_batch_create(const anu_lp* base, int32_t num_cases, const double* c
     auto h = std::make_unique<anu_pdhg_batch>();
     h->options = *options;
     h->problem = anu::make_problem(*base, *options, &h->scaling_seconds, &h->norm_seconds);
-    if (options->split_stacks && num_cases >= anu::kSplitStack)
+    // A stack that runs persistent chunks is one stack: its chunk kernel
+    // fills the device on its own, and two of them may not overlap.
+    if (options->split_stacks && num_cases >= anu::kSplitStack &&
+        !anu::stack_runs_persistent(*h->problem, std::min(num_cases, anu::kMaxCasesPerRun),
+                                    *options))
       h->twin = anu::clone_problem(*h->problem);
     h->cases.reserve(num_cases);
     for (int32_t k = 0; k < num_cases; ++k) {

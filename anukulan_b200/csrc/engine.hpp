@@ -39,6 +39,14 @@ void clear_last_error();
 // is ordered by that stream; the scope synchronises the stream when it
 // ends, so no copy from a pinned block is still pending when the host
 // writes into it again.
+//
+// A pool that is destroyed hands its idle blocks to a process-wide cache
+// (per device for device blocks) instead of freeing them, and a pool that
+// misses takes from that cache before it allocates: a create-solve-destroy
+// cycle of handles of like size then allocates and frees nothing after the
+// first. The destroying handle has synchronised its stream, and the pool
+// synchronises its device before the hand-over, so no work of the old
+// handle can still touch a block the next handle receives.
 class MemoryPool {
  public:
   MemoryPool() = default;
@@ -53,7 +61,15 @@ class MemoryPool {
   std::mutex lock_;
   std::multimap<size_t, void*> free_[2];
   size_t cached_[2] = {0, 0};
+  int device_ = -1;  // device of the device blocks, set by the first one
 };
+
+// Frees every block in the process-wide cache; returns the bytes freed.
+size_t release_cached_blocks();
+
+// Held by a stack while a cooperative chunk kernel of it may run on
+// `device`, so this process never has two of them in flight on one device.
+std::mutex& cooperative_mutex(int device);
 
 // The pool of the innermost PoolScope on this thread, or null.
 MemoryPool* current_pool();
@@ -193,8 +209,12 @@ std::unique_ptr<Problem> make_problem(const anu_lp& lp, const anu_pdhg_options& 
 // power iteration again.
 std::unique_ptr<Problem> clone_problem(const Problem& src);
 
-// Case stacks of at least this many cases run as two half-stacks at once.
+// Case stacks of at least this many cases run as two half-stacks at once,
+// unless they run persistent chunks.
 constexpr int kSplitStack = 16;
+
+// Whether run_cases takes a stack of K cases on `p` through chunk_kernel.
+bool stack_runs_persistent(const Problem& p, int K, const anu_pdhg_options& o);
 
 CaseData make_case(const Problem& p, const double* c, const double* q, const double* lower,
                    const double* upper, double objective_scale, double objective_offset);

@@ -530,6 +530,234 @@ __global__ void __launch_bounds__(kThreads) seg_kernel(CsrView<V> a, const X* __
   }
 }
 
+// ------------------------------------------------------------ chunk_kernel
+
+// A chunk of iterations of a case stack in ONE cooperative launch. The two
+// products of an iteration (K'y with the primal step, K x_bar with the dual
+// step) are separated by grid barriers instead of launch boundaries, which
+// removes the per-launch latency that bounds seg_kernel on stacks whose
+// matrix fits in one wave of CTAs. Each CTA owns the same slice of both
+// segment schedules for the whole chunk: its lanes load their segment's
+// index and value once into registers and keep them, so an iteration's
+// critical path is barrier -> gather -> segment sums -> epilogue. The
+// epilogue inputs of a phase are this thread's own elements (written by the
+// same thread in the previous iteration), so they are prefetched before the
+// barrier that precedes the phase. Vectors written by other CTAs during the
+// chunk (y for the K'y gather, x_bar for the K x_bar gather) are read with
+// plain loads ordered after the barrier's acquire, never through the
+// read-only path, which could return a line cached before the barrier.
+//
+// Every CTA must be resident at once: the launch is cooperative and the
+// host sizes the grid to fit one wave. Each barrier wait gives up after a
+// bounded number of polls, records kSyncTimedOut and returns, and a CTA
+// that sees another's failure returns too, so a grid that cannot meet ends
+// with an error status instead of spinning.
+struct GridSync {
+  unsigned int* arrived;  // arrivals so far; zeroed before each launch
+  int* status;            // 0, or kSyncTimedOut once a wait gave up
+};
+constexpr int kSyncTimedOut = 1;
+constexpr unsigned kBarrierFastPolls = 4096;
+constexpr unsigned kBarrierPollLimit = 1u << 24;  // ~1 s of 64 ns sleeps
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Waits until `target` arrivals (this CTA's included) have been counted.
+// False when the wait gave up; the caller returns.
+__device__ __forceinline__ bool grid_barrier(const GridSync& g, unsigned target, int* ok_flag) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    // Release: the CTA's writes (ordered before this thread by the
+    // __syncthreads above) before its arrival.
+    asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(g.arrived) : "memory");
+    unsigned polls = 0;
+    while (ld_acquire_u32(g.arrived) < target) {
+      ++polls;
+      if (polls > kBarrierFastPolls) {
+        if ((polls & 255u) == 0 && *reinterpret_cast<volatile int*>(g.status) != 0) {
+          ok = 0;
+          break;
+        }
+        if (polls > kBarrierPollLimit) {
+          atomicExch(g.status, kSyncTimedOut);
+          ok = 0;
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    // The acquire load that saw the last arrival orders the other CTAs'
+    // writes before this CTA's reads (after the __syncthreads below).
+    *ok_flag = ok;
+  }
+  __syncthreads();
+  return *ok_flag != 0;
+}
+
+// A plain (weak, L1-cacheable) global load. The compiler may not turn it
+// into a read-only-path load, whose cache is not kept coherent with writes
+// made during the kernel; a weak load after the barrier's acquire sees every
+// write from before the other CTAs' arrivals.
+__device__ __forceinline__ float ld_weak(const float* p) {
+  float v;
+  asm volatile("ld.global.f32 %0, [%1];" : "=f"(v) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ double ld_weak(const double* p) {
+  double v;
+  asm volatile("ld.global.f64 %0, [%1];" : "=d"(v) : "l"(p));
+  return v;
+}
+
+// One CTA's slice of a segment schedule, held for the whole chunk. Lane
+// groups are whole warps (32 lanes); each lane keeps one of the segment's
+// first 32 nonzeros. Segments are longer only in rows of more than
+// kSegNnz * kSegPerCta nonzeros; their remaining nonzeros are loaded again
+// in each phase.
+template <class V>
+struct SegSlice {
+  int32_t r0 = 0, r1 = 0, s0 = 0, s1 = 0, seg = 0, b = 0, len = 0, idx = 0;
+  V val = 0;
+  bool active = false;
+  __device__ __forceinline__ void load(const CsrView<V>& a, int32_t cta) {
+    if (cta >= a.num_ctas) return;
+    r0 = a.cta_row[cta];
+    r1 = a.cta_row[cta + 1];
+    s0 = a.cta_seg[cta];
+    s1 = a.cta_seg[cta + 1];
+    seg = s0 + static_cast<int32_t>(threadIdx.x / 32);
+    active = seg < s1;
+    if (!active) return;
+    b = a.seg_begin[seg];
+    len = a.seg_begin[seg + 1] - b;
+    const int lane = threadIdx.x % 32;
+    if (lane < len) {
+      idx = a.index[b + lane];
+      val = a.value[b + lane];
+    }
+  }
+};
+
+constexpr int kChunkPrefetch = 2;  // epilogue items prefetched per thread
+// Resident CTAs per SM the chunk kernel is compiled for: 4 x 148 = 592
+// slices, enough for schedules of up to ~75,000 nonzeros in either product.
+constexpr int kChunkCtasPerSm = 4;
+
+template <class V, class Epi>
+__device__ __forceinline__ void chunk_prefetch(const SegSlice<V>& s, int32_t K, const Epi& epi,
+                                               typename Epi::Pre* pre) {
+  const int32_t items = (s.r1 - s.r0) * K;
+#pragma unroll
+  for (int q = 0; q < kChunkPrefetch; ++q) {
+    const int32_t t = threadIdx.x + q * kThreads;
+    if (t < items) pre[q] = epi.prefetch(s.r0 + t / K, t % K);
+  }
+}
+
+template <class V, int CPL, class Epi>
+__device__ __forceinline__ void chunk_phase(const CsrView<V>& a, const SegSlice<V>& s,
+                                            const V* x, int32_t K, const Epi& epi,
+                                            const typename Epi::Pre* pre,
+                                            V (*part)[kMaxCaseLanes]) {
+  const int lane = threadIdx.x % 32;
+  V acc[CPL];
+#pragma unroll
+  for (int c = 0; c < CPL; ++c) acc[c] = 0;
+  // s.len is uniform over the warp. Unrolled so the x loads of successive
+  // nonzeros are in flight together.
+  for (int32_t base = 0; base < s.len; base += 32) {
+    int32_t idx = s.idx;
+    V val = s.val;
+    if (base > 0) {
+      idx = 0;
+      val = 0;
+      if (base + lane < s.len) {
+        idx = a.index[s.b + base + lane];
+        val = a.value[s.b + base + lane];
+      }
+    }
+    const int32_t cnt = min(32, s.len - base);
+#pragma unroll 8
+    for (int32_t t = 0; t < cnt; ++t) {
+      const int32_t col = __shfl_sync(0xffffffffu, idx, t);
+      const V v = __shfl_sync(0xffffffffu, val, t);
+      const V* xc = x + (size_t)col * K;
+#pragma unroll
+      for (int c = 0; c < CPL; ++c) {
+        const int32_t cs = lane + c * 32;
+        if (cs < K) acc[c] = madd(acc[c], v, ld_weak(xc + cs));
+      }
+    }
+  }
+  if (s.active) {
+#pragma unroll
+    for (int c = 0; c < CPL; ++c)
+      if (lane + c * 32 < kMaxCaseLanes) part[s.seg - s.s0][lane + c * 32] = acc[c];
+  }
+  __syncthreads();
+  const int32_t items = (s.r1 - s.r0) * K;
+  for (int32_t t = threadIdx.x, q = 0; t < items; t += kThreads, ++q) {
+    const int32_t row = s.r0 + t / K;
+    const int32_t k = t % K;
+    V sum = 0;
+    for (int32_t g = a.row_seg[row]; g < a.row_seg[row + 1]; ++g) sum = add(sum, part[g - s.s0][k]);
+    if (q < kChunkPrefetch) {
+      typename Epi::Pre r;
+#pragma unroll
+      for (int qq = 0; qq < kChunkPrefetch; ++qq)
+        if (qq == q) r = pre[qq];
+      epi.finish(row, k, sum, r);
+    } else {
+      epi.finish(row, k, sum, epi.prefetch(row, k));
+    }
+  }
+}
+
+// `len` iterations over cases 0..K-1 (17 <= K <= 32*CPL) of a stack with
+// vectors case-interleaved; y and x_bar are the gather sources of the two
+// products (the dual iterate and the primal extrapolation). The last
+// iteration runs with `last_flags`, the others with `flags`.
+template <class T, int CPL>
+__global__ void __launch_bounds__(kThreads, kChunkCtasPerSm)
+    chunk_kernel(CsrView<T> kt, CsrView<T> k, const T* y, const T* x_bar, int32_t K, int32_t len,
+                 uint32_t flags, uint32_t last_flags, PrimalEpi<T> pe, DualEpi<T> de,
+                 GridSync sync) {
+  static_assert(kSegNnz <= 32 && kThreads / 32 >= kSegPerCta, "one warp per segment");
+  __shared__ T part[kSegPerCta][kMaxCaseLanes];
+  __shared__ int ok_flag;
+  SegSlice<T> sa, sb;
+  sa.load(kt, blockIdx.x);
+  sb.load(k, blockIdx.x);
+  const unsigned G = gridDim.x;
+  unsigned target = 0;
+  for (int32_t it = 0; it < len; ++it) {
+    const uint32_t f = it == len - 1 ? last_flags : flags;
+    PrimalEpi<T> ep = pe;
+    ep.it = it;
+    ep.flags = f;
+    typename PrimalEpi<T>::Pre pre_a[kChunkPrefetch];
+    chunk_prefetch(sa, K, ep, pre_a);
+    if (it > 0) {  // the previous dual step wrote y
+      target += G;
+      if (!grid_barrier(sync, target, &ok_flag)) return;
+    }
+    chunk_phase<T, CPL>(kt, sa, y, K, ep, pre_a, part);
+    DualEpi<T> ed = de;
+    ed.it = it;
+    ed.flags = f;
+    typename DualEpi<T>::Pre pre_b[kChunkPrefetch];
+    chunk_prefetch(sb, K, ed, pre_b);
+    target += G;  // the primal step wrote x_bar
+    if (!grid_barrier(sync, target, &ok_flag)) return;
+    chunk_phase<T, CPL>(k, sb, x_bar, K, ed, pre_b, part);
+  }
+}
+
 // ------------------------------------------------------- term reductions
 
 // Stage 1 of a per-case reduction over `len` rows (or columns): groups of L

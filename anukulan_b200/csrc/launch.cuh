@@ -72,6 +72,59 @@ void product(Exec& p, const Mat& a, const X* x, int K, const Epi& epi, bool pdl 
   ++p.launches;
 }
 
+// Most CTAs of chunk_kernel<T, CPL> resident at once on the current device.
+template <class T, int CPL>
+int chunk_capacity() {
+  int dev = 0, sms = 0, per_sm = 0;
+  cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+  cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev),
+             "cudaDeviceGetAttribute");
+  cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, chunk_kernel<T, CPL>,
+                                                           kThreads, 0),
+             "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+  return sms * per_sm;
+}
+
+// Whether a stack of K cases over (kt, k) can run as chunk_kernel: 17 to
+// 64 cases, and one CTA per schedule slice of the larger product, all of
+// them resident at once.
+template <class T, class Mat>
+bool chunk_fits(const Mat& kt, const Mat& k, int K) {
+  if (K < 17 || K > 2 * 32) return false;
+  if (kt.rows == 0 || k.rows == 0) return false;
+  const int grid = kt.num_ctas > k.num_ctas ? kt.num_ctas : k.num_ctas;
+  const int cap = K <= 32 ? chunk_capacity<T, 1>() : chunk_capacity<T, 2>();
+  return grid >= 1 && grid <= cap;
+}
+
+// `len` iterations of the stack in one cooperative launch; sync.arrived
+// must be zero on the stream when the kernel starts.
+template <class T, class Mat>
+void launch_chunk(Exec& p, const Mat& kt, const Mat& k, const T* y, const T* x_bar, int K,
+                  int len, uint32_t flags, uint32_t last_flags, const PrimalEpi<T>& pe,
+                  const DualEpi<T>& de, GridSync sync) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(kt.num_ctas > k.num_ctas ? kt.num_ctas : k.num_ctas);
+  cfg.blockDim = dim3(kThreads);
+  cfg.stream = p.stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  const CsrView<T> vt = kt.template view<T>();
+  const CsrView<T> vk = k.template view<T>();
+  if (K <= 32)
+    cuda_check(cudaLaunchKernelEx(&cfg, chunk_kernel<T, 1>, vt, vk, y, x_bar, K, len, flags,
+                                  last_flags, pe, de, sync),
+               "chunk_kernel launch");
+  else
+    cuda_check(cudaLaunchKernelEx(&cfg, chunk_kernel<T, 2>, vt, vk, y, x_bar, K, len, flags,
+                                  last_flags, pe, de, sync),
+               "chunk_kernel launch");
+  ++p.launches;
+}
+
 // Two-stage per-case reduction of `t` over len rows; results land in
 // out[case*stride + offset + term] (device).
 template <class Terms, class Buf>

@@ -373,6 +373,29 @@ def sparse_random_lp(m: int, n: int, per_col: int = 8,
     return _kkt_lp(a, rng, f"sparse_random_{m}x{n}")
 
 
+def long_row_stack(m: int = 600, n: int = 900, per_col: int = 6, long_rows: int = 3,
+                   long_len: int = 700, cases: int = 20,
+                   seed: int = BASE_SEED + 5) -> CaseStack:
+    """A stack of `cases` known-optimum LPs sharing one matrix that mixes
+    `per_col` random rows per column with `long_rows` rows of `long_len`
+    nonzeros (longer than eight 32-nonzero segments). Cases differ in c."""
+    rng = np.random.default_rng(seed)
+    rows = np.concatenate([rng.integers(long_rows, m, size=n * per_col),
+                           np.repeat(np.arange(long_rows), long_len)])
+    cols = np.concatenate([np.repeat(np.arange(n), per_col),
+                           np.concatenate([rng.choice(n, long_len, replace=False)
+                                           for _ in range(long_rows)])])
+    vals = rng.standard_normal(rows.size)
+    key = rows.astype(np.int64) * n + cols
+    _, first = np.unique(key, return_index=True)
+    a = Csr.from_triplets(m, n, rows[first], cols[first], vals[first])
+    lp, _ = _kkt_lp(a, rng, f"long_rows_{m}x{n}")
+    c = lp.c[None, :] * (1.0 + 0.05 * rng.standard_normal((cases, n)))
+    return CaseStack(lp, [f"long_rows_case{k}" for k in range(cases)], c,
+                     np.repeat(lp.q[None, :], cases, 0), np.repeat(lp.lower[None, :], cases, 0),
+                     np.repeat(lp.upper[None, :], cases, 0))
+
+
 def packed_batch(count: int = 256, seed: int = BASE_SEED + 3,
                  min_rows: int = 500, max_rows: int = 50_000) -> List[Tuple[StandardLp, float]]:
     """`count` independent known-optimum LPs, rows log-uniform in

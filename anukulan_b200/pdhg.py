@@ -27,6 +27,7 @@ _lib = None
 # Every function the C ABI declares (include/anu_pdhg.h).
 EXPORTS = (
     "anu_pdhg_version", "anu_pdhg_default_options", "anu_last_error", "anu_device_count",
+    "anu_release_cached_memory",
     "anu_pdhg_solve", "anu_pdhg_create", "anu_pdhg_run", "anu_pdhg_destroy",
     "anu_evaluate_residual", "anu_estimate_matrix_norm",
     "anu_backend_allocate", "anu_backend_deallocate", "anu_backend_upload",
@@ -70,6 +71,7 @@ def lib():
     d("anu_pdhg_default_options", None, [_P(anu_pdhg_options)])
     d("anu_last_error", C.c_int, [C.c_char_p, C.c_int32])
     d("anu_device_count", C.c_int32, [])
+    d("anu_release_cached_memory", C.c_int64, [])
     d("anu_pdhg_solve", C.c_int, [_P(anu_lp), _P(anu_pdhg_options), _P(C.c_double),
                                   _P(C.c_double), _P(C.c_double), _P(C.c_double),
                                   _P(anu_pdhg_result)])
@@ -144,6 +146,12 @@ def version() -> str:
 
 def device_count() -> int:
     return int(lib().anu_device_count())
+
+
+def release_cached_memory() -> int:
+    """Frees the blocks destroyed solvers left cached for reuse; the bytes
+    freed."""
+    return int(lib().anu_release_cached_memory())
 
 
 def default_options() -> anu_pdhg_options:

@@ -407,7 +407,8 @@ def run_engine(args, rank, world, local_rank):
                                 device_id=torch.device("cuda", local_rank))
     st, cfg = stack_workload()
     opts = make_options(tolerance=TOL, precision=PRECISION_FP32, device=local_rank, profile=1,
-                        split_stacks=0 if args.no_split else 1)
+                        split_stacks=0 if args.no_split else 1,
+                        persistent_chunks=1 if args.persistent else 0)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
 
     def barrier():
@@ -488,7 +489,7 @@ def run_engine(args, rank, world, local_rank):
         # The engine runs a stack of 16 or more cases as two half-stacks at
         # once (two streams): a launch carries half the cases, and two are in
         # flight at a time.
-        split = st.num_cases >= 16 and not args.no_split
+        split = st.num_cases >= 16 and not args.no_split and not args.persistent
         per_launch_cases = (st.num_cases + 1) // 2 if split else st.num_cases
         bytes_it = algorithmic_bytes_per_iteration(nnz, m, n, per_launch_cases, 4, 4)
         per_launch_s = dev_iter_s / max(dev_iters, 1) / 2.0
@@ -520,7 +521,8 @@ def run_engine(args, rank, world, local_rank):
                     "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                     "parts_ms_median": ({k: round(1e3 * float(np.median([p[i] for p in e2e_parts])), 2)
                                          for i, k in enumerate(("create", "solve", "close"))}
-                                        if e2e_parts else None)},
+                                        if e2e_parts else None),
+                    "step_ms": [round(v, 2) for v in e2e_ms]},
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None,
@@ -648,6 +650,8 @@ def main(argv=None):
                     help="skip the end-to-end pass (profiling runs)")
     ap.add_argument("--no-split", action="store_true",
                     help="run the stack as one stack on one stream (profiling)")
+    ap.add_argument("--persistent", action="store_true",
+                    help="run each iteration chunk of the stack as one cooperative kernel")
     ap.add_argument("--workload", default="stack",
                     choices=["stack", "spmv", "packed", "adjoint", "powerlaw"])
     ap.add_argument("--tolerance", type=float, default=1e-6,

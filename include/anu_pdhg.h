@@ -160,8 +160,16 @@ typedef struct anu_pdhg_options {
    * Events do not serialise the stream. 0 = off. */
   int32_t profile;
   /* Case stacks of 16 or more cases run as two half-stacks at once, each on
-   * its own stream and host thread. 0 = one stack on one stream. 1 */
+   * its own stream and host thread. 0 = one stack on one stream. 1.
+   * Not used when the stack runs persistent chunks (below). */
   int32_t split_stacks;
+  /* 1: a case stack of 17 to 64 cases whose segment schedule fits in one
+   * wave of CTAs runs each chunk of iterations between termination checks
+   * as one cooperative kernel with grid barriers between its products, as
+   * one stack. 0 (default): graphs of two launches per iteration. On B200
+   * a grid barrier costs about as much as the launch it replaces, so the
+   * graphs of two half-stacks are faster on the stacks measured so far. */
+  int32_t persistent_chunks;
 } anu_pdhg_options;
 
 /* PdhgResidual, src/anukulan/pdhg.hpp:429-496. */
@@ -236,6 +244,14 @@ int anu_last_error(char* buf, int32_t size);
 
 /* Number of CUDA devices visible (0 when none). Never fails. */
 int32_t anu_device_count(void);
+
+/* Destroyed handles leave their device and pinned host blocks in a
+ * process-wide cache, from which the next handles on the same device take
+ * them instead of allocating. This frees every cached block and returns the
+ * bytes freed. Safe at any time: no live handle owns a cached block. No
+ * counterpart in the reference, which allocates through its backend per
+ * solve (src/anukulan/pdhg.cpp:377-1285). */
+int64_t anu_release_cached_memory(void);
 
 /* ----------------------------------------------------------- single LP */
 

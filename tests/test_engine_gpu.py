@@ -285,6 +285,63 @@ def test_case_stack_warm_start_matches_single(engine, stack, count):
         assert abs(warm[k].objective - single.objective) <= 1e-8 * abs(single.objective), k
 
 
+def test_cached_blocks_reused_across_solvers(engine, stack):
+    # Each closed solver leaves its blocks in the process-wide cache and the
+    # next one takes them: the results of successive create-solve-close
+    # cycles (two half-stacks, FP32) must be identical, before and after the
+    # cache is released.
+    sub = _rolling(stack, list(range(20)))
+
+    def cycle():
+        solver = engine.CaseStackSolver(sub.base, sub.c, sub.q, sub.lower, sub.upper,
+                                        tolerance=1e-6, precision=PRECISION_FP32)
+        try:
+            return solver.solve()
+        finally:
+            solver.close()
+
+    first = cycle()
+    again = cycle()
+    assert engine.release_cached_memory() > 0
+    after = cycle()
+    for res in (again, after):
+        for a, b in zip(first, res):
+            assert a.status == b.status == OPTIMAL
+            assert a.iterations == b.iterations
+            assert np.array_equal(a.x, b.x) and np.array_equal(a.y, b.y)
+
+
+@pytest.mark.parametrize("precision", [0, PRECISION_FP32])
+def test_persistent_chunks_match_graphs(engine, stack, precision):
+    # One cooperative launch per chunk runs the same arithmetic in the same
+    # order as the two launches per iteration of the graphs: identical
+    # iterates, iteration counts and restarts, case by case.
+    kw = dict(tolerance=1e-6, precision=precision, split_stacks=0)
+    persistent = engine.solve_case_stack(stack, persistent_chunks=1, **kw)
+    graphs = engine.solve_case_stack(stack, persistent_chunks=0, **kw)
+    for k, (a, b) in enumerate(zip(persistent, graphs)):
+        assert a.status == b.status == OPTIMAL, (k, a.message)
+        assert a.iterations == b.iterations and a.restarts == b.restarts, k
+        assert np.array_equal(a.x, b.x) and np.array_equal(a.y, b.y), k
+    assert persistent[0].kernel_launches < graphs[0].kernel_launches
+
+
+@pytest.mark.parametrize("precision", [0, PRECISION_FP32])
+def test_persistent_chunks_long_rows(engine, precision):
+    # Rows of 700 nonzeros cut into segments longer than a warp: the chunk
+    # kernel reloads the tail of those segments in every phase. A fixed
+    # iteration budget, compared bit for bit with the graphs.
+    st = lpgen.long_row_stack()
+    kw = dict(max_iterations=400, precision=precision, split_stacks=0,
+              polish_on_exit=0, polish_feasibility=0)
+    persistent = engine.solve_case_stack(st, persistent_chunks=1, **kw)
+    graphs = engine.solve_case_stack(st, persistent_chunks=0, **kw)
+    for k, (a, b) in enumerate(zip(persistent, graphs)):
+        assert a.iterations == b.iterations == 400, k
+        assert np.array_equal(a.x, b.x) and np.array_equal(a.y, b.y), k
+    assert persistent[0].kernel_launches < graphs[0].kernel_launches
+
+
 def test_case_stack_equals_single_solves(engine, stack):
     sub = lpgen.CaseStack(stack.base, stack.names[:5], stack.c[:5], stack.q[:5],
                           stack.lower[:5], stack.upper[:5])

@@ -131,7 +131,8 @@ def test_defaults_match_reference_pdhg_options():
     ref = abi.options_dict(oracle.ref_default_options())
     mine = abi.options_dict(abi.make_options())
     for k, v in ref.items():
-        if k in ("precision", "refinement", "device", "use_graphs", "profile", "split_stacks"):
+        if k in ("precision", "refinement", "device", "use_graphs", "profile", "split_stacks",
+                 "persistent_chunks"):
             continue
         assert mine[k] == v, k
 
