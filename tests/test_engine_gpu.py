@@ -23,6 +23,7 @@ from anukulan_b200.abi import (ITERATION_LIMIT, OPTIMAL, PRECISION_FP32,
 pytestmark = pytest.mark.gpu
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "pdhg_golden.npz")
+SIMPLEX = os.path.join(os.path.dirname(__file__), "golden", "simplex_objectives.npz")
 FP64_ITERATE_RTOL = 1e-10
 
 
@@ -79,6 +80,8 @@ def test_random_lp_full_solve_fp64_matches_golden(engine):
     assert abs(r.iterations - int(g["random_1000x1500/iterations"])) <= 40
     assert abs(r.objective - float(g["random_1000x1500/objective"])) <= 1e-9 * abs(obj)
     assert abs(r.objective - obj) <= 1e-5 * abs(obj)
+    simplex = float(np.load(SIMPLEX)["random_1000x1500/objective"])
+    assert abs(r.objective - simplex) <= 1e-6 * max(1.0, abs(simplex))
 
 
 def test_random_lp_fp32_reaches_tolerance(engine):
@@ -88,6 +91,8 @@ def test_random_lp_fp32_reaches_tolerance(engine):
     res = oracle.oracle_residual(lp, r.x, r.y)
     assert res.converged(1e-6), res
     assert abs(r.objective - obj) <= 1e-5 * abs(obj)
+    simplex = float(np.load(SIMPLEX)["random_1000x1500/objective"])
+    assert abs(r.objective - simplex) <= 1e-6 * max(1.0, abs(simplex))
 
 
 @pytest.mark.parametrize("tol", [1e-6, 1e-8])
@@ -233,6 +238,19 @@ def test_case_stack_fp32_reaches_tolerance(engine, stack):
             assert res_k.converged(1e-6), (k, res_k)
             ref_obj = float(g[f"refinery_case{k}/objective"])
             assert abs(r.objective - ref_obj) <= 1e-5 * abs(ref_obj)
+
+
+@pytest.mark.parametrize("precision", [0, PRECISION_FP32])
+def test_case_stack_objectives_match_simplex(engine, stack, precision):
+    # The objective oracle: the reference's dual simplex on every one of the
+    # 60 cases (tests/golden/simplex_objectives.npz). Solved to relative KKT
+    # 1e-6, each case's objective is within 1e-6 of it, relative.
+    g = np.load(SIMPLEX)
+    res = engine.solve_case_stack(stack, tolerance=1e-6, precision=precision)
+    for k, r in enumerate(res):
+        assert r.status == OPTIMAL, (k, r.message)
+        ref_obj = float(g["refinery/objective"][k])
+        assert abs(r.objective - ref_obj) <= 1e-6 * max(1.0, abs(ref_obj)), (k, r.objective, ref_obj)
 
 
 def _rolling(stack, idx):
