@@ -54,34 +54,7 @@ void cuda_check(cudaError_t status, const char* what) {
 
 // ------------------------------------------------------------ matrices
 
-static_assert(sizeof(SlabRows) == sizeof(SlabBlock) && alignof(SlabRows) == alignof(SlabBlock),
-              "host and device slab blocks share a layout");
-
-namespace {
-
-// The slab kernels' shared-memory limit, set once per device for every
-// epilogue the slab path is instantiated for.
-void allow_slab_smem(size_t bytes) {
-  int dev = 0;
-  ANU_CUDA(cudaGetDevice(&dev));
-  static std::mutex lock;
-  static std::map<int, size_t> done;
-  std::lock_guard<std::mutex> g(lock);
-  size_t& have = done[dev];
-  if (have >= bytes) return;
-  const int b = static_cast<int>(bytes);
-  ANU_CUDA(cudaFuncSetAttribute(slab_kernel<PrimalEpi<float>>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, b));
-  ANU_CUDA(cudaFuncSetAttribute(slab_kernel<DualEpi<float>>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, b));
-  ANU_CUDA(cudaFuncSetAttribute(slab_kernel<StoreEpi<float>>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, b));
-  have = bytes;
-}
-
-}  // namespace
-
-void DevCsr::upload(const HostCsr& a, bool with_fp32, cudaStream_t s, bool with_slabs) {
+void DevCsr::upload(const HostCsr& a, bool with_fp32, cudaStream_t s) {
   rows = a.rows;
   cols = a.cols;
   nnz = a.nnz();
@@ -124,41 +97,6 @@ void DevCsr::upload(const HostCsr& a, bool with_fp32, cudaStream_t s, bool with_
   put(row_seg, sch.row_seg);
   put(cta_row, sch.cta_row);
   put(cta_seg, sch.cta_seg);
-  slabs = 0;
-  SlabSchedule sl;
-  if (with_fp32 && with_slabs && cols >= kSlabMinCols && nnz >= kSlabMinNnz)
-    sl = slab_schedule(a, kSlabWidthMax, kSlabUnitTarget, kSlabUnitMax, kSlabBlockRows);
-  int dev = 0, sms = 0, smem_optin = 0;
-  if (sl.ok) {
-    ANU_CUDA(cudaGetDevice(&dev));
-    ANU_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    ANU_CUDA(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-  }
-  const int32_t workers = sl.ok ? std::max(1, sms / sl.slabs) : 0;
-  const int32_t nb = static_cast<int32_t>(sl.blocks.size());
-  if (sl.ok && slab_smem_bytes(sl.width) <= static_cast<size_t>(smem_optin) &&
-      nb <= static_cast<int64_t>(workers) * kSlabThreads) {
-    allow_slab_smem(slab_smem_bytes(sl.width));
-    slabs = sl.slabs;
-    slab_width = sl.width;
-    slab_blocks = nb;
-    slab_grid = sl.slabs * workers;
-    slab_rows.alloc(sl.blocks.size());
-    ANU_CUDA(cudaMemcpyAsync(slab_rows.p, sl.blocks.data(), sizeof(SlabRows) * sl.blocks.size(),
-                             cudaMemcpyHostToDevice, s));
-    put(slab_unit, sl.unit_begin);
-    slab_packed.alloc(std::max<size_t>(sl.packed.size(), 1));
-    slab_value.alloc(std::max<size_t>(sl.value.size(), 1));
-    if (!sl.packed.empty()) {
-      ANU_CUDA(cudaMemcpyAsync(slab_packed.p, sl.packed.data(), sizeof(uint32_t) * sl.packed.size(),
-                               cudaMemcpyHostToDevice, s));
-      ANU_CUDA(cudaMemcpyAsync(slab_value.p, sl.value.data(), sizeof(float) * sl.value.size(),
-                               cudaMemcpyHostToDevice, s));
-    }
-    slab_part.alloc(static_cast<size_t>(sl.slabs) * rows);
-    slab_arrivals.alloc(sl.blocks.size());
-    ANU_CUDA(cudaMemsetAsync(slab_arrivals.p, 0, sizeof(uint32_t) * sl.blocks.size(), s));
-  }
   ANU_CUDA(cudaStreamSynchronize(s));
 }
 
@@ -495,9 +433,8 @@ std::unique_ptr<Problem> make_problem(const anu_lp& lp, const anu_pdhg_options& 
   p->kt = transpose(p->k);
   if (scaling_seconds) *scaling_seconds = now_seconds() - t0;
   const bool fp32 = o.precision == ANU_PRECISION_FP32;
-  p->slab_products = o.slab_products != 0;
-  p->dk.upload(p->k, fp32, p->stream, p->slab_products);
-  p->dkt.upload(p->kt, fp32, p->stream, p->slab_products);
+  p->dk.upload(p->k, fp32, p->stream);
+  p->dkt.upload(p->kt, fp32, p->stream);
   p->row_scale.alloc(std::max(p->m, 1));
   p->col_scale.alloc(std::max(p->n, 1));
   if (p->m > 0)
@@ -540,9 +477,8 @@ std::unique_ptr<Problem> clone_problem(const Problem& src) {
   p->unit_scaling = src.unit_scaling;
   p->matrix_norm = src.matrix_norm;
   const bool fp32 = p->precision == ANU_PRECISION_FP32;
-  p->slab_products = src.slab_products;
-  p->dk.upload(p->k, fp32, p->stream, p->slab_products);
-  p->dkt.upload(p->kt, fp32, p->stream, p->slab_products);
+  p->dk.upload(p->k, fp32, p->stream);
+  p->dkt.upload(p->kt, fp32, p->stream);
   p->row_scale.alloc(std::max(p->m, 1));
   p->col_scale.alloc(std::max(p->n, 1));
   if (p->m > 0)
@@ -2390,7 +2326,6 @@ void anu_pdhg_default_options(anu_pdhg_options* o) {
   o->profile = 0;
   o->split_stacks = 1;
   o->persistent_chunks = 0;
-  o->slab_products = 1;
 }
 
 int anu_last_error(char* buf, int32_t size) { return anu::copy_last_error(buf, size); }
@@ -2473,41 +2408,6 @@ int anu_estimate_matrix_norm(const anu_lp* lp, int32_t iterations, double tolera
     o.known_matrix_norm = 1.0;  // skip the default estimate; measured below
     auto p = anu::make_problem(*lp, o, nullptr, nullptr);
     *norm = anu::device_matrix_norm(*p, iterations, tolerance);
-  });
-}
-
-int anu_spmv_fp32(const anu_csr* a, const float* x, float* y, int32_t kernel, int32_t* used) {
-  return guarded([&] {
-    if (a == nullptr || (a->cols > 0 && x == nullptr) || (a->rows > 0 && y == nullptr))
-      throw Error(ANU_ERR_INVALID, "null argument");
-    if (kernel < ANU_SPMV_AUTO || kernel > ANU_SPMV_SLABS) throw Error(ANU_ERR_INVALID, "unknown kernel");
-    const std::string e = anu::validate_csr(a->rows, a->cols, a->nnz, a->start, a->index);
-    if (!e.empty()) throw Error(ANU_ERR_INVALID, "invalid matrix: " + e);
-    if (a->nnz > 0 && a->value == nullptr) throw Error(ANU_ERR_INVALID, "null matrix values");
-    int count = 0;
-    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
-      cudaGetLastError();
-      throw Error(ANU_ERR_NO_DEVICE, "no CUDA device is available; this engine has no CPU fallback");
-    }
-    const anu::HostCsr h = anu::copy_csr(a->rows, a->cols, a->nnz, a->start, a->index, a->value);
-    anu::Exec ex;
-    ANU_CUDA(cudaStreamCreateWithFlags(&ex.stream, cudaStreamNonBlocking));
-    struct StreamGuard {
-      cudaStream_t s;
-      ~StreamGuard() { cudaStreamDestroy(s); }
-    } guard{ex.stream};
-    anu::DevCsr d;
-    d.upload(h, true, ex.stream, kernel != ANU_SPMV_ROWS);
-    if (kernel == ANU_SPMV_SLABS && d.slabs == 0)
-      throw Error(ANU_ERR_INVALID, "the matrix does not take column slabs");
-    anu::DevBuf<float> dx(std::max<int32_t>(a->cols, 1)), dy(std::max<int32_t>(a->rows, 1));
-    if (a->cols > 0)
-      ANU_CUDA(cudaMemcpyAsync(dx.p, x, sizeof(float) * a->cols, cudaMemcpyHostToDevice, ex.stream));
-    anu::product<float, float, float>(ex, d, dx.p, 1, anu::StoreEpi<float>{1, dy.p});
-    if (a->rows > 0)
-      ANU_CUDA(cudaMemcpyAsync(y, dy.p, sizeof(float) * a->rows, cudaMemcpyDeviceToHost, ex.stream));
-    ANU_CUDA(cudaStreamSynchronize(ex.stream));
-    if (used) *used = d.slabs > 0 ? ANU_SPMV_SLABS : ANU_SPMV_ROWS;
   });
 }
 

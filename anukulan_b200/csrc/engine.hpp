@@ -158,29 +158,10 @@ struct DevCsr {
   int32_t num_blocks = 0;
   DevBuf<int32_t> seg_begin, row_seg, cta_row, cta_seg;
   int32_t num_ctas = 0;
-  // Column-slab schedule of the single-LP FP32 product, built when the
-  // matrix is wide and large enough (slabs == 0: the row blocks are used).
-  int32_t slabs = 0, slab_width = 0, slab_blocks = 0, slab_grid = 0;
-  DevBuf<SlabRows> slab_rows;
-  DevBuf<int32_t> slab_unit;
-  DevBuf<uint32_t> slab_packed;
-  DevBuf<float> slab_value, slab_part;
-  DevBuf<uint32_t> slab_arrivals;
-  // with_slabs: build the slab schedule where it applies (FP32 values only).
-  void upload(const HostCsr& a, bool with_fp32, cudaStream_t s, bool with_slabs = false);
+  void upload(const HostCsr& a, bool with_fp32, cudaStream_t s);
   template <class V>
   CsrView<V> view() const;
-  SlabView slab_view() const {
-    return {rows, cols, slabs, slab_width, slab_blocks, slab_rows.p, slab_unit.p,
-            slab_packed.p, slab_value.p, slab_part.p, slab_arrivals.p};
-  }
 };
-
-// Matrices at least this wide and with this many nonzeros take the column
-// slabs in FP32 single-LP products: below that the gathered vector stays in
-// L1 and the staged slab would cost more than it saves.
-constexpr int32_t kSlabMinCols = 131072;
-constexpr int32_t kSlabMinNnz = 1 << 20;
 
 // Everything that depends on the matrix alone: the scaled matrix and its
 // transpose (host and device), the scaling, ||K~||, the stream.
@@ -197,7 +178,6 @@ struct Problem : Exec {
   DevBuf<double> row_scale, col_scale;
   double matrix_norm = 0.0;
   bool owns_stream = false;
-  bool slab_products = true;  // options.slab_products
   int device = 0;
   ~Problem();
 };

@@ -530,195 +530,6 @@ __global__ void __launch_bounds__(kThreads) seg_kernel(CsrView<V> a, const X* __
   }
 }
 
-// ----------------------------------------------------------- slab_kernel
-
-// One LP in FP32 whose gathered vector is too long for the gathers to stay
-// in L1: every gathered element is a random 4-byte load that costs a whole
-// 32-byte sector and an L1 tag lookup, and that, not the bytes, bounds the
-// row-block kernel. Here the columns are cut into slabs small enough for
-// shared memory. A CTA is bound to one slab: it copies that slab of x into
-// shared memory once (coalesced, 16-byte loads), then walks units - the
-// nonzeros of one row block that fall in its slab, stored contiguously as
-// packed (row in block, column in slab) pairs with their values - and
-// gathers from shared memory. Each unit's per-row partial sums (its rows
-// summed left to right, a warp per row longer than kSerialRow) go to
-// part[slab][row]. When a CTA has written all its units it counts itself
-// in on each of their blocks; the CTA that arrives last on a block adds the
-// block's slab partials in slab order (fixed, so the sums are
-// deterministic) and runs the epilogue over the block's rows.
-//
-// The grid is slabs x workers CTAs, CTA c on slab c % slabs, taking blocks
-// c / slabs, + workers, ... No CTA waits for another: the last arrival is
-// decided by an atomic counter per block, which that CTA resets to zero for
-// the next launch.
-constexpr int kSlabThreads = 512;
-constexpr int kSlabWidthMax = 45056;  // floats of a slab: 176 KB of shared memory
-constexpr int kSlabUnitTarget = 2048;
-constexpr int kSlabUnitMax = 4096;
-constexpr int kSlabBlockRows = 1024;
-constexpr int kSlabPerThread = kSlabUnitMax / kSlabThreads;
-static_assert(kSlabBlockRows <= 2 * kSlabThreads, "two rows per thread in the row sums");
-
-struct SlabRows {
-  int32_t row_begin;
-  int32_t row_end;
-};
-
-struct SlabView {
-  int32_t rows;
-  int32_t cols;
-  int32_t slabs;
-  int32_t width;
-  int32_t num_blocks;
-  const SlabRows* __restrict__ blocks;
-  const int32_t* __restrict__ unit_begin;
-  const uint32_t* __restrict__ packed;
-  const float* __restrict__ value;
-  float* part;           // slabs x rows
-  uint32_t* arrivals;    // num_blocks, zero between launches
-};
-
-// Dynamic shared memory of slab_kernel for a slab width.
-__host__ __device__ constexpr size_t slab_smem_bytes(int32_t width) {
-  return sizeof(float) * static_cast<size_t>((width + 3) / 4 * 4)  // the slab of x
-         + sizeof(float) * kSlabUnitMax                            // products
-         + sizeof(uint16_t) * kSlabUnitMax                         // row of each product
-         + 2 * sizeof(uint16_t) * kSlabBlockRows                   // row ranges
-         + sizeof(uint16_t) * kSlabBlockRows                       // long rows
-         + sizeof(int32_t) * kSlabThreads;                         // blocks to finish
-}
-
-template <class Epi>
-__global__ void __launch_bounds__(kSlabThreads, 1)
-    slab_kernel(SlabView a, const float* __restrict__ x, Epi epi) {
-  extern __shared__ __align__(16) unsigned char slab_smem[];
-  const int32_t width4 = (a.width + 3) / 4 * 4;
-  float* xs = reinterpret_cast<float*>(slab_smem);
-  float* prod = xs + width4;
-  uint16_t* rid = reinterpret_cast<uint16_t*>(prod + kSlabUnitMax);
-  uint16_t* rbeg = rid + kSlabUnitMax;
-  uint16_t* rend = rbeg + kSlabBlockRows;
-  uint16_t* long_rows = rend + kSlabBlockRows;
-  int32_t* finish = reinterpret_cast<int32_t*>(long_rows + kSlabBlockRows);
-  __shared__ int32_t nlong;
-  __shared__ int32_t nfinish;
-  const int t = threadIdx.x;
-  const int warp = t / 32;
-  const int lane = t % 32;
-  const int32_t P = a.slabs;
-  const int32_t slab = static_cast<int32_t>(blockIdx.x) % P;
-  const int32_t workers = static_cast<int32_t>(gridDim.x) / P;
-  const int32_t first = static_cast<int32_t>(blockIdx.x) / P;
-  // ---- independent of the previous launch: the first unit.
-  uint32_t pk[kSlabPerThread];
-  float pv[kSlabPerThread];
-  int32_t ub = 0, un = 0;
-  auto load_unit = [&](int32_t b) {
-    const int32_t u = b * P + slab;
-    ub = a.unit_begin[u];
-    un = a.unit_begin[u + 1] - ub;
-#pragma unroll
-    for (int q = 0; q < kSlabPerThread; ++q) {
-      const int32_t k = q * kSlabThreads + t;
-      pk[q] = k < un ? a.packed[ub + k] : 0u;
-      pv[q] = k < un ? a.value[ub + k] : 0.0f;
-    }
-  };
-  if (first < a.num_blocks) load_unit(first);
-  if (t == 0) nfinish = 0;
-  // ---- the slab of x is the previous launch's output.
-  pdl_wait();
-  pdl_launch();
-  {
-    const int32_t c0 = slab * a.width;
-    const int32_t len = min(a.width, a.cols - c0);
-    const float* src = x + c0;
-    int32_t done = 0;
-    if ((reinterpret_cast<uintptr_t>(src) & 15u) == 0) {
-      const int32_t n4 = len / 4;
-      const float4* s4 = reinterpret_cast<const float4*>(src);
-      float4* d4 = reinterpret_cast<float4*>(xs);
-      for (int32_t i = t; i < n4; i += kSlabThreads) d4[i] = s4[i];
-      done = n4 * 4;
-    }
-    for (int32_t i = done + t; i < len; i += kSlabThreads) xs[i] = src[i];
-  }
-  for (int32_t b = first; b < a.num_blocks; b += workers) {
-    const SlabRows blk = a.blocks[b];
-    const int32_t nrows = blk.row_end - blk.row_begin;
-    const int32_t n = un;
-    __syncthreads();  // the slab is staged; the previous unit is done with shared memory
-    for (int32_t i = t; i < nrows; i += kSlabThreads) {
-      rbeg[i] = 0;
-      rend[i] = 0;
-    }
-    if (t == 0) nlong = 0;
-#pragma unroll
-    for (int q = 0; q < kSlabPerThread; ++q) {
-      const int32_t k = q * kSlabThreads + t;
-      if (k < n) {
-        prod[k] = pv[q] * xs[pk[q] & 0xffffu];
-        rid[k] = static_cast<uint16_t>(pk[q] >> 16);
-      }
-    }
-    // The next unit's loads fly while this one is summed.
-    if (b + workers < a.num_blocks) load_unit(b + workers);
-    __syncthreads();
-    for (int32_t k = t; k < n; k += kSlabThreads) {
-      const uint16_t r = rid[k];
-      if (k == 0 || rid[k - 1] != r) rbeg[r] = static_cast<uint16_t>(k);
-      if (k == n - 1 || rid[k + 1] != r) rend[r] = static_cast<uint16_t>(k + 1);
-    }
-    __syncthreads();
-    float* out = a.part + static_cast<size_t>(slab) * a.rows + blk.row_begin;
-    for (int32_t i = t; i < nrows; i += kSlabThreads) {
-      const int32_t kb = rbeg[i], ke = rend[i];
-      if (ke - kb > kSerialRow) {
-        long_rows[atomicAdd(&nlong, 1)] = static_cast<uint16_t>(i);
-      } else {
-        float s = 0.0f;
-        for (int32_t k = kb; k < ke; ++k) s += prod[k];
-        out[i] = s;
-      }
-    }
-    __syncthreads();
-    for (int32_t li = warp; li < nlong; li += kSlabThreads / 32) {
-      const int32_t i = long_rows[li];
-      const int32_t kb = rbeg[i], ke = rend[i];
-      float s = 0.0f;
-      for (int32_t k = kb + lane; k < ke; k += 32) s += prod[k];
-#pragma unroll
-      for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
-      if (lane == 0) out[i] = s;
-    }
-  }
-  // Count in on every block this CTA wrote; the last arrival finishes it.
-  __syncthreads();
-  {
-    const int32_t mine = first < a.num_blocks ? (a.num_blocks - 1 - first) / workers + 1 : 0;
-    if (t < mine) {
-      const int32_t b = first + t * workers;
-      __threadfence();  // this CTA's partials (ordered before by the barrier) first
-      const uint32_t before = atomicAdd(&a.arrivals[b], 1u);
-      if (before == static_cast<uint32_t>(P - 1)) {
-        __threadfence();  // the other CTAs' partials after their arrivals
-        a.arrivals[b] = 0u;
-        finish[atomicAdd(&nfinish, 1)] = b;
-      }
-    }
-  }
-  __syncthreads();
-  for (int32_t f = 0; f < nfinish; ++f) {
-    const SlabRows blk = a.blocks[finish[f]];
-    for (int32_t r = blk.row_begin + t; r < blk.row_end; r += kSlabThreads) {
-      typename Epi::Pre pre = epi.prefetch(r, 0);
-      float s = 0.0f;
-      for (int32_t q = 0; q < P; ++q) s += __ldcg(a.part + static_cast<size_t>(q) * a.rows + r);
-      epi.finish(r, 0, s, pre);
-    }
-  }
-}
-
 // ------------------------------------------------------------ chunk_kernel
 
 // A chunk of iterations of a case stack in ONE cooperative launch. The two

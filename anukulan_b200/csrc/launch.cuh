@@ -6,7 +6,6 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
-#include <type_traits>
 
 #include "kernels.cuh"
 
@@ -29,36 +28,11 @@ inline int grid_for(int64_t items, int per_block, int cap) {
 }
 
 
-// Epilogues the column-slab kernel is instantiated for (FP32 products).
-template <class Epi> struct SlabEpi : std::false_type {};
-template <> struct SlabEpi<PrimalEpi<float>> : std::true_type {};
-template <> struct SlabEpi<DualEpi<float>> : std::true_type {};
-template <> struct SlabEpi<StoreEpi<float>> : std::true_type {};
-
 // y = A x (any epilogue) for K cases.
 template <class V, class X, class Acc, class Epi, class Mat>
 void product(Exec& p, const Mat& a, const X* x, int K, const Epi& epi, bool pdl = false) {
   if (a.rows == 0) return;
   cudaStream_t s = p.stream;
-  if constexpr (std::is_same<V, float>::value && std::is_same<X, float>::value &&
-                std::is_same<Acc, float>::value && SlabEpi<Epi>::value) {
-    if (K == 1 && a.slabs > 0) {
-      cudaLaunchConfig_t cfg = {};
-      cfg.gridDim = dim3(a.slab_grid);
-      cfg.blockDim = dim3(kSlabThreads);
-      cfg.dynamicSmemBytes = slab_smem_bytes(a.slab_width);
-      cfg.stream = s;
-      cudaLaunchAttribute attr[1];
-      attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-      attr[0].val.programmaticStreamSerializationAllowed = 1;
-      cfg.attrs = attr;
-      cfg.numAttrs = pdl ? 1 : 0;
-      cuda_check(cudaLaunchKernelEx(&cfg, slab_kernel<Epi>, a.slab_view(), x, epi),
-                 "slab_kernel launch");
-      ++p.launches;
-      return;
-    }
-  }
   if (K == 1) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(a.num_blocks);

@@ -217,67 +217,4 @@ SegmentSchedule segment_schedule(const HostCsr& a, int32_t seg_nnz, int32_t seg_
   return s;
 }
 
-SlabSchedule slab_schedule(const HostCsr& a, int32_t width_max, int32_t unit_target,
-                           int32_t unit_max, int32_t block_rows) {
-  SlabSchedule s;
-  if (a.rows == 0 || a.cols == 0 || width_max < 4 || block_rows > (1 << 16) ||
-      width_max > (1 << 16))
-    return s;
-  // Equal slabs, each a multiple of 4 columns so its start is 16-byte aligned.
-  int32_t slabs = (a.cols + width_max - 1) / width_max;
-  int32_t width = (a.cols + slabs - 1) / slabs;
-  width = (width + 3) / 4 * 4;
-  slabs = (a.cols + width - 1) / width;
-  s.slabs = slabs;
-  s.width = width;
-  // Blocks of consecutive rows.
-  const int64_t budget = static_cast<int64_t>(slabs) * unit_target;
-  std::vector<SlabBlock> blocks;
-  for (int32_t r = 0; r < a.rows;) {
-    const int32_t r0 = r;
-    int64_t nz = 0;
-    while (r < a.rows && r - r0 < block_rows) {
-      const int32_t len = a.start[r + 1] - a.start[r];
-      if (r > r0 && nz + len > budget) break;
-      nz += len;
-      ++r;
-    }
-    blocks.push_back({r0, r});
-  }
-  auto block_nnz = [&](const SlabBlock& b) { return a.start[b.row_end] - a.start[b.row_begin]; };
-  std::stable_sort(blocks.begin(), blocks.end(), [&](const SlabBlock& x, const SlabBlock& y) {
-    return block_nnz(x) > block_nnz(y);
-  });
-  // Units: a counting sort of each block's nonzeros by slab, rows in order.
-  s.unit_begin.reserve(blocks.size() * slabs + 1);
-  s.packed.resize(a.nnz());
-  s.value.resize(a.nnz());
-  std::vector<int32_t> count(slabs), at(slabs);
-  int32_t base = 0;
-  for (const SlabBlock& b : blocks) {
-    std::fill(count.begin(), count.end(), 0);
-    for (int32_t k = a.start[b.row_begin]; k < a.start[b.row_end]; ++k) ++count[a.index[k] / width];
-    for (int32_t q = 0; q < slabs; ++q) {
-      if (count[q] > unit_max) return SlabSchedule{};
-      s.unit_begin.push_back(base);
-      at[q] = base;
-      base += count[q];
-    }
-    for (int32_t r = b.row_begin; r < b.row_end; ++r) {
-      const uint32_t local_row = static_cast<uint32_t>(r - b.row_begin) << 16;
-      for (int32_t k = a.start[r]; k < a.start[r + 1]; ++k) {
-        const int32_t col = a.index[k];
-        const int32_t q = col / width;
-        s.packed[at[q]] = local_row | static_cast<uint32_t>(col - q * width);
-        s.value[at[q]] = static_cast<float>(a.value[k]);
-        ++at[q];
-      }
-    }
-  }
-  s.unit_begin.push_back(base);
-  s.blocks = std::move(blocks);
-  s.ok = true;
-  return s;
-}
-
 }  // namespace anu

@@ -81,33 +81,6 @@ struct SegmentSchedule {
 SegmentSchedule segment_schedule(const HostCsr& a, int32_t seg_nnz, int32_t seg_per_cta,
                                  int32_t row_max);
 
-// Column-slab schedule of the single-LP FP32 product (see slab_kernel): the
-// columns are cut into `slabs` slabs of `width` columns (the last shorter),
-// so one slab of the gathered vector fits in a CTA's shared memory; the rows
-// into blocks of consecutive rows (at most `block_rows`, about
-// slabs * unit_target nonzeros). The nonzeros of block b in slab s form unit
-// (b, s), stored contiguously at unit_begin[b * slabs + s] in row order, each
-// as (row - block's first row) << 16 | (column - slab's first column) with
-// its FP32 value. Blocks are listed with the most nonzeros first.
-// `ok` is false when some unit would hold more than `unit_max` nonzeros (a
-// row with that many nonzeros in one slab); the matrix then takes the row
-// blocks instead.
-struct SlabBlock {
-  int32_t row_begin;
-  int32_t row_end;
-};
-struct SlabSchedule {
-  bool ok = false;
-  int32_t slabs = 0;
-  int32_t width = 0;
-  std::vector<SlabBlock> blocks;
-  std::vector<int32_t> unit_begin;  // blocks * slabs + 1
-  std::vector<uint32_t> packed;
-  std::vector<float> value;
-};
-SlabSchedule slab_schedule(const HostCsr& a, int32_t width_max, int32_t unit_target,
-                           int32_t unit_max, int32_t block_rows);
-
 double now_seconds();
 
 }  // namespace anu

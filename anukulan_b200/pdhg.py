@@ -29,7 +29,7 @@ EXPORTS = (
     "anu_pdhg_version", "anu_pdhg_default_options", "anu_last_error", "anu_device_count",
     "anu_release_cached_memory",
     "anu_pdhg_solve", "anu_pdhg_create", "anu_pdhg_run", "anu_pdhg_destroy",
-    "anu_evaluate_residual", "anu_estimate_matrix_norm", "anu_spmv_fp32",
+    "anu_evaluate_residual", "anu_estimate_matrix_norm",
     "anu_backend_allocate", "anu_backend_deallocate", "anu_backend_upload",
     "anu_backend_download", "anu_backend_fill", "anu_backend_copy", "anu_backend_prepare",
     "anu_backend_release", "anu_backend_multiply", "anu_backend_dot", "anu_backend_two_norm",
@@ -83,8 +83,6 @@ def lib():
                                          _P(anu_pdhg_residual)])
     d("anu_estimate_matrix_norm", C.c_int, [_P(anu_lp), C.c_int32, C.c_double,
                                             _P(C.c_double)])
-    d("anu_spmv_fp32", C.c_int, [_P(anu_csr), _P(C.c_float), _P(C.c_float), C.c_int32,
-                                 _P(C.c_int32)])
     d("anu_pdhg_batch_create", C.c_int, [_P(anu_lp), C.c_int32, _P(C.c_double),
                                          _P(C.c_double), _P(C.c_double), _P(C.c_double),
                                          _P(anu_pdhg_options), _P(C.c_void_p)])
@@ -236,25 +234,6 @@ def estimate_matrix_norm(lp: StandardLp, iterations: int = 200, tolerance: float
     out = C.c_double(0.0)
     check(lib().anu_estimate_matrix_norm(CLp(lp).ref(), iterations, tolerance, C.byref(out)))
     return out.value
-
-
-SPMV_AUTO, SPMV_ROWS, SPMV_SLABS = 0, 1, 2
-
-
-def spmv_fp32(a, x, kernel: int = SPMV_AUTO):
-    """y = A x in FP32 through the engine's single-LP product kernels
-    (``anu_spmv_fp32``); returns (y, kernel that ran)."""
-    start = np.ascontiguousarray(a.start, np.int32)
-    index = np.ascontiguousarray(a.index, np.int32)
-    value = np.ascontiguousarray(a.value, np.float64)
-    xs = np.ascontiguousarray(x, np.float32)
-    y = np.zeros(a.rows, np.float32)
-    m = anu_csr(a.rows, a.cols, a.nnz, start.ctypes.data_as(_P(C.c_int32)),
-                index.ctypes.data_as(_P(C.c_int32)), value.ctypes.data_as(_P(C.c_double)))
-    used = C.c_int32(0)
-    check(lib().anu_spmv_fp32(C.byref(m), xs.ctypes.data_as(_P(C.c_float)),
-                              y.ctypes.data_as(_P(C.c_float)), kernel, C.byref(used)))
-    return y, used.value
 
 
 class CaseStackSolver:

@@ -159,20 +159,16 @@ def spmv_leg(iterations, device, peak):
            "peak_GBps": peak,
            "note": "algorithmic bytes = 2 nnz (s_a + 4) + 4 (m + n + 2) + s_x (8n + 7m); "
                    "each gathered x or y element also moves a 32-byte sector through L1"}
-    legs = (("fp32", PRECISION_FP32, 4, 1, "slab_kernel (column slabs in shared memory)"),
-            ("fp32_row_blocks", PRECISION_FP32, 4, 0, "rows_kernel (gathers through L1)"),
-            ("fp64", PRECISION_FP64, 8, 1, "rows_kernel (gathers through L1)"))
-    for name, prec, size, slabs, kernel in legs:
+    for name, prec, size in (("fp32", PRECISION_FP32, 4), ("fp64", PRECISION_FP64, 8)):
         opts = make_options(tolerance=1e-12, precision=prec, max_iterations=iterations,
-                            profile=1, polish_feasibility=0, polish_on_exit=0, device=device,
-                            slab_products=slabs)
+                            profile=1, polish_feasibility=0, polish_on_exit=0, device=device)
         r = pdhg.solve_pdhg(lp, opts)
         per_it = r.device_iteration_seconds / max(r.device_iterations, 1)
         b = algorithmic_bytes_per_iteration(nnz, m, n, 1, size, size)
         out[name] = {"us_per_iteration": per_it * 1e6, "iterations_per_second": 1.0 / per_it,
                      "algorithmic_bytes_per_iteration": b,
                      "achieved_GBps": b / per_it / 1e9, "frac": b / per_it / 1e9 / peak,
-                     "kernel": kernel, "kernel_launches": int(r.kernel_launches)}
+                     "kernel_launches": int(r.kernel_launches)}
     return out
 
 

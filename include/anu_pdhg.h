@@ -170,13 +170,6 @@ typedef struct anu_pdhg_options {
    * a grid barrier costs about as much as the launch it replaces, so the
    * graphs of two half-stacks are faster on the stacks measured so far. */
   int32_t persistent_chunks;
-  /* 1 (default): single-LP FP32 products over a matrix with at least
-   * 131,072 columns and 2^20 nonzeros gather from column slabs staged in
-   * shared memory (slab_kernel) instead of from global memory through L1
-   * (rows_kernel). The two sum in different orders, so FP32 iterates differ
-   * in rounding. 0: always the row blocks. FP64 products always take the
-   * row blocks. */
-  int32_t slab_products;
 } anu_pdhg_options;
 
 /* PdhgResidual, src/anukulan/pdhg.hpp:429-496. */
@@ -291,16 +284,6 @@ int anu_evaluate_residual(const anu_lp* lp, const double* x, const double* y,
  * iteration on K'K on the device, FP64. */
 int anu_estimate_matrix_norm(const anu_lp* lp, int32_t iterations,
                              double tolerance, double* norm);
-
-/* y = A x in FP32 through the single-LP product kernels, from host arrays
- * (x: cols, y: rows), on the current device: the FP32 counterpart of
- * LinAlgBackend::multiply (src/anukulan/backend.hpp:58) that the engine's
- * FP32 iterations run. kernel: ANU_SPMV_AUTO picks as a solve does,
- * ANU_SPMV_ROWS forces the row blocks, ANU_SPMV_SLABS the column slabs
- * (ANU_ERR_INVALID when the matrix does not take them). *used receives the
- * kernel that ran (ANU_SPMV_ROWS or ANU_SPMV_SLABS); it may be NULL. */
-enum { ANU_SPMV_AUTO = 0, ANU_SPMV_ROWS = 1, ANU_SPMV_SLABS = 2 };
-int anu_spmv_fp32(const anu_csr* a, const float* x, float* y, int32_t kernel, int32_t* used);
 
 /* ------------------------------------------------------ LinAlgBackend seam
  * The coarse operations of LinAlgBackend (src/anukulan/backend.hpp:24-215) on
