@@ -124,9 +124,15 @@ class ClockSampler:
 
 # ---------------------------------------------------------------- workloads
 
-def stack_workload():
+def stack_workload(cases=None):
     from anukulan_b200 import lpgen
     st = lpgen.refinery_stack()
+    if cases is not None and cases < st.num_cases:
+        # The first `cases` cases: a profiling case with one launch's case
+        # count of the split stack, on one stream.
+        idx = list(range(cases))
+        st = lpgen.CaseStack(st.base, [st.names[i] for i in idx], st.c[idx], st.q[idx],
+                             st.lower[idx], st.upper[idx])
     cfg = {"workload": "refinery_case_stack", "cases": st.num_cases,
            "rows": st.base.num_rows, "cols": st.base.num_cols, "nnz": st.base.k.nnz,
            "tolerance": TOL, "precision": "fp32 iterates, fp64 checks",
@@ -405,7 +411,7 @@ def run_engine(args, rank, world, local_rank):
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600),
                                 device_id=torch.device("cuda", local_rank))
-    st, cfg = stack_workload()
+    st, cfg = stack_workload(args.cases)
     opts = make_options(tolerance=TOL, precision=PRECISION_FP32, device=local_rank, profile=1,
                         split_stacks=0 if args.no_split else 1,
                         persistent_chunks=1 if args.persistent else 0)
@@ -643,6 +649,8 @@ def main(argv=None):
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--cases", type=int, default=None,
+                    help="solve only the first N cases of the stack (profiling)")
     ap.add_argument("--ref-seconds", type=float, default=10.0)
     ap.add_argument("--no-gpu-reference", dest="gpu_reference", action="store_false",
                     help="reference arm: skip the reference's own CUDA backend leg")

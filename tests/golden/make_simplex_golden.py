@@ -11,8 +11,11 @@ stack and the seeded 1000 x 1500 random LP, and stores per LP the simplex
 status, objective and iteration count. The same LPs are solved again by
 scipy's bundled HiGHS (an independent simplex/IPM) and its objectives are
 stored beside them as a cross-check; the random LP also stores its planted
-optimum c'x0. The tests check the engine's objectives against these without
-the reference at run time.
+optimum c'x0. For the refinery cases it also stores the objective, status and
+iteration count of the reference's own FP64 PDHG (solve_pdhg, cpu_backend,
+default options) at relative KKT 1e-6, which is how far from the simplex
+objective that tolerance lets PDHG land. The tests check the engine's
+objectives against these without the reference at run time.
 """
 import os
 import sys
@@ -52,22 +55,29 @@ def highs_objective(lp):
 def main():
     out = {}
     stack = lpgen.refinery_stack()
-    status, obj, its, hobj = [], [], [], []
+    status, obj, its, hobj, pobj, pst, pits = [], [], [], [], [], [], []
     t0 = time.perf_counter()
     for k in range(stack.num_cases):
         lp = stack.case(k)
         st, o, it, _, _ = oracle.ref_simplex(lp)
         hs, ho = highs_objective(lp)
+        pd = oracle.ref_solve(lp, tolerance=1e-6)
+        pobj.append(pd.objective)
+        pst.append(pd.status)
+        pits.append(pd.iterations)
         status.append(st)
         obj.append(o)
         its.append(it)
         hobj.append(ho)
         print(f"refinery case {k:2d} {stack.names[k]:28s} simplex {st} {o:.12g} ({it} it)"
-              f"  highs {hs} {ho:.12g}")
+              f"  highs {hs} {ho:.12g}  pdhg {pd.objective:.12g} ({pd.iterations} it)")
     out["refinery/status"] = np.array(status, np.int32)
     out["refinery/objective"] = np.array(obj)
     out["refinery/iterations"] = np.array(its, np.int32)
     out["refinery/highs_objective"] = np.array(hobj)
+    out["refinery/pdhg_objective"] = np.array(pobj)
+    out["refinery/pdhg_status"] = np.array(pst, np.int32)
+    out["refinery/pdhg_iterations"] = np.array(pits, np.int32)
     print(f"refinery stack: {time.perf_counter() - t0:.1f} s")
 
     lp, planted = lpgen.random_lp()

@@ -243,14 +243,26 @@ def test_case_stack_fp32_reaches_tolerance(engine, stack):
 @pytest.mark.parametrize("precision", [0, PRECISION_FP32])
 def test_case_stack_objectives_match_simplex(engine, stack, precision):
     # The objective oracle: the reference's dual simplex on every one of the
-    # 60 cases (tests/golden/simplex_objectives.npz). Solved to relative KKT
-    # 1e-6, each case's objective is within 1e-6 of it, relative.
+    # 60 cases (tests/golden/simplex_objectives.npz). Relative KKT 1e-6 bounds
+    # the duality gap by 1e-6 (1 + |c'x| + |q'y|), about 2e-6 of the
+    # objective, so each case is held to 2e-6 relative. The reference's own
+    # PDHG at 1e-6 puts 59 of the 60 within 1e-6 (case 46, a demand cut, at
+    # 1.30e-6); so must the engine, in either precision.
     g = np.load(SIMPLEX)
     res = engine.solve_case_stack(stack, tolerance=1e-6, precision=precision)
+    beyond = []
     for k, r in enumerate(res):
         assert r.status == OPTIMAL, (k, r.message)
         ref_obj = float(g["refinery/objective"][k])
-        assert abs(r.objective - ref_obj) <= 1e-6 * max(1.0, abs(ref_obj)), (k, r.objective, ref_obj)
+        rel = abs(r.objective - ref_obj) / max(1.0, abs(ref_obj))
+        assert rel <= 2e-6, (k, r.objective, ref_obj)
+        if rel > 1e-6:
+            beyond.append(k)
+        if precision == 0:
+            # FP64: the reference PDHG's own objective at 1e-6, case by case.
+            pd = float(g["refinery/pdhg_objective"][k])
+            assert abs(r.objective - pd) <= 1e-9 * abs(pd), (k, r.objective, pd)
+    assert len(beyond) <= 1, beyond
 
 
 def _rolling(stack, idx):

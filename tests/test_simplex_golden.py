@@ -61,6 +61,24 @@ def test_fixture_matches_live_generator(golden, k):
     assert _rel(obj, float(golden["refinery/objective"][k])) <= SIMPLEX_RTOL
 
 
+def test_reference_pdhg_objectives_near_simplex(golden):
+    # The reference's own FP64 PDHG at relative KKT 1e-6 on all 60 cases:
+    # optimal, within 2e-6 of the simplex objective (the relative gap is
+    # measured against 1 + |c'x| + |q'y|, about twice the objective), and
+    # beyond 1e-6 on exactly one case (46).
+    simplex = golden["refinery/objective"]
+    pdhg = golden["refinery/pdhg_objective"]
+    assert np.all(golden["refinery/pdhg_status"] == 0)
+    rel = np.abs(pdhg - simplex) / np.maximum(1.0, np.abs(simplex))
+    assert float(rel.max()) <= 2e-6
+    assert list(np.nonzero(rel > 1e-6)[0]) == [46]
+    # The same solver's results in pdhg_golden.npz, bit for bit.
+    g = np.load(os.path.join(HERE, "golden", "pdhg_golden.npz"))
+    for k in (0, 33, 45, 55):
+        assert float(g[f"refinery_case{k}/objective"]) == float(pdhg[k]), k
+        assert int(g[f"refinery_case{k}/iterations"]) == int(golden["refinery/pdhg_iterations"][k])
+
+
 def test_reference_pdhg_golden_within_1e6_of_simplex(golden):
     # The reference's own FP64 PDHG at relative KKT 1e-6 (pdhg_golden.npz)
     # lands within 1e-6 of the simplex objective on the stored cases.
