@@ -53,10 +53,11 @@ sys.path.insert(0, ROOT)
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM = 6650.0
 TOL = 1e-6
-# DRAM bytes (read + write) per fused seg_kernel launch on this workload, mean
-# of the primal and dual kernels, from one cold-cache ncu capture
-# (profiles/seg_kernel_refinery_stack.md): 5.68 MB and 5.27 MB.
-SEG_KERNEL_TRAFFIC = 5.475e6
+# DRAM bytes (read + write) per fused seg_kernel launch of 30 cases (one
+# half of the split stack), mean of the primal and dual kernels, from one
+# cold-cache ncu capture (profiles/seg_kernel_refinery_stack.md): 3.04 MB
+# and 2.84 MB.
+SEG_KERNEL_TRAFFIC = 2.94e6
 
 
 def hbm_peak():
