@@ -710,10 +710,24 @@ struct Workspace {
   DevBuf<StepParams> params;
   DevBuf<double> w_table;
   DevBuf<int32_t> mask;
-  DevBuf<double> partial, terms, kkt, weights;
+  DevBuf<double> partial, partial2, terms, kkt, weights;
   std::map<std::pair<int, int>, cudaGraphExec_t> graphs;
+  // The device work of a termination check and of a re-centring, captured
+  // as graphs once their buffers have settled and replayed at later checks.
+  struct Replay {
+    cudaGraphExec_t exec = nullptr;
+    const double* partial = nullptr;  // reduction scratch the graph was captured with
+    size_t partial_n = 0;
+    const double* partial2 = nullptr;
+    size_t partial2_n = 0;
+    int64_t launches = 0;  // kernels in the graph
+    int seen = 0;
+  };
+  Replay check_replay, recenter_replay;
   ~Workspace() {
     for (auto& g : graphs) cudaGraphExecDestroy(g.second);
+    if (check_replay.exec) cudaGraphExecDestroy(check_replay.exec);
+    if (recenter_replay.exec) cudaGraphExecDestroy(recenter_replay.exec);
   }
 };
 
@@ -1267,6 +1281,29 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
                   "chunk_kernel: a grid barrier wait gave up (the grid was not co-resident)");
   };
 
+  // A polishing sub-stack, started from its parent's step sizes.
+  const bool sub_run = init_eta != nullptr;
+
+  // A refined check's products and reductions in two concurrent branches:
+  // the row side on the engine stream, the column side (and the Farkas
+  // product) on a second stream, joined before the terms are read back.
+  // Each check kernel is latency-bound, so the branches overlap.
+  struct CheckFork {
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork = nullptr, xcomb = nullptr, ycomb = nullptr, join = nullptr;
+    ~CheckFork() {
+      if (side) cudaStreamSynchronize(side);
+      for (cudaEvent_t e : {fork, xcomb, ycomb, join})
+        if (e) cudaEventDestroy(e);
+      if (side) cudaStreamDestroy(side);
+    }
+  } fk;
+  const bool fork_checks = refine && !sub_run && !slow;
+  if (fork_checks) {
+    ANU_CUDA(cudaStreamCreateWithFlags(&fk.side, cudaStreamNonBlocking));
+    for (cudaEvent_t* e : {&fk.fork, &fk.xcomb, &fk.ycomb, &fk.join})
+      ANU_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+  }
   auto run_chunk_body = [&](int len, bool check_at_end) {
     const uint32_t base_flags = averaging ? kAccumulate : 0u;
     if (persistent) {
@@ -1355,6 +1392,38 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
     const double* ktdy = o.detect_infeasibility ? w.ktdy64.p : nullptr;
     const double* los = o.detect_infeasibility ? w.los.p : nullptr;
     const double* his = o.detect_infeasibility ? w.his.p : nullptr;
+    if (refine && fork_checks) {
+      // The judged point is base + offset, in FP64.
+      const int64_t tn = static_cast<int64_t>(n) * K, tm = static_cast<int64_t>(m) * K;
+      RowCheckTerms<double, T, double> rt{K, p.num_eq, w.kx64.p, w.y_comb.p, yv, w.dy.p,
+                                          w.y_restart.p, yprev, w.q0.p, qsc, rs};
+      ColCheckTerms<double, T> ct{K, w.kty64.p, w.x_comb.p, xv, w.dx.p, w.x_restart.p, xprev,
+                                  w.c0.p, w.lo0.p, w.hi0.p, cs, ktdy, los, his};
+      Exec side;
+      side.stream = fk.side;
+      ANU_CUDA(cudaEventRecord(fk.fork, st));
+      ANU_CUDA(cudaStreamWaitEvent(fk.side, fk.fork, 0));
+      // Column side: y~ = yb + y, K'y~ and K'dy; its terms also need x~.
+      combine_kernel<T><<<grid_for(tm, 256, 1184), 256, 0, fk.side>>>(tm, w.yb.p, yv, w.y_comb.p);
+      ANU_CUDA(cudaGetLastError());
+      ANU_CUDA(cudaEventRecord(fk.ycomb, fk.side));
+      product<double, double, double>(side, p.dkt, w.y_comb.p, K, StoreEpi<double>{K, w.kty64.p});
+      if (o.detect_infeasibility)
+        product<double, T, double>(side, p.dkt, w.dy.p, K, StoreEpi<double>{K, w.ktdy64.p});
+      // Row side: x~ = xb + x and K x~; its terms also need y~.
+      combine_kernel<T><<<grid_for(tn, 256, 1184), 256, 0, st>>>(tn, w.xb.p, xv, w.x_comb.p);
+      ANU_CUDA(cudaGetLastError());
+      ANU_CUDA(cudaEventRecord(fk.xcomb, st));
+      product<double, double, double>(p, p.dk, w.x_comb.p, K, StoreEpi<double>{K, w.kx64.p});
+      ANU_CUDA(cudaStreamWaitEvent(fk.side, fk.xcomb, 0));
+      reduce_terms(side, n, K, ct, w.partial2, out_dev, kCheckTerms, kRowTerms);
+      ANU_CUDA(cudaEventRecord(fk.join, fk.side));
+      ANU_CUDA(cudaStreamWaitEvent(st, fk.ycomb, 0));
+      reduce_terms(p, m, K, rt, w.partial, out_dev, kCheckTerms, 0);
+      ANU_CUDA(cudaStreamWaitEvent(st, fk.join, 0));
+      p.launches += side.launches + 2;
+      return;
+    }
     if (o.detect_infeasibility)
       product<double, T, double>(p, p.dkt, w.dy.p, K, StoreEpi<double>{K, w.ktdy64.p});
     if (refine) {
@@ -1388,6 +1457,47 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
     ColCheckTerms<T, T> ct{K, w.kty64.p, xv, xv, w.dx.p, w.x_restart.p, xprev, w.c0.p, w.lo0.p,
                            w.hi0.p, cs, ktdy, los, his};
     reduce_terms(p, n, K, ct, w.partial, out_dev, kCheckTerms, kRowTerms);
+  };
+
+  // Runs `body`, device work on the stream over the workspace's fixed
+  // buffers, as a CUDA graph from its second call on: the same kernels with
+  // the same arguments at every check, so one graph launch replaces a dozen
+  // kernel launches. The first call runs directly and sizes the reduction
+  // scratch; a graph whose scratch has since been reallocated is captured
+  // again. Off where the iterate buffers swap (the host-driven path) and in
+  // polishing sub-stacks, whose few checks would not repay the capture.
+  auto replay = [&](typename Workspace<T>::Replay& r, auto&& body) {
+    if (!o.use_graphs || slow || sub_run) {
+      body();
+      return;
+    }
+    if (r.exec && (r.partial != w.partial.p || r.partial_n != w.partial.n ||
+                   r.partial2 != w.partial2.p || r.partial2_n != w.partial2.n)) {
+      cudaGraphExecDestroy(r.exec);
+      r.exec = nullptr;
+    }
+    if (r.exec == nullptr) {
+      if (++r.seen < 2) {
+        body();
+        return;
+      }
+      const int64_t before = p.launches;
+      cudaGraph_t graph = nullptr;
+      ANU_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+      body();
+      ANU_CUDA(cudaStreamEndCapture(st, &graph));
+      const cudaError_t ie = cudaGraphInstantiate(&r.exec, graph, 0);
+      cudaGraphDestroy(graph);
+      ANU_CUDA(ie);
+      r.launches = p.launches - before;
+      p.launches = before;
+      r.partial = w.partial.p;
+      r.partial_n = w.partial.n;
+      r.partial2 = w.partial2.p;
+      r.partial2_n = w.partial2.n;
+    }
+    ANU_CUDA(cudaGraphLaunch(r.exec, st));
+    p.launches += r.launches;
   };
 
   auto set_mask = [&](const std::vector<int32_t>& mk) {
@@ -1430,26 +1540,28 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
     }
     const bool det = o.detect_infeasibility != 0;
     const int64_t tn = static_cast<int64_t>(n) * K, tm = static_cast<int64_t>(m) * K;
-    ANU_CUDA(cudaMemsetAsync(w.x_comb.p, 0, sizeof(double) * NK, st));
-    recenter_columns_kernel<T><<<grid_for(tn, 256, 1184), 256, 0, st>>>(
-        tn, K, w.mask.p, w.l0s.p, w.u0s.p, w.xb.p, w.x.p, w.anchor_x.p, w.x_restart.p,
-        o.pid_primal_weight ? nullptr : w.x_prev.p, averaging ? w.sum_x.p : nullptr,
-        w.sum_weight.p, w.lo.p, w.hi.p, det ? w.los.p : nullptr, det ? w.his.p : nullptr,
-        w.x_comb.p);
-    ANU_CUDA(cudaGetLastError());
-    product<double, double, double>(p, p.dk, w.x_comb.p, K, StoreEpi<double>{K, w.kshift.p});
-    recenter_rows_kernel<T><<<grid_for(tm, 256, 1184), 256, 0, st>>>(
-        tm, K, p.num_eq, w.mask.p, w.yb.p, w.y.p, w.anchor_y.p, w.y_restart.p,
-        o.pid_primal_weight ? nullptr : w.y_prev.p, averaging ? w.sum_y.p : nullptr,
-        w.sum_weight.p, w.ylo.p, w.kx.p, w.anchor_kx.p, w.kshift.p);
-    ANU_CUDA(cudaGetLastError());
-    product<double, double, double>(p, p.dk, w.xb.p, K, StoreEpi<double>{K, w.kx64.p});
-    product<double, double, double>(p, p.dkt, w.yb.p, K, StoreEpi<double>{K, w.kty64.p});
-    correction_data_kernel<T><<<grid_for(tn + tm, 256, 1184), 256, 0, st>>>(
-        tn, tm, K, w.mask.p, w.c0s.p, w.kty64.p, w.c.p, w.q0s.p, w.kx64.p, w.q.p,
-        det ? w.qs.p : nullptr);
-    ANU_CUDA(cudaGetLastError());
-    p.launches += 3;
+    replay(w.recenter_replay, [&]() {
+      ANU_CUDA(cudaMemsetAsync(w.x_comb.p, 0, sizeof(double) * NK, st));
+      recenter_columns_kernel<T><<<grid_for(tn, 256, 1184), 256, 0, st>>>(
+          tn, K, w.mask.p, w.l0s.p, w.u0s.p, w.xb.p, w.x.p, w.anchor_x.p, w.x_restart.p,
+          o.pid_primal_weight ? nullptr : w.x_prev.p, averaging ? w.sum_x.p : nullptr,
+          w.sum_weight.p, w.lo.p, w.hi.p, det ? w.los.p : nullptr, det ? w.his.p : nullptr,
+          w.x_comb.p);
+      ANU_CUDA(cudaGetLastError());
+      product<double, double, double>(p, p.dk, w.x_comb.p, K, StoreEpi<double>{K, w.kshift.p});
+      recenter_rows_kernel<T><<<grid_for(tm, 256, 1184), 256, 0, st>>>(
+          tm, K, p.num_eq, w.mask.p, w.yb.p, w.y.p, w.anchor_y.p, w.y_restart.p,
+          o.pid_primal_weight ? nullptr : w.y_prev.p, averaging ? w.sum_y.p : nullptr,
+          w.sum_weight.p, w.ylo.p, w.kx.p, w.anchor_kx.p, w.kshift.p);
+      ANU_CUDA(cudaGetLastError());
+      product<double, double, double>(p, p.dk, w.xb.p, K, StoreEpi<double>{K, w.kx64.p});
+      product<double, double, double>(p, p.dkt, w.yb.p, K, StoreEpi<double>{K, w.kty64.p});
+      correction_data_kernel<T><<<grid_for(tn + tm, 256, 1184), 256, 0, st>>>(
+          tn, tm, K, w.mask.p, w.c0s.p, w.kty64.p, w.c.p, w.q0s.p, w.kx64.p, w.q.p,
+          det ? w.qs.p : nullptr);
+      ANU_CUDA(cudaGetLastError());
+      p.launches += 3;
+    });
     for (int k = 0; k < K; ++k)
       if (mk[k]) ++R_ptr->at(k).r.refinement_rounds;
   };
@@ -1836,7 +1948,7 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
     bool any_avg = false;
     for (int k = 0; k < K; ++k) any_avg = any_avg || (S[k].active && averaging && S[k].sum_weight > 0.0);
     const bool fresh_kx = !fp64 || !o.reuse_products;
-    check_terms(w.x.p, w.y.p, w.kx.p, fresh_kx, w.terms.p);
+    replay(w.check_replay, [&]() { check_terms(w.x.p, w.y.p, w.kx.p, fresh_kx, w.terms.p); });
     const bool need_kkt = need_kkt_any;
     if (need_kkt) kkt_terms(w.x.p, w.y.p, w.kkt.p);
     if (any_avg) {

@@ -265,6 +265,22 @@ def test_case_stack_objectives_match_simplex(engine, stack, precision):
     assert len(beyond) <= 1, beyond
 
 
+@pytest.mark.parametrize("precision", [0, PRECISION_FP32])
+def test_case_stack_graphs_bit_identical(engine, stack, precision):
+    # Iteration chunks, termination checks and re-centrings replayed as CUDA
+    # graphs run the same kernels on the same buffers as direct launches:
+    # 20 cases (two half-stacks), results identical bit for bit.
+    sub = _rolling(stack, list(range(20)))
+    kw = dict(tolerance=1e-6, precision=precision)
+    graphs = engine.solve_case_stack(sub, use_graphs=1, **kw)
+    direct = engine.solve_case_stack(sub, use_graphs=0, **kw)
+    for k, (a, b) in enumerate(zip(graphs, direct)):
+        assert a.status == b.status == OPTIMAL, (k, a.message)
+        assert a.iterations == b.iterations and a.restarts == b.restarts, k
+        assert np.array_equal(a.x, b.x) and np.array_equal(a.y, b.y), k
+    assert graphs[0].refinement_rounds == direct[0].refinement_rounds
+
+
 def _rolling(stack, idx):
     return lpgen.CaseStack(stack.base, [stack.names[i] for i in idx], stack.c[idx], stack.q[idx],
                            stack.lower[idx], stack.upper[idx])
