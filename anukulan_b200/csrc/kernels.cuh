@@ -39,8 +39,17 @@ constexpr int kBlockNnz = 1024;
 constexpr int kBlockRows = 128;
 // Case-stack product: nonzeros per segment, segments per CTA, rows per CTA,
 // and the most cases one launch carries.
-constexpr int kSegNnz = 16;
-constexpr int kSegPerCta = 8;
+// The segment shape is a build-time choice (-DANU_SEG_NNZ, -DANU_SEG_PER_CTA)
+// so it can be swept; a CTA has one warp per segment at 32 lanes.
+#ifndef ANU_SEG_NNZ
+#define ANU_SEG_NNZ 16
+#endif
+#ifndef ANU_SEG_PER_CTA
+#define ANU_SEG_PER_CTA 8
+#endif
+constexpr int kSegNnz = ANU_SEG_NNZ;
+constexpr int kSegPerCta = ANU_SEG_PER_CTA;
+constexpr int kSegThreads = 32 * kSegPerCta;
 constexpr int kSegRows = 64;
 constexpr int kMaxCaseLanes = 64;
 
@@ -442,9 +451,9 @@ __global__ void __launch_bounds__(kRowThreads)
 // epilogue runs over (row, case) pairs of the CTA - case-contiguous, so its
 // vector traffic is coalesced.
 template <class V, class X, class Acc, class Epi, int L, int CPL>
-__global__ void __launch_bounds__(kThreads) seg_kernel(CsrView<V> a, const X* __restrict__ x,
+__global__ void __launch_bounds__(kSegThreads) seg_kernel(CsrView<V> a, const X* __restrict__ x,
                                                         int32_t K, Epi epi) {
-  constexpr int kGroups = kThreads / L;  // >= kSegPerCta: one segment per group
+  constexpr int kGroups = kSegThreads / L;  // >= kSegPerCta: one segment per group
   constexpr int kPrefetch = 2;           // epilogue items prefetched per thread
   static_assert(kGroups >= kSegPerCta, "one segment per lane group");
   __shared__ Acc part[kSegPerCta][kMaxCaseLanes];
@@ -472,7 +481,7 @@ __global__ void __launch_bounds__(kThreads) seg_kernel(CsrView<V> a, const X* __
   typename Epi::Pre pre[kPrefetch];
 #pragma unroll
   for (int q = 0; q < kPrefetch; ++q) {
-    const int32_t t = threadIdx.x + q * kThreads;
+    const int32_t t = threadIdx.x + q * kSegThreads;
     if (t < items) pre[q] = epi.prefetch(r0 + t / K, t % K);
   }
   // ---- the gather reads the previous launch's output.
@@ -513,7 +522,7 @@ __global__ void __launch_bounds__(kThreads) seg_kernel(CsrView<V> a, const X* __
     for (int c = 0; c < CPL; ++c) part[sg - s0][lane + c * L] = acc[c];
   }
   __syncthreads();
-  for (int32_t t = threadIdx.x, q = 0; t < items; t += kThreads, ++q) {
+  for (int32_t t = threadIdx.x, q = 0; t < items; t += kSegThreads, ++q) {
     const int32_t row = r0 + t / K;
     const int32_t k = t % K;
     Acc sum = 0;
@@ -654,7 +663,7 @@ __device__ __forceinline__ void chunk_prefetch(const SegSlice<V>& s, int32_t K, 
   const int32_t items = (s.r1 - s.r0) * K;
 #pragma unroll
   for (int q = 0; q < kChunkPrefetch; ++q) {
-    const int32_t t = threadIdx.x + q * kThreads;
+    const int32_t t = threadIdx.x + q * kSegThreads;
     if (t < items) pre[q] = epi.prefetch(s.r0 + t / K, t % K);
   }
 }
@@ -701,7 +710,7 @@ __device__ __forceinline__ void chunk_phase(const CsrView<V>& a, const SegSlice<
   }
   __syncthreads();
   const int32_t items = (s.r1 - s.r0) * K;
-  for (int32_t t = threadIdx.x, q = 0; t < items; t += kThreads, ++q) {
+  for (int32_t t = threadIdx.x, q = 0; t < items; t += kSegThreads, ++q) {
     const int32_t row = s.r0 + t / K;
     const int32_t k = t % K;
     V sum = 0;
@@ -723,11 +732,11 @@ __device__ __forceinline__ void chunk_phase(const CsrView<V>& a, const SegSlice<
 // products (the dual iterate and the primal extrapolation). The last
 // iteration runs with `last_flags`, the others with `flags`.
 template <class T, int CPL>
-__global__ void __launch_bounds__(kThreads, kChunkCtasPerSm)
+__global__ void __launch_bounds__(kSegThreads, kChunkCtasPerSm)
     chunk_kernel(CsrView<T> kt, CsrView<T> k, const T* y, const T* x_bar, int32_t K, int32_t len,
                  uint32_t flags, uint32_t last_flags, PrimalEpi<T> pe, DualEpi<T> de,
                  GridSync sync) {
-  static_assert(kSegNnz <= 32 && kThreads / 32 >= kSegPerCta, "one warp per segment");
+  static_assert(kSegNnz <= 32 && kSegThreads / 32 >= kSegPerCta, "one warp per segment");
   __shared__ T part[kSegPerCta][kMaxCaseLanes];
   __shared__ int ok_flag;
   SegSlice<T> sa, sb;

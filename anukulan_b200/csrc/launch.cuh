@@ -50,7 +50,7 @@ void product(Exec& p, const Mat& a, const X* x, int K, const Epi& epi, bool pdl 
   do {                                                                                   \
     cudaLaunchConfig_t cfg = {};                                                         \
     cfg.gridDim = dim3(a.num_ctas);                                                      \
-    cfg.blockDim = dim3(kThreads);                                                       \
+    cfg.blockDim = dim3(kSegThreads);                                                    \
     cfg.stream = s;                                                                      \
     cudaLaunchAttribute attr[1];                                                         \
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;                     \
@@ -80,7 +80,7 @@ int chunk_capacity() {
   cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev),
              "cudaDeviceGetAttribute");
   cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, chunk_kernel<T, CPL>,
-                                                           kThreads, 0),
+                                                           kSegThreads, 0),
              "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
   return sms * per_sm;
 }
@@ -105,7 +105,7 @@ void launch_chunk(Exec& p, const Mat& kt, const Mat& k, const T* y, const T* x_b
                   const DualEpi<T>& de, GridSync sync) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(kt.num_ctas > k.num_ctas ? kt.num_ctas : k.num_ctas);
-  cfg.blockDim = dim3(kThreads);
+  cfg.blockDim = dim3(kSegThreads);
   cfg.stream = p.stream;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeCooperative;
