@@ -1213,7 +1213,10 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
   if (o.restarts && !o.restart_on_fixed_point) {
     // pdhg.cpp:604 - the KKT error at the starting point.
     kkt_terms(w.x.p, w.y.p, w.kkt.p);
-    ANU_CUDA(cudaMemcpy(h_kkt.p, w.kkt.p, sizeof(double) * kKktTerms * K, cudaMemcpyDeviceToHost));
+    // On the engine stream: a plain cudaMemcpy would not wait for it.
+    ANU_CUDA(cudaMemcpyAsync(h_kkt.p, w.kkt.p, sizeof(double) * kKktTerms * K,
+                             cudaMemcpyDeviceToHost, st));
+    ANU_CUDA(cudaStreamSynchronize(st));
     for (int k = 0; k < K; ++k) S[k].kkt_at_restart = kkt_value(&h_kkt.p[k * kKktTerms], S[k].omega);
   }
 
@@ -1298,7 +1301,7 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
       if (side) cudaStreamDestroy(side);
     }
   } fk;
-  const bool fork_checks = refine && !sub_run && !slow;
+  const bool fork_checks = refine && !sub_run && !slow && K > 1;
   if (fork_checks) {
     ANU_CUDA(cudaStreamCreateWithFlags(&fk.side, cudaStreamNonBlocking));
     for (cudaEvent_t* e : {&fk.fork, &fk.xcomb, &fk.ycomb, &fk.join})
@@ -1464,10 +1467,12 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
   // the same arguments at every check, so one graph launch replaces a dozen
   // kernel launches. The first call runs directly and sizes the reduction
   // scratch; a graph whose scratch has since been reallocated is captured
-  // again. Off where the iterate buffers swap (the host-driven path) and in
-  // polishing sub-stacks, whose few checks would not repay the capture.
+  // again. Only for case stacks: not where the iterate buffers swap (the
+  // host-driven path), not in polishing sub-stacks, whose few checks would
+  // not repay the capture, and not for a single LP, which packed batches run
+  // by the hundred from many host threads at once.
   auto replay = [&](typename Workspace<T>::Replay& r, auto&& body) {
-    if (!o.use_graphs || slow || sub_run) {
+    if (!o.use_graphs || slow || sub_run || K == 1) {
       body();
       return;
     }
@@ -1809,7 +1814,9 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
     masked_copy<T, double>(p, m, K, w.mask.p, w.kx64.p, w.kx.p);
     if (o.restarts && !o.restart_on_fixed_point) {
       kkt_terms(w.x.p, w.y.p, w.kkt.p);
-      ANU_CUDA(cudaMemcpy(h_kkt.p, w.kkt.p, sizeof(double) * kKktTerms * K, cudaMemcpyDeviceToHost));
+      ANU_CUDA(cudaMemcpyAsync(h_kkt.p, w.kkt.p, sizeof(double) * kKktTerms * K,
+                               cudaMemcpyDeviceToHost, st));
+      ANU_CUDA(cudaStreamSynchronize(st));
       S[k].kkt_at_restart = kkt_value(&h_kkt.p[static_cast<size_t>(k) * kKktTerms], S[k].omega);
     }
     // The staged host columns stay alive until the copies are done.
