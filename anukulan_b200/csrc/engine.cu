@@ -54,7 +54,10 @@ void cuda_check(cudaError_t status, const char* what) {
 
 // ------------------------------------------------------------ matrices
 
-void DevCsr::upload(const HostCsr& a, bool with_fp32, cudaStream_t s) {
+void DevCsr::upload(const HostCsr& a, bool with_fp32, cudaStream_t s, int32_t seg_nnz,
+                    int32_t seg_per) {
+  if (seg_nnz < 1 || seg_per < 1 || seg_per > kSegPerCtaMax)
+    throw Error(ANU_ERR_INTERNAL, "segment shape out of range");
   rows = a.rows;
   cols = a.cols;
   nnz = a.nnz();
@@ -86,7 +89,8 @@ void DevCsr::upload(const HostCsr& a, bool with_fp32, cudaStream_t s) {
   if (!bd.empty())
     ANU_CUDA(cudaMemcpyAsync(blocks.p, bd.data(), sizeof(RowBlockDev) * bd.size(),
                              cudaMemcpyHostToDevice, s));
-  const SegmentSchedule sch = segment_schedule(a, kSegNnz, kSegPerCta, kSegRows);
+  const SegmentSchedule sch = segment_schedule(a, seg_nnz, seg_per, kSegRows);
+  seg_per_cta = seg_per;
   num_ctas = static_cast<int32_t>(sch.cta_row.size()) - 1;
   auto put = [&](DevBuf<int32_t>& d, const std::vector<int32_t>& h) {
     d.alloc(std::max<size_t>(h.size(), 1));
@@ -103,12 +107,12 @@ void DevCsr::upload(const HostCsr& a, bool with_fp32, cudaStream_t s) {
 template <>
 CsrView<double> DevCsr::view<double>() const {
   return {rows, cols, start.p, index.p, v64.p, blocks.p, num_blocks,
-          seg_begin.p, row_seg.p, cta_row.p, cta_seg.p, num_ctas};
+          seg_begin.p, row_seg.p, cta_row.p, cta_seg.p, num_ctas, seg_per_cta};
 }
 template <>
 CsrView<float> DevCsr::view<float>() const {
   return {rows, cols, start.p, index.p, v32.p, blocks.p, num_blocks,
-          seg_begin.p, row_seg.p, cta_row.p, cta_seg.p, num_ctas};
+          seg_begin.p, row_seg.p, cta_row.p, cta_seg.p, num_ctas, seg_per_cta};
 }
 
 Problem::~Problem() {
@@ -409,7 +413,8 @@ void validate_options(const anu_pdhg_options& o) {
 // -------------------------------------------------------------- setup
 
 std::unique_ptr<Problem> make_problem(const anu_lp& lp, const anu_pdhg_options& o,
-                                      double* scaling_seconds, double* norm_seconds) {
+                                      double* scaling_seconds, double* norm_seconds,
+                                      int32_t seg_nnz, int32_t seg_per_cta) {
   int count = 0;
   const cudaError_t ce = cudaGetDeviceCount(&count);
   if (ce != cudaSuccess || count == 0)
@@ -433,8 +438,10 @@ std::unique_ptr<Problem> make_problem(const anu_lp& lp, const anu_pdhg_options& 
   p->kt = transpose(p->k);
   if (scaling_seconds) *scaling_seconds = now_seconds() - t0;
   const bool fp32 = o.precision == ANU_PRECISION_FP32;
-  p->dk.upload(p->k, fp32, p->stream);
-  p->dkt.upload(p->kt, fp32, p->stream);
+  p->seg_nnz = seg_nnz;
+  p->seg_per_cta = seg_per_cta;
+  p->dk.upload(p->k, fp32, p->stream, seg_nnz, seg_per_cta);
+  p->dkt.upload(p->kt, fp32, p->stream, seg_nnz, seg_per_cta);
   p->row_scale.alloc(std::max(p->m, 1));
   p->col_scale.alloc(std::max(p->n, 1));
   if (p->m > 0)
@@ -477,8 +484,10 @@ std::unique_ptr<Problem> clone_problem(const Problem& src) {
   p->unit_scaling = src.unit_scaling;
   p->matrix_norm = src.matrix_norm;
   const bool fp32 = p->precision == ANU_PRECISION_FP32;
-  p->dk.upload(p->k, fp32, p->stream);
-  p->dkt.upload(p->kt, fp32, p->stream);
+  p->seg_nnz = src.seg_nnz;
+  p->seg_per_cta = src.seg_per_cta;
+  p->dk.upload(p->k, fp32, p->stream, p->seg_nnz, p->seg_per_cta);
+  p->dkt.upload(p->kt, fp32, p->stream, p->seg_nnz, p->seg_per_cta);
   p->row_scale.alloc(std::max(p->m, 1));
   p->col_scale.alloc(std::max(p->n, 1));
   if (p->m > 0)

@@ -158,7 +158,11 @@ struct DevCsr {
   int32_t num_blocks = 0;
   DevBuf<int32_t> seg_begin, row_seg, cta_row, cta_seg;
   int32_t num_ctas = 0;
-  void upload(const HostCsr& a, bool with_fp32, cudaStream_t s);
+  int32_t seg_per_cta = kSegPerCta;
+  // seg_nnz, seg_per_cta: the segment schedule's shape (at most
+  // kSegPerCtaMax segments per CTA).
+  void upload(const HostCsr& a, bool with_fp32, cudaStream_t s, int32_t seg_nnz = kSegNnz,
+              int32_t seg_per_cta = kSegPerCta);
   template <class V>
   CsrView<V> view() const;
 };
@@ -179,6 +183,7 @@ struct Problem : Exec {
   double matrix_norm = 0.0;
   bool owns_stream = false;
   int device = 0;
+  int32_t seg_nnz = kSegNnz, seg_per_cta = kSegPerCta;  // segment schedule shape
   ~Problem();
 };
 
@@ -202,8 +207,10 @@ struct CaseResult {
 
 // Builds the problem from a validated LP: copies, scales, uploads, and
 // estimates ||K~|| unless known_matrix_norm is given.
+// seg_nnz, seg_per_cta: the shape of the case-stack segment schedule.
 std::unique_ptr<Problem> make_problem(const anu_lp& lp, const anu_pdhg_options& o,
-                                      double* scaling_seconds, double* norm_seconds);
+                                      double* scaling_seconds, double* norm_seconds,
+                                      int32_t seg_nnz = kSegNnz, int32_t seg_per_cta = kSegPerCta);
 // A second problem on its own stream and memory pool with the same scaled
 // matrix (host and device copies), scaling and norm, made without scaling or
 // power iteration again.

@@ -53,6 +53,10 @@ constexpr int kBlockRows = 128;
 constexpr int kSegNnz = ANU_SEG_NNZ;
 constexpr int kSegPerCta = ANU_SEG_PER_CTA;
 constexpr int kSegThreads = 32 * kSegPerCta;
+// A matrix may carry another segment shape (the unrolled adjoint's does);
+// seg_kernel takes it from the schedule, up to this many segments per CTA.
+constexpr int kSegPerCtaMax = 16;
+static_assert(kSegPerCta <= kSegPerCtaMax, "segment shape");
 constexpr int kSegRows = 64;
 constexpr int kMaxCaseLanes = 64;
 
@@ -101,12 +105,14 @@ struct CsrView {
   // Segment schedule of the case-stack product: every row cut into
   // segments of at most a few nonzeros (seg_begin, in nonzero order; the
   // segments of row r are row_seg[r] .. row_seg[r+1]-1), and consecutive rows
-  // grouped so a CTA holds at most kSegPerCta segments (cta_row, cta_seg).
+  // grouped so a CTA holds at most seg_per_cta segments (cta_row, cta_seg).
+  // seg_kernel runs 32 * seg_per_cta threads per CTA.
   const int32_t* __restrict__ seg_begin;
   const int32_t* __restrict__ row_seg;
   const int32_t* __restrict__ cta_row;
   const int32_t* __restrict__ cta_seg;
   int32_t num_ctas;
+  int32_t seg_per_cta;
 };
 
 // ------------------------------------------------------- per-case state
@@ -453,13 +459,18 @@ __global__ void __launch_bounds__(kRowThreads)
 // memory and are added per row in segment order (deterministic), and the
 // epilogue runs over (row, case) pairs of the CTA - case-contiguous, so its
 // vector traffic is coalesced.
-template <class V, class X, class Acc, class Epi, int L, int CPL>
-__global__ void __launch_bounds__(kSegThreads) seg_kernel(CsrView<V> a, const X* __restrict__ x,
-                                                        int32_t K, Epi epi) {
-  constexpr int kGroups = kSegThreads / L;  // >= kSegPerCta: one segment per group
-  constexpr int kPrefetch = 2;           // epilogue items prefetched per thread
-  static_assert(kGroups >= kSegPerCta, "one segment per lane group");
-  __shared__ Acc part[kSegPerCta][kMaxCaseLanes];
+//
+// A CTA has 32 * a.seg_per_cta threads (at most kMaxThreads, the bound the
+// instantiation is compiled for), so at least one lane group per segment at
+// any L; the segment partials live in dynamic shared memory (seg_per_cta x
+// kMaxCaseLanes values).
+template <class V, class X, class Acc, class Epi, int L, int CPL, int kMaxThreads>
+__global__ void __launch_bounds__(kMaxThreads)
+    seg_kernel(CsrView<V> a, const X* __restrict__ x, int32_t K, Epi epi) {
+  constexpr int kPrefetch = 2;  // epilogue items prefetched per thread
+  extern __shared__ __align__(16) unsigned char seg_smem[];
+  Acc* part = reinterpret_cast<Acc*>(seg_smem);
+  const int32_t threads = static_cast<int32_t>(blockDim.x);
   const int32_t cta = blockIdx.x;
   const int32_t r0 = a.cta_row[cta];
   const int32_t r1 = a.cta_row[cta + 1];
@@ -484,7 +495,7 @@ __global__ void __launch_bounds__(kSegThreads) seg_kernel(CsrView<V> a, const X*
   typename Epi::Pre pre[kPrefetch];
 #pragma unroll
   for (int q = 0; q < kPrefetch; ++q) {
-    const int32_t t = threadIdx.x + q * kSegThreads;
+    const int32_t t = threadIdx.x + q * threads;
     if (t < items) pre[q] = epi.prefetch(r0 + t / K, t % K);
   }
   // ---- the gather reads the previous launch's output.
@@ -522,14 +533,15 @@ __global__ void __launch_bounds__(kSegThreads) seg_kernel(CsrView<V> a, const X*
   }
   if (active) {
 #pragma unroll
-    for (int c = 0; c < CPL; ++c) part[sg - s0][lane + c * L] = acc[c];
+    for (int c = 0; c < CPL; ++c) part[(sg - s0) * kMaxCaseLanes + lane + c * L] = acc[c];
   }
   __syncthreads();
-  for (int32_t t = threadIdx.x, q = 0; t < items; t += kSegThreads, ++q) {
+  for (int32_t t = threadIdx.x, q = 0; t < items; t += threads, ++q) {
     const int32_t row = r0 + t / K;
     const int32_t k = t % K;
     Acc sum = 0;
-    for (int32_t g = a.row_seg[row]; g < a.row_seg[row + 1]; ++g) sum = add(sum, part[g - s0][k]);
+    for (int32_t g = a.row_seg[row]; g < a.row_seg[row + 1]; ++g)
+      sum = add(sum, part[(g - s0) * kMaxCaseLanes + k]);
     if (q < kPrefetch) {
       typename Epi::Pre r;
 #pragma unroll

@@ -50,15 +50,19 @@ void product(Exec& p, const Mat& a, const X* x, int K, const Epi& epi, bool pdl 
   do {                                                                                   \
     cudaLaunchConfig_t cfg = {};                                                         \
     cfg.gridDim = dim3(a.num_ctas);                                                      \
-    cfg.blockDim = dim3(kSegThreads);                                                    \
+    cfg.blockDim = dim3(32 * a.seg_per_cta);                                             \
+    cfg.dynamicSmemBytes = sizeof(Acc) * a.seg_per_cta * kMaxCaseLanes;                  \
     cfg.stream = s;                                                                      \
     cudaLaunchAttribute attr[1];                                                         \
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;                     \
     attr[0].val.programmaticStreamSerializationAllowed = 1;                              \
     cfg.attrs = attr;                                                                    \
     cfg.numAttrs = pdl ? 1 : 0;                                                          \
-    cuda_check(cudaLaunchKernelEx(&cfg, seg_kernel<V, X, Acc, Epi, L_, CPL_>,            \
-                                  a.template view<V>(), x, K, epi),                      \
+    /* The default shape has its own instantiation, compiled for its CTA size. */     \
+    auto kernel = a.seg_per_cta <= kSegPerCta                                            \
+                      ? seg_kernel<V, X, Acc, Epi, L_, CPL_, kSegThreads>                \
+                      : seg_kernel<V, X, Acc, Epi, L_, CPL_, 32 * kSegPerCtaMax>;        \
+    cuda_check(cudaLaunchKernelEx(&cfg, kernel, a.template view<V>(), x, K, epi),        \
                "seg_kernel launch");                                                     \
   } while (0)
     if (K <= 4) ANU_CASES(4, 1);
@@ -92,6 +96,8 @@ template <class T, class Mat>
 bool chunk_fits(const Mat& kt, const Mat& k, int K) {
   if (K < 17 || K > 2 * 32) return false;
   if (kt.rows == 0 || k.rows == 0) return false;
+  // The chunk kernel is built for the default segment shape.
+  if (kt.seg_per_cta != kSegPerCta || k.seg_per_cta != kSegPerCta) return false;
   const int grid = kt.num_ctas > k.num_ctas ? kt.num_ctas : k.num_ctas;
   const int cap = K <= 32 ? chunk_capacity<T, 1>() : chunk_capacity<T, 2>();
   return grid >= 1 && grid <= cap;
