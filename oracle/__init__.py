@@ -7,6 +7,10 @@
 * :func:`ref_lib` - ``_ref/libanuref.so``, the reference's own sources compiled
   by oracle/Makefile, present where the reference tree was available at build
   time (the built file travels with the working tree).
+* :func:`ref_b200_lib` - ``_ref/libanuref_b200.so``, the reference's solver
+  with its CUDA backend replaced by the adapter over the engine; with it the
+  reference's own ``test_backend`` and ``test_pdhg`` binaries
+  (``_ref/test_*_b200``), built from its unmodified test sources.
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
 this package. The engine never does.
@@ -29,11 +33,15 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libanuref.so")
 REF_CUDA_SO = os.path.join(HERE, "_ref", "libanuref_cuda.so")
+REF_B200_SO = os.path.join(HERE, "_ref", "libanuref_b200.so")
+REF_B200_TEST_BACKEND = os.path.join(HERE, "_ref", "test_backend_b200")
+REF_B200_TEST_PDHG = os.path.join(HERE, "_ref", "test_pdhg_b200")
 REF_SRC = "/root/reference/src/anukulan/pdhg.cpp"
 
 _oracle = None
 _ref = None
 _ref_cuda = None
+_ref_b200 = None
 
 _P = C.POINTER
 
@@ -46,7 +54,7 @@ def build(with_reference: Optional[bool] = None) -> None:
     if with_reference is None:
         with_reference = os.path.exists(REF_SRC)
     if with_reference:
-        subprocess.run(["make", "-s", "-j8", "-C", HERE, "ref", "ref_cuda"], check=True)
+        subprocess.run(["make", "-s", "-j8", "-C", HERE, "ref", "ref_cuda", "ref_b200"], check=True)
 
 
 def _declare(lib, name, restype, argtypes):
@@ -150,19 +158,54 @@ def ref_cuda_lib():
     return _ref_cuda
 
 
-def ref_cuda_solve(lp: StandardLp, options=None, **kw) -> PdhgResult:
+def ref_cuda_solve(lp: StandardLp, options=None, lib=None, **kw) -> PdhgResult:
     """The reference's own solve_pdhg on its CUDA backend (cuda_backend.cu,
-    FP64, one LP per call)."""
+    FP64, one LP per call), or on whatever `lib`'s cuda_backend() is."""
     cl = CLp(lp)
     o = _opts(options, **kw)
     x = np.zeros(cl.n)
     y = np.zeros(cl.m)
     r = anu_pdhg_result()
-    rc = ref_cuda_lib().ref_pdhg_solve(cl.ref(), C.byref(o), -2, None, None, f64_ptr(x),
-                                       f64_ptr(y), C.byref(r))
+    lib = lib if lib is not None else ref_cuda_lib()
+    rc = lib.ref_pdhg_solve(cl.ref(), C.byref(o), -2, None, None, f64_ptr(x),
+                            f64_ptr(y), C.byref(r))
     if rc != 0:
         raise RuntimeError(r.message.decode())
     return PdhgResult.from_c(r, x, y)
+
+
+def have_reference_b200() -> bool:
+    return all(os.path.exists(p) for p in (REF_B200_SO, REF_B200_TEST_BACKEND,
+                                            REF_B200_TEST_PDHG))
+
+
+def ref_b200_lib():
+    """_ref/libanuref_b200.so: the reference's unmodified solver with
+    anukulan::cuda_backend() resolved to the LinAlgBackend adapter over the
+    engine (include/anu_b200_backend.hpp). It loads the engine library."""
+    global _ref_b200
+    if _ref_b200 is None:
+        if not os.path.exists(REF_B200_SO):
+            raise FileNotFoundError("oracle/_ref/libanuref_b200.so is not built")
+        lib = C.CDLL(REF_B200_SO)
+        _declare(lib, "ref_pdhg_solve", C.c_int,
+                 [C.c_void_p, _P(anu_pdhg_options), C.c_int, _P(C.c_double),
+                  _P(C.c_double), _P(C.c_double), _P(C.c_double), _P(anu_pdhg_result)])
+        _declare(lib, "ref_default_backend_name", C.c_int, [C.c_char_p, C.c_int])
+        _ref_b200 = lib
+    return _ref_b200
+
+
+def ref_b200_backend_name() -> str:
+    buf = C.create_string_buffer(64)
+    ref_b200_lib().ref_default_backend_name(buf, 64)
+    return buf.value.decode()
+
+
+def ref_b200_solve(lp: StandardLp, options=None, **kw) -> PdhgResult:
+    """The reference's own solve_pdhg, unchanged, with the engine's kernels
+    under its LinAlgBackend seam (FP64, one seam call per launch)."""
+    return ref_cuda_solve(lp, options, lib=ref_b200_lib(), **kw)
 
 
 def ref_solve(lp: StandardLp, options=None, threads: int = 1, warm_x=None, warm_y=None,

@@ -259,6 +259,15 @@ int ref_simplex_solve(const anu_lp* lp_in, double time_limit, double* x, double*
 
 int ref_default_thread_count(void) { return anukulan::default_thread_count(); }
 
+// LinAlgBackend::name() of the backend solve_pdhg gets when it names none
+// (default_backend(), backend.cpp:209-221): "cpu" without a device, "cuda"
+// in the reference's own CUDA build, "b200" where cuda_backend() is the
+// adapter over the engine. Returns the length written.
+int ref_default_backend_name(char* buf, int size) {
+  const std::string name = anukulan::default_backend().name();
+  return std::snprintf(buf, static_cast<std::size_t>(size), "%s", name.c_str());
+}
+
 // PdhgOptions{} (src/anukulan/pdhg.hpp:19-415) written into the engine's
 // options struct, so the tests can check both carry the same defaults.
 void ref_default_options(anu_pdhg_options* o) {

@@ -4,6 +4,7 @@ library loads and exports every symbol its header declares."""
 import ctypes as C
 import os
 import re
+import subprocess
 
 import numpy as np
 import pytest
@@ -168,3 +169,20 @@ def test_struct_layout_roundtrip():
     # with a field-by-field sum plus natural alignment.
     assert C.sizeof(abi.anu_pdhg_residual) == 12 * 8
     assert C.sizeof(abi.anu_pdhg_phases) == 6 * 8
+
+
+@pytest.mark.skipif(not oracle.have_reference_b200(), reason="adapter build absent")
+def test_reference_adapter_without_device_falls_back_and_fails_loudly():
+    """Built with the adapter as anukulan::cuda_backend(), the reference keeps
+    its own no-device behaviour: default_backend() is the CPU reference
+    (backend.cpp:209-221), and asking for the device backend raises."""
+    from anukulan_b200 import pdhg
+    if pdhg.device_count() > 0:
+        pytest.skip("a device is present")
+    assert oracle.ref_b200_backend_name() == "cpu"
+    lp = lp_cases.standard(lp_cases.wyndor())
+    with pytest.raises(RuntimeError, match="no CUDA device"):
+        oracle.ref_b200_solve(lp, tolerance=1e-6)
+    for path in (oracle.REF_B200_TEST_BACKEND, oracle.REF_B200_TEST_PDHG):
+        p = subprocess.run([path], capture_output=True, text=True, timeout=300)
+        assert p.returncode == 0, p.stdout + p.stderr
