@@ -16,6 +16,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <numeric>
 #include <thread>
 #include <utility>
 
@@ -345,10 +346,18 @@ double device_matrix_norm(Problem& p, int iterations, double tolerance) {
   if (n == 0 || m == 0 || p.dk.nnz == 0) return 0.0;
   // Deterministic non-uniform start, normalised on the host exactly as the
   // reference does (pdhg.cpp:233-238).
+  // A relabelled problem starts from the same vector, entry for entry, so
+  // the sum runs over the original order.
   std::vector<double> v(n);
-  for (int32_t j = 0; j < n; ++j) v[j] = 1.0 + 0.1 * static_cast<double>(j % 7);
   double ss = 0.0;
-  for (double a : v) ss += a * a;
+  for (int32_t j = 0; j < n; ++j) {
+    const double a = 1.0 + 0.1 * static_cast<double>(j % 7);
+    ss += a * a;
+  }
+  for (int32_t j = 0; j < n; ++j) {
+    const int32_t orig = p.col_old.empty() ? j : p.col_old[j];
+    v[j] = 1.0 + 0.1 * static_cast<double>(orig % 7);
+  }
   const double norm = std::sqrt(ss);
   if (norm == 0.0) return 0.0;
   for (double& a : v) a /= norm;
@@ -410,11 +419,92 @@ void validate_options(const anu_pdhg_options& o) {
   if (o.termination < 0 || o.termination > 2) throw Error(ANU_ERR_INVALID, "unknown termination");
 }
 
+// ------------------------------------------------ locality relabelling
+
+Relabel locality_relabel(const anu_lp& lp) {
+  const int32_t m = lp.k.rows, n = lp.k.cols, ne = lp.num_equalities;
+  Relabel r;
+  if (m == 0 || n == 0) return r;
+  const int32_t* start = lp.k.start;
+  r.row_old.resize(m);
+  std::iota(r.row_old.begin(), r.row_old.end(), 0);
+  const auto longer = [start](int32_t a, int32_t b) {
+    return start[a + 1] - start[a] > start[b + 1] - start[b];
+  };
+  std::stable_sort(r.row_old.begin(), r.row_old.begin() + ne, longer);
+  std::stable_sort(r.row_old.begin() + ne, r.row_old.end(), longer);
+  r.row_new.resize(m);
+  for (int32_t i = 0; i < m; ++i) r.row_new[r.row_old[i]] = i;
+  // A column's key is the first relabelled row it appears in (m if none).
+  std::vector<int32_t> key(n, m);
+  for (int32_t i = 0; i < m; ++i)
+    for (int32_t e = start[i]; e < start[i + 1]; ++e) {
+      int32_t& k = key[lp.k.index[e]];
+      k = std::min(k, r.row_new[i]);
+    }
+  r.col_old.resize(n);
+  std::iota(r.col_old.begin(), r.col_old.end(), 0);
+  std::stable_sort(r.col_old.begin(), r.col_old.end(),
+                   [&key](int32_t a, int32_t b) { return key[a] < key[b]; });
+  r.col_new.resize(n);
+  for (int32_t j = 0; j < n; ++j) r.col_new[r.col_old[j]] = j;
+  return r;
+}
+
+namespace {
+
+// Rows taken in the order row_old, each with its nonzeros in stored order,
+// column indices mapped through col_new.
+HostCsr relabel_csr(const HostCsr& a, const std::vector<int32_t>& row_old,
+                    const std::vector<int32_t>& col_new) {
+  HostCsr b;
+  b.rows = a.rows;
+  b.cols = a.cols;
+  b.start.assign(static_cast<size_t>(a.rows) + 1, 0);
+  b.index.resize(a.index.size());
+  b.value.resize(a.value.size());
+  int32_t e = 0;
+  for (int32_t r = 0; r < a.rows; ++r) {
+    const int32_t i = row_old[r];
+    for (int32_t s = a.start[i]; s < a.start[i + 1]; ++s, ++e) {
+      b.index[e] = col_new[a.index[s]];
+      b.value[e] = a.value[s];
+    }
+    b.start[r + 1] = e;
+  }
+  return b;
+}
+
+std::vector<double> take(const std::vector<double>& v, const std::vector<int32_t>& old) {
+  std::vector<double> out(old.size());
+  for (size_t i = 0; i < old.size(); ++i) out[i] = v[old[i]];
+  return out;
+}
+
+std::vector<double> take(const double* v, const std::vector<int32_t>& old) {
+  std::vector<double> out(old.size());
+  for (size_t i = 0; i < old.size(); ++i) out[i] = v[old[i]];
+  return out;
+}
+
+void apply_relabel(Problem& p, const Relabel& r) {
+  p.k = relabel_csr(p.k, r.row_old, r.col_new);
+  p.kt = relabel_csr(p.kt, r.col_old, r.row_new);
+  p.scaling.row_scale = take(p.scaling.row_scale, r.row_old);
+  p.scaling.col_scale = take(p.scaling.col_scale, r.col_old);
+  for (auto& d : p.sweeps.d1) d = take(d, r.row_old);
+  for (auto& d : p.sweeps.d2) d = take(d, r.col_old);
+  p.col_old = r.col_old;
+}
+
+}  // namespace
+
 // -------------------------------------------------------------- setup
 
 std::unique_ptr<Problem> make_problem(const anu_lp& lp, const anu_pdhg_options& o,
                                       double* scaling_seconds, double* norm_seconds,
-                                      int32_t seg_nnz, int32_t seg_per_cta) {
+                                      int32_t seg_nnz, int32_t seg_per_cta,
+                                      const Relabel* relabel) {
   int count = 0;
   const cudaError_t ce = cudaGetDeviceCount(&count);
   if (ce != cudaSuccess || count == 0)
@@ -436,6 +526,7 @@ std::unique_ptr<Problem> make_problem(const anu_lp& lp, const anu_pdhg_options& 
   p->k = copy_csr(lp.k.rows, lp.k.cols, lp.k.nnz, lp.k.start, lp.k.index, lp.k.value);
   p->scaling = scale_matrix_sweeps(&p->k, o.ruiz_iterations, o.pock_chambolle != 0, &p->sweeps);
   p->kt = transpose(p->k);
+  if (relabel != nullptr && !relabel->empty()) apply_relabel(*p, *relabel);
   if (scaling_seconds) *scaling_seconds = now_seconds() - t0;
   const bool fp32 = o.precision == ANU_PRECISION_FP32;
   p->seg_nnz = seg_nnz;
@@ -483,6 +574,7 @@ std::unique_ptr<Problem> clone_problem(const Problem& src) {
   p->sweeps = src.sweeps;
   p->unit_scaling = src.unit_scaling;
   p->matrix_norm = src.matrix_norm;
+  p->col_old = src.col_old;
   const bool fp32 = p->precision == ANU_PRECISION_FP32;
   p->seg_nnz = src.seg_nnz;
   p->seg_per_cta = src.seg_per_cta;
@@ -2384,6 +2476,9 @@ void fill_result(const anu::Problem& p, const anu::CaseResult& cr, double scalin
 
 struct anu_pdhg {
   std::unique_ptr<anu::Problem> problem;
+  // Set when options.locality_order is on: the problem and its case data
+  // are relabelled, and x, y and warm starts are mapped at the boundary.
+  anu::Relabel relabel;
   anu::CaseData data;
   anu_pdhg_options options;
   double scaling_seconds = 0.0;
@@ -2454,6 +2549,7 @@ void anu_pdhg_default_options(anu_pdhg_options* o) {
   o->profile = 0;
   o->split_stacks = 1;
   o->persistent_chunks = 0;
+  o->locality_order = 0;
 }
 
 int anu_last_error(char* buf, int32_t size) { return anu::copy_last_error(buf, size); }
@@ -2481,9 +2577,20 @@ int anu_pdhg_create(const anu_lp* lp, const anu_pdhg_options* options, anu_pdhg*
     if (!e.empty()) throw Error(ANU_ERR_INVALID, "invalid LP: " + e);
     auto h = std::make_unique<anu_pdhg>();
     h->options = *options;
-    h->problem = anu::make_problem(*lp, *options, &h->scaling_seconds, &h->norm_seconds);
-    h->data = anu::make_case(*h->problem, lp->c, lp->q, lp->lower, lp->upper, lp->objective_scale,
-                             lp->objective_offset);
+    if (options->locality_order != 0) h->relabel = anu::locality_relabel(*lp);
+    h->problem = anu::make_problem(*lp, *options, &h->scaling_seconds, &h->norm_seconds,
+                                   anu::kSegNnz, anu::kSegPerCta, &h->relabel);
+    if (h->relabel.empty()) {
+      h->data = anu::make_case(*h->problem, lp->c, lp->q, lp->lower, lp->upper,
+                               lp->objective_scale, lp->objective_offset);
+    } else {
+      const anu::Relabel& r = h->relabel;
+      const std::vector<double> c = anu::take(lp->c, r.col_old), q = anu::take(lp->q, r.row_old),
+                                lo = anu::take(lp->lower, r.col_old),
+                                up = anu::take(lp->upper, r.col_old);
+      h->data = anu::make_case(*h->problem, c.data(), q.data(), lo.data(), up.data(),
+                               lp->objective_scale, lp->objective_offset);
+    }
     *handle = h.release();
   });
 }
@@ -2495,17 +2602,30 @@ int anu_pdhg_run(anu_pdhg* h, const double* warm_x, const double* warm_y, double
     const double start = anu::now_seconds();
     std::vector<double> wx, wy;
     std::vector<const std::vector<double>*> vwx(1, nullptr), vwy(1, nullptr);
+    const anu::Relabel& r = h->relabel;
     if (warm_x != nullptr && warm_y != nullptr) {
-      wx.assign(warm_x, warm_x + h->problem->n);
-      wy.assign(warm_y, warm_y + h->problem->m);
+      if (r.empty()) {
+        wx.assign(warm_x, warm_x + h->problem->n);
+        wy.assign(warm_y, warm_y + h->problem->m);
+      } else {
+        wx = anu::take(warm_x, r.col_old);
+        wy = anu::take(warm_y, r.row_old);
+      }
       vwx[0] = &wx;
       vwy[0] = &wy;
     }
     std::vector<anu::CaseResult> res;
     anu::run_cases(*h->problem, {&h->data}, h->options, vwx, vwy, &res, start);
     fill_result(*h->problem, res[0], h->scaling_seconds, h->norm_seconds, result);
-    if (x) std::copy(res[0].x.begin(), res[0].x.end(), x);
-    if (y) std::copy(res[0].y.begin(), res[0].y.end(), y);
+    if (r.empty()) {
+      if (x) std::copy(res[0].x.begin(), res[0].x.end(), x);
+      if (y) std::copy(res[0].y.begin(), res[0].y.end(), y);
+    } else {
+      if (x)
+        for (size_t j = 0; j < r.col_old.size(); ++j) x[r.col_old[j]] = res[0].x[j];
+      if (y)
+        for (size_t i = 0; i < r.row_old.size(); ++i) y[r.row_old[i]] = res[0].y[i];
+    }
   });
 }
 

@@ -167,6 +167,22 @@ struct DevCsr {
   CsrView<V> view() const;
 };
 
+// A relabelling of the rows and columns of K that gives the gathers of the
+// two products locality. Rows are ordered by decreasing length, within the
+// equality block and within the inequality block, so the first num_equalities
+// rows are still the equalities. Columns are ordered by the first relabelled
+// row they touch, so the columns of one long row sit together. row_old[r] is
+// the original row of relabelled row r and row_new its inverse; likewise for
+// the columns. Every row of K and of K' keeps its nonzeros in their original
+// order, so each product entry is summed in the same order as without it.
+struct Relabel {
+  std::vector<int32_t> row_old, row_new, col_old, col_new;
+  bool empty() const { return row_old.empty() || col_old.empty(); }
+};
+
+// The relabelling of `lp`'s matrix (empty when it has no rows or columns).
+Relabel locality_relabel(const anu_lp& lp);
+
 // Everything that depends on the matrix alone: the scaled matrix and its
 // transpose (host and device), the scaling, ||K~||, the stream.
 struct Problem : Exec {
@@ -184,6 +200,9 @@ struct Problem : Exec {
   bool owns_stream = false;
   int device = 0;
   int32_t seg_nnz = kSegNnz, seg_per_cta = kSegPerCta;  // segment schedule shape
+  // Original column of each column when the problem is relabelled (empty
+  // otherwise); the power iteration's start vector follows it.
+  std::vector<int32_t> col_old;
   ~Problem();
 };
 
@@ -208,9 +227,13 @@ struct CaseResult {
 // Builds the problem from a validated LP: copies, scales, uploads, and
 // estimates ||K~|| unless known_matrix_norm is given.
 // seg_nnz, seg_per_cta: the shape of the case-stack segment schedule.
+// relabel: when given and not empty, the scaled matrix, its transpose and the
+// scaling are relabelled after scaling (which runs in the original order);
+// every case vector handed to this problem must then be relabelled too.
 std::unique_ptr<Problem> make_problem(const anu_lp& lp, const anu_pdhg_options& o,
                                       double* scaling_seconds, double* norm_seconds,
-                                      int32_t seg_nnz = kSegNnz, int32_t seg_per_cta = kSegPerCta);
+                                      int32_t seg_nnz = kSegNnz, int32_t seg_per_cta = kSegPerCta,
+                                      const Relabel* relabel = nullptr);
 // A second problem on its own stream and memory pool with the same scaled
 // matrix (host and device copies), scaling and norm, made without scaling or
 // power iteration again.

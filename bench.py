@@ -153,7 +153,7 @@ def flush_l2(torch, buf):
     buf.zero_()
 
 
-def spmv_leg(iterations, device, peak):
+def spmv_leg(iterations, device, peak, only=None):
     """Per-iteration time of the single-LP path on the power-law LP: two fused
     SpMV + step kernels per iteration, graph-captured, timed by the engine's
     CUDA events around every iteration chunk (`profile`)."""
@@ -166,9 +166,17 @@ def spmv_leg(iterations, device, peak):
            "peak_GBps": peak,
            "note": "algorithmic bytes = 2 nnz (s_a + 4) + 4 (m + n + 2) + s_x (8n + 7m); "
                    "each gathered x or y element also moves a 32-byte sector through L1"}
-    for name, prec, size in (("fp32", PRECISION_FP32, 4), ("fp64", PRECISION_FP64, 8)):
+    # *_relabelled: the same with options.locality_order (rows by length,
+    # columns grouped under their first row), which gives the gathers cache
+    # locality; the arithmetic and its summation order are unchanged.
+    legs = (("fp32", PRECISION_FP32, 4, 0), ("fp64", PRECISION_FP64, 8, 0),
+            ("fp32_relabelled", PRECISION_FP32, 4, 1), ("fp64_relabelled", PRECISION_FP64, 8, 1))
+    for name, prec, size, relabel in legs:
+        if only and name not in only:
+            continue
         opts = make_options(tolerance=1e-12, precision=prec, max_iterations=iterations,
-                            profile=1, polish_feasibility=0, polish_on_exit=0, device=device)
+                            profile=1, polish_feasibility=0, polish_on_exit=0, device=device,
+                            locality_order=relabel)
         r = pdhg.solve_pdhg(lp, opts)
         per_it = r.device_iteration_seconds / max(r.device_iterations, 1)
         b = algorithmic_bytes_per_iteration(nnz, m, n, 1, size, size)
@@ -670,6 +678,9 @@ def main(argv=None):
     ap.add_argument("--packed-workers", type=int, default=0,
                     help="LPs in flight for --workload packed (0: autotune)")
     ap.add_argument("--spmv-iterations", type=int, default=2000)
+    ap.add_argument("--spmv-legs", default="",
+                    help="comma list of spmv legs to run with --workload spmv "
+                         "(fp32, fp64, fp32_relabelled, fp64_relabelled; default all)")
     ap.add_argument("--no-side", dest="side", action="store_false",
                     help="skip the spmv and fp64 single-case side measurements")
     args = ap.parse_args(argv)
@@ -690,7 +701,8 @@ def main(argv=None):
             import torch
             torch.cuda.set_device(local_rank)
             peak, kind = hbm_peak()
-            out = spmv_leg(args.spmv_iterations, local_rank, peak)
+            out = spmv_leg(args.spmv_iterations, local_rank, peak,
+                           args.spmv_legs.split(",") if args.spmv_legs else None)
             out["peak_source"] = kind
     else:
         out = run_engine(args, rank, world, local_rank)

@@ -170,6 +170,17 @@ typedef struct anu_pdhg_options {
    * a grid barrier costs about as much as the launch it replaces, so the
    * graphs of two half-stacks are faster on the stacks measured so far. */
   int32_t persistent_chunks;
+  /* 1: anu_pdhg_create / anu_pdhg_solve relabel the rows and columns of the
+   * scaled matrix so the gathers of the two products share cache lines: rows
+   * by decreasing length (within the equality and the inequality block),
+   * columns by the first such row they touch. Scaling runs before it, in the
+   * original order; every row keeps its nonzeros in their original order, so
+   * each product entry is summed as without it. x, y and warm starts stay in
+   * the caller's order. The reductions of the checks then sum in another
+   * order, so FP64 results agree with the unrelabelled solve to rounding,
+   * not bit for bit. Case stacks, packed batches and the unrolled program
+   * ignore it. 0 (default) = off. */
+  int32_t locality_order;
 } anu_pdhg_options;
 
 /* PdhgResidual, src/anukulan/pdhg.hpp:429-496. */
