@@ -59,7 +59,7 @@ class anu_pdhg_options(C.Structure):
         ("stop", C.POINTER(i32)),
         ("precision", i32), ("refinement", i32), ("device", i32), ("use_graphs", i32),
         ("profile", i32), ("split_stacks", i32), ("persistent_chunks", i32),
-        ("locality_order", i32),
+        ("locality_order", i32), ("scaling_on_device", i32),
     ]
 
 
@@ -106,7 +106,7 @@ DEFAULTS = dict(
     known_matrix_norm=0.0, initial_step_size=0.0, initial_primal_weight=0.0,
     verbose=0, log_frequency=5000, precision=0, refinement=1,
     device=0, use_graphs=1, profile=0, split_stacks=1,
-    persistent_chunks=0, locality_order=0,
+    persistent_chunks=0, locality_order=0, scaling_on_device=1,
 )
 
 

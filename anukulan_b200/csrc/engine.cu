@@ -361,29 +361,67 @@ double device_matrix_norm(Problem& p, int iterations, double tolerance) {
   const double norm = std::sqrt(ss);
   if (norm == 0.0) return 0.0;
   for (double& a : v) a /= norm;
-  DevBuf<double> dv(n), dkv(m), dktkv(n), partial, sumsq(1), est(std::max(iterations, 1));
-  ANU_CUDA(cudaMemcpyAsync(dv.p, v.data(), sizeof(double) * n, cudaMemcpyHostToDevice, p.stream));
-  std::vector<double> h_est(std::max(iterations, 1));
   // Chunks of iterations between host looks; the convergence test reads the
-  // estimates in order, so running past convergence changes nothing.
+  // estimates in order, so running past convergence (or past `iterations`,
+  // in the last chunk) changes nothing. Estimate slots are per position in
+  // the chunk, so after the first chunk (run directly, which also sizes the
+  // reduction scratch) every chunk is the same work: one CUDA graph,
+  // captured once and replayed.
   const int chunk = 16;
-  double sigma = 0.0;
-  for (int base = 0; base < iterations; base += chunk) {
-    const int count = std::min(chunk, iterations - base);
+  DevBuf<double> dv(n), dkv(m), dktkv(n), partial, sumsq(1), est(chunk);
+  ANU_CUDA(cudaMemcpyAsync(dv.p, v.data(), sizeof(double) * n, cudaMemcpyHostToDevice, p.stream));
+  std::vector<double> h_est(chunk);
+  auto enqueue = [&](int count) {
     for (int it = 0; it < count; ++it) {
       product<double, double, double>(p, p.dk, dv.p, 1, StoreEpi<double>{1, dkv.p});
       product<double, double, double>(p, p.dkt, dkv.p, 1, StoreEpi<double>{1, dktkv.p});
       reduce_terms(p, n, 1, SquareTerms<double>{1, dktkv.p}, partial, sumsq.p, 1, 0);
       normalize_kernel<<<grid_for(n, 256, 296), 256, 0, p.stream>>>(n, dktkv.p, sumsq.p, dv.p,
-                                                                     est.p, base + it);
+                                                                     est.p, it);
       ANU_CUDA(cudaGetLastError());
       ++p.launches;
     }
-    ANU_CUDA(cudaMemcpyAsync(h_est.data() + base, est.p + base, sizeof(double) * count,
+  };
+  struct GraphGuard {
+    cudaGraphExec_t exec = nullptr;
+    ~GraphGuard() {
+      if (exec) cudaGraphExecDestroy(exec);
+    }
+  } graph;
+  int64_t graph_launches = 0;
+  double sigma = 0.0;
+  for (int base = 0; base < iterations; base += chunk) {
+    const int count = std::min(chunk, iterations - base);
+    if (base == 0) {
+      enqueue(count);
+    } else {
+      if (graph.exec == nullptr) {
+        const int64_t before = p.launches;
+        ANU_CUDA(cudaStreamBeginCapture(p.stream, cudaStreamCaptureModeThreadLocal));
+        try {
+          enqueue(chunk);
+        } catch (...) {
+          cudaGraph_t broken = nullptr;
+          cudaStreamEndCapture(p.stream, &broken);
+          if (broken) cudaGraphDestroy(broken);
+          throw;
+        }
+        cudaGraph_t g = nullptr;
+        ANU_CUDA(cudaStreamEndCapture(p.stream, &g));
+        const cudaError_t e = cudaGraphInstantiate(&graph.exec, g, 0);
+        cudaGraphDestroy(g);
+        ANU_CUDA(e);
+        graph_launches = p.launches - before;
+        p.launches = before;
+      }
+      ANU_CUDA(cudaGraphLaunch(graph.exec, p.stream));
+      p.launches += graph_launches;
+    }
+    ANU_CUDA(cudaMemcpyAsync(h_est.data(), est.p, sizeof(double) * count,
                              cudaMemcpyDeviceToHost, p.stream));
     ANU_CUDA(cudaStreamSynchronize(p.stream));
     for (int it = base; it < base + count; ++it) {
-      const double next = h_est[it];
+      const double next = h_est[it - base];
       if (next == 0.0) return 0.0;
       const double estimate = std::sqrt(next);
       if (it > 0 && std::fabs(estimate - sigma) <= tolerance * estimate) return estimate;
@@ -524,8 +562,14 @@ std::unique_ptr<Problem> make_problem(const anu_lp& lp, const anu_pdhg_options& 
   p->precision = o.precision;
   double t0 = now_seconds();
   p->k = copy_csr(lp.k.rows, lp.k.cols, lp.k.nnz, lp.k.start, lp.k.index, lp.k.value);
-  p->scaling = scale_matrix_sweeps(&p->k, o.ruiz_iterations, o.pock_chambolle != 0, &p->sweeps);
-  p->kt = transpose(p->k);
+  const int sweeps = o.ruiz_iterations + (o.pock_chambolle != 0 ? 1 : 0);
+  if (o.scaling_on_device != 0 && sweeps > 0 && p->k.nnz() > 0) {
+    p->scaling = scale_matrix_sweeps_device(*p, &p->k, &p->kt, o.ruiz_iterations,
+                                            o.pock_chambolle != 0, &p->sweeps);
+  } else {
+    p->scaling = scale_matrix_sweeps(&p->k, o.ruiz_iterations, o.pock_chambolle != 0, &p->sweeps);
+    p->kt = transpose(p->k);
+  }
   if (relabel != nullptr && !relabel->empty()) apply_relabel(*p, *relabel);
   if (scaling_seconds) *scaling_seconds = now_seconds() - t0;
   const bool fp32 = o.precision == ANU_PRECISION_FP32;
@@ -2550,6 +2594,7 @@ void anu_pdhg_default_options(anu_pdhg_options* o) {
   o->split_stacks = 1;
   o->persistent_chunks = 0;
   o->locality_order = 0;
+  o->scaling_on_device = 1;
 }
 
 int anu_last_error(char* buf, int32_t size) { return anu::copy_last_error(buf, size); }

@@ -234,6 +234,12 @@ std::unique_ptr<Problem> make_problem(const anu_lp& lp, const anu_pdhg_options& 
                                       double* scaling_seconds, double* norm_seconds,
                                       int32_t seg_nnz = kSegNnz, int32_t seg_per_cta = kSegPerCta,
                                       const Relabel* relabel = nullptr);
+// scale_matrix_sweeps on the device: the same norms, factors and roundings,
+// so the scaled matrix and the factors are bit-identical to the host's.
+// Scales *k in place and writes its transpose to *kt.
+Scaling scale_matrix_sweeps_device(Exec& ex, HostCsr* k, HostCsr* kt, int ruiz_iterations,
+                                   bool pock_chambolle, ScalingSweeps* sweeps);
+
 // A second problem on its own stream and memory pool with the same scaled
 // matrix (host and device copies), scaling and norm, made without scaling or
 // power iteration again.

@@ -40,7 +40,9 @@ HostCsr copy_csr(int32_t rows, int32_t cols, int32_t nnz, const int32_t* start,
   return a;
 }
 
-HostCsr transpose(const HostCsr& a) {
+HostCsr transpose(const HostCsr& a) { return transpose(a, nullptr); }
+
+HostCsr transpose(const HostCsr& a, std::vector<int32_t>* pos) {
   HostCsr t;
   t.rows = a.cols;
   t.cols = a.rows;
@@ -50,11 +52,13 @@ HostCsr transpose(const HostCsr& a) {
   for (const int32_t c : a.index) t.start[static_cast<std::size_t>(c) + 1]++;
   for (std::size_t i = 1; i < t.start.size(); ++i) t.start[i] += t.start[i - 1];
   std::vector<int32_t> cursor(t.start.begin(), t.start.end() - 1);
+  if (pos != nullptr) pos->resize(a.index.size());
   for (int32_t r = 0; r < a.rows; ++r) {
     for (int32_t k = a.start[r]; k < a.start[r + 1]; ++k) {
       const int32_t dest = cursor[a.index[k]]++;
       t.index[dest] = r;
       t.value[dest] = a.value[k];
+      if (pos != nullptr) (*pos)[dest] = k;
     }
   }
   return t;
@@ -102,6 +106,8 @@ double spread(const std::vector<double>& norms) {
 }
 
 }  // namespace
+
+double norm_spread(const std::vector<double>& norms) { return spread(norms); }
 
 Scaling scale_matrix_sweeps(HostCsr* k, int ruiz_iterations, bool pock_chambolle,
                             ScalingSweeps* sweeps) {

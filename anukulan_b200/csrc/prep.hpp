@@ -30,6 +30,8 @@ HostCsr copy_csr(int32_t rows, int32_t cols, int32_t nnz, const int32_t* start,
 // SparseMatrix::transpose (src/anukulan/sparse.cpp:93-117): counting sort with
 // rows visited in increasing order, so each transposed row is sorted.
 HostCsr transpose(const HostCsr& a);
+// The same, and pos[t] = the position in `a` of the transpose's entry t.
+HostCsr transpose(const HostCsr& a, std::vector<int32_t>* pos);
 
 // y = A x, each row summed left to right (sparse.cpp:72-80).
 void multiply(const HostCsr& a, const double* x, double* y);
@@ -55,6 +57,10 @@ struct ScalingSweeps {
 };
 Scaling scale_matrix_sweeps(HostCsr* k, int ruiz_iterations, bool pock_chambolle,
                             ScalingSweeps* sweeps);
+// Largest over smallest positive norm (1 when all are zero), the spread
+// scale_lp reports (scaling.cpp:18-28).
+double norm_spread(const std::vector<double>& norms);
+
 void scale_vectors(const ScalingSweeps& sw, int32_t m, int32_t n, double* c, double* q,
                    double* lower, double* upper);
 

@@ -180,10 +180,19 @@ def spmv_leg(iterations, device, peak, only=None):
         r = pdhg.solve_pdhg(lp, opts)
         per_it = r.device_iteration_seconds / max(r.device_iterations, 1)
         b = algorithmic_bytes_per_iteration(nnz, m, n, 1, size, size)
-        out[name] = {"us_per_iteration": per_it * 1e6, "iterations_per_second": 1.0 / per_it,
+        out[name] = {"setup_ms": {k: round(r.phases[k] * 1e3, 2)
+                                  for k in ("scaling", "matrix_norm")},
+                     "us_per_iteration": per_it * 1e6, "iterations_per_second": 1.0 / per_it,
                      "algorithmic_bytes_per_iteration": b,
                      "achieved_GBps": b / per_it / 1e9, "frac": b / per_it / 1e9 / peak,
                      "kernel_launches": int(r.kernel_launches)}
+    if not only or "host_scaling" in only:
+        # The same set-up with scale_lp's sweeps on the host instead.
+        r = pdhg.solve_pdhg(lp, make_options(max_iterations=1, polish_feasibility=0,
+                                             polish_on_exit=0, device=device,
+                                             scaling_on_device=0))
+        out["host_scaling_setup_ms"] = {k: round(r.phases[k] * 1e3, 2)
+                                        for k in ("scaling", "matrix_norm")}
     return out
 
 

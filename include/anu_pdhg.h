@@ -181,6 +181,12 @@ typedef struct anu_pdhg_options {
    * not bit for bit. Case stacks, packed batches and the unrolled program
    * ignore it. 0 (default) = off. */
   int32_t locality_order;
+  /* 1 (default): scale_lp's Ruiz and Pock-Chambolle sweeps run on the
+   * device, with the same norms in the same summation order, the same
+   * correctly rounded factors and the same two roundings per nonzero, so the
+   * scaled matrix and every factor are bit-identical to the host sweeps.
+   * 0 = on the host. */
+  int32_t scaling_on_device;
 } anu_pdhg_options;
 
 /* PdhgResidual, src/anukulan/pdhg.hpp:429-496. */

@@ -133,7 +133,7 @@ def test_defaults_match_reference_pdhg_options():
     mine = abi.options_dict(abi.make_options())
     for k, v in ref.items():
         if k in ("precision", "refinement", "device", "use_graphs", "profile", "split_stacks",
-                 "persistent_chunks"):
+                 "persistent_chunks", "locality_order", "scaling_on_device"):
             continue
         assert mine[k] == v, k
 
