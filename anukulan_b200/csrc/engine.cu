@@ -577,6 +577,8 @@ std::unique_ptr<Problem> make_problem(const anu_lp& lp, const anu_pdhg_options& 
   p->seg_per_cta = seg_per_cta;
   p->dk.upload(p->k, fp32, p->stream, seg_nnz, seg_per_cta);
   p->dkt.upload(p->kt, fp32, p->stream, seg_nnz, seg_per_cta);
+  if (fp32) prepare_iteration_kernels<float>(p->stream);
+  else prepare_iteration_kernels<double>(p->stream);
   p->row_scale.alloc(std::max(p->m, 1));
   p->col_scale.alloc(std::max(p->n, 1));
   if (p->m > 0)

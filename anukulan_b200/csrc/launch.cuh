@@ -5,6 +5,8 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <atomic>
 #include <cstdint>
 
 #include "kernels.cuh"
@@ -28,12 +30,69 @@ inline int grid_for(int64_t items, int per_block, int cap) {
 }
 
 
+// Shared-memory carveout for rows_kernel. Its residency is set by registers:
+// in FP32 12 CTAs of 128 threads at 40 registers, which need about 75 KB of
+// shared memory, while the driver by default sizes the carveout for the
+// shared-memory limit alone (21 CTAs, 132 KB) and leaves the rest to L1. The
+// hint asks for what the register-bound CTAs need, so every CTA stays
+// resident and the gathered vectors get the remaining L1. Set once per
+// instantiation; it is only a hint, and a failure to set it is ignored.
+template <class F>
+void prefer_register_bound_carveout(F kernel, int threads) {
+  int dev = 0;
+  cudaFuncAttributes fa{};
+  int smem_sm = 0, regs_sm = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaFuncGetAttributes(&fa, kernel) != cudaSuccess ||
+      cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) !=
+          cudaSuccess ||
+      cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev) !=
+          cudaSuccess ||
+      fa.numRegs <= 0 || smem_sm <= 0) {
+    cudaGetLastError();
+    return;
+  }
+  const int by_regs = regs_sm / (fa.numRegs * threads);
+  const int by_warps = 64 / ((threads + 31) / 32);
+  const int blocks = std::max(1, std::min(by_regs, by_warps));
+  const size_t need = static_cast<size_t>(blocks) * (fa.sharedSizeBytes + 1024);
+  const int percent = static_cast<int>(std::min<size_t>(100, (need * 100 + smem_sm - 1) / smem_sm));
+  if (cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, percent) !=
+      cudaSuccess)
+    cudaGetLastError();
+}
+
+// Applied at the first launch of each instantiation that is not being
+// captured into a graph (no attribute calls inside a capture).
+template <class V, class X, class Acc, class Epi>
+void rows_kernel_setup(cudaStream_t s) {
+  static std::atomic<bool> done{false};
+  if (done.load(std::memory_order_acquire)) return;
+  cudaStreamCaptureStatus status = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &status) != cudaSuccess) {
+    cudaGetLastError();
+    return;
+  }
+  if (status != cudaStreamCaptureStatusNone) return;
+  prefer_register_bound_carveout(rows_kernel<V, X, Acc, Epi>, kRowThreads);
+  done.store(true, std::memory_order_release);
+}
+
+// The carveout hint for the single-LP iteration kernels of precision T. Their
+// first launches are usually inside a graph capture, where rows_kernel_setup
+// leaves them alone, so the problem set-up applies it beforehand.
+template <class T>
+void prepare_iteration_kernels(cudaStream_t s) {
+  rows_kernel_setup<T, T, T, PrimalEpi<T>>(s);
+  rows_kernel_setup<T, T, T, DualEpi<T>>(s);
+}
+
 // y = A x (any epilogue) for K cases.
 template <class V, class X, class Acc, class Epi, class Mat>
 void product(Exec& p, const Mat& a, const X* x, int K, const Epi& epi, bool pdl = false) {
   if (a.rows == 0) return;
   cudaStream_t s = p.stream;
   if (K == 1) {
+    rows_kernel_setup<V, X, Acc, Epi>(s);
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(a.num_blocks);
     cfg.blockDim = dim3(kRowThreads);
