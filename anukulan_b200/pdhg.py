@@ -14,8 +14,8 @@ from typing import Optional, Sequence
 
 import numpy as np
 
-from .abi import (CLp, PdhgResult, Residual, anu_csr, anu_lp, anu_pdhg_options,
-                  anu_pdhg_residual, anu_pdhg_result, f64_ptr, make_options)
+from .abi import (OPTIMAL, PRIMAL_INFEASIBLE, CLp, PdhgResult, Residual, anu_csr, anu_lp,
+                  anu_pdhg_options, anu_pdhg_residual, anu_pdhg_result, f64_ptr, make_options)
 from .model import StandardLp
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -280,6 +280,49 @@ class CaseStackSolver:
             self.close()
         except Exception:
             pass
+
+
+class NodeRelaxation:
+    """One branch-and-bound node's first-order relaxation, judged as
+    branch_and_bound.cpp:532-565 judges it.
+
+    A first-order point is only nearly optimal, so its objective is no bound.
+    The dual objective is one by weak duality, as long as y is dual feasible.
+    The node therefore counts as solved (`optimal`) when PDHG reports optimal
+    and dual_residual_inf <= 1e-7 * max(1, |dual objective|). `bound` is then
+    that dual objective (standard form, a minimisation), and NaN otherwise.
+    `proved_infeasible` is a primal infeasibility certificate."""
+
+    __slots__ = ("result", "optimal", "proved_infeasible", "bound")
+
+    def __init__(self, result: PdhgResult):
+        d = result.residual.dual_objective
+        enough = 1e-7 * max(1.0, abs(d))
+        self.result = result
+        self.optimal = result.status == OPTIMAL and result.residual.dual_residual_inf <= enough
+        self.proved_infeasible = result.status == PRIMAL_INFEASIBLE
+        self.bound = d if self.optimal else float("nan")
+
+
+def solve_node_relaxations(lp: StandardLp, lower, upper,
+                           options: Optional[anu_pdhg_options] = None, **kw):
+    """Relaxations of branch-and-bound nodes as one case stack.
+
+    The nodes differ from `lp` only in column bounds: `lower` and `upper`
+    are (nodes x n). The reference solves each node with solve_pdhg
+    (branch_and_bound.cpp:532-537). That call passes the parent's x alone as
+    warm_x, and solve_pdhg takes a warm start only when both x and y are
+    given (pdhg.cpp:481-484), so every node starts from the origin, as here.
+    Returns one :class:`NodeRelaxation` per node."""
+    lower = np.atleast_2d(np.asarray(lower, np.float64))
+    upper = np.atleast_2d(np.asarray(upper, np.float64))
+    if lower.shape != upper.shape or lower.shape[1] != lp.num_cols:
+        raise ValueError("node bounds must be (nodes x columns), the same for lower and upper")
+    solver = CaseStackSolver(lp, lower=lower, upper=upper, options=options, **kw)
+    try:
+        return [NodeRelaxation(r) for r in solver.solve()]
+    finally:
+        solver.close()
 
 
 def solve_case_stack(stack, options: Optional[anu_pdhg_options] = None, **kw):

@@ -186,3 +186,27 @@ def test_reference_adapter_without_device_falls_back_and_fails_loudly():
     for path in (oracle.REF_B200_TEST_BACKEND, oracle.REF_B200_TEST_PDHG):
         p = subprocess.run([path], capture_output=True, text=True, timeout=300)
         assert p.returncode == 0, p.stdout + p.stderr
+
+
+def test_node_relaxation_rule():
+    """NodeRelaxation judges a node as branch_and_bound.cpp:556-565 does:
+    certified only when optimal and dual feasible to 1e-7 of the dual
+    objective; the bound is then the dual objective."""
+    from anukulan_b200.abi import PdhgResult, Residual
+    from anukulan_b200.pdhg import NodeRelaxation
+
+    def result(status, dual_objective, dual_inf):
+        res = Residual(dual_residual_inf=dual_inf, dual_objective=dual_objective)
+        return PdhgResult(status, np.zeros(1), np.zeros(1), 0.0, 0, 0, 0, 0, False, 0.0, 0.0,
+                          0.0, 0.0, {}, res, (1.0, 1.0, 1.0, 1.0), 0, 0, 0.0, 0, "")
+
+    ok = NodeRelaxation(result(abi.OPTIMAL, -2.0e6, 0.1))
+    assert ok.optimal and ok.bound == -2.0e6 and not ok.proved_infeasible
+    loose = NodeRelaxation(result(abi.OPTIMAL, -2.0e6, 0.3))
+    assert not loose.optimal and np.isnan(loose.bound)
+    small = NodeRelaxation(result(abi.OPTIMAL, 0.5, 1.0e-7))
+    assert small.optimal and small.bound == 0.5
+    assert not NodeRelaxation(result(abi.OPTIMAL, 0.5, 1.1e-7)).optimal
+    inf = NodeRelaxation(result(abi.PRIMAL_INFEASIBLE, 0.0, 0.0))
+    assert inf.proved_infeasible and not inf.optimal
+    assert not NodeRelaxation(result(abi.ITERATION_LIMIT, 1.0, 0.0)).optimal
