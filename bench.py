@@ -638,7 +638,12 @@ def run_reference(args, rank, world):
                 "d2h_bytes_per_step": 0},
     }
     if args.gpu_reference and oracle.have_reference_cuda():
-        out["gpu_reference"] = reference_gpu_leg(st)
+        # A side leg: without a usable device it records why instead of
+        # ending the reference arm's line.
+        try:
+            out["gpu_reference"] = reference_gpu_leg(st)
+        except RuntimeError as e:
+            out["gpu_reference"] = {"unavailable": str(e)}
     return out
 
 
