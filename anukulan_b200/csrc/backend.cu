@@ -4,9 +4,12 @@
 // backend interface, so a thin C++ adapter class can implement LinAlgBackend
 // over this library and run the reference's own solve_pdhg on these kernels.
 // Matrices are cached under the caller's identity key (SparseMatrix::id(),
-// src/anukulan/sparse.hpp:51), never by address. Operations run on one
-// library stream and have completed when they return, matching the
-// reference's synchronous CUDA backend (cuda_backend.cu:530-559).
+// src/anukulan/sparse.hpp:51), never by address. Operations run in order on
+// one library stream. Those that hand the host a value or take a host buffer
+// (upload, download, the reductions, allocate) return when done; the pure
+// device operations (fill, copy, the products, the updates, accumulate,
+// scale_into) return once queued, as the reference's CUDA backend's kernel
+// launches do (cuda_backend.cu:530-559, 832-858).
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -39,7 +42,10 @@ void ensure(BackendState& s) {
     cudaGetLastError();
     throw Error(ANU_ERR_NO_DEVICE, "no CUDA device is available; this engine has no CPU fallback");
   }
-  ANU_CUDA(cudaStreamCreateWithFlags(&s.exec.stream, cudaStreamNonBlocking));
+  // A blocking stream: ordered with the legacy default stream, so work a
+  // caller queues there (anu_backend_convergence_terms_noalloc among it)
+  // runs after the seam operations queued before it.
+  ANU_CUDA(cudaStreamCreateWithFlags(&s.exec.stream, cudaStreamDefault));
   s.out.alloc(16);
   s.ready = true;
 }
@@ -219,7 +225,6 @@ int anu_backend_fill(double* dev, int64_t n, double value) {
     if (n <= 0) return;
     anu::fill_kernel<<<anu::grid_n(n), 256, 0, s.exec.stream>>>(n, value, dev);
     ANU_CUDA(cudaGetLastError());
-    ANU_CUDA(cudaStreamSynchronize(s.exec.stream));
   });
 }
 
@@ -228,7 +233,6 @@ int anu_backend_copy(const double* source, double* target, int64_t n) {
     if (n <= 0) return;
     ANU_CUDA(cudaMemcpyAsync(target, source, sizeof(double) * n, cudaMemcpyDeviceToDevice,
                              s.exec.stream));
-    ANU_CUDA(cudaStreamSynchronize(s.exec.stream));
   });
 }
 
@@ -254,7 +258,6 @@ int anu_backend_multiply(uint64_t id, const double* x, double* y) {
     auto it = s.matrices.find(id);
     if (it == s.matrices.end()) throw Error(ANU_ERR_INVALID, "matrix was not prepared");
     anu::product<double, double, double>(s.exec, *it->second, x, 1, anu::StoreEpi<double>{1, y});
-    ANU_CUDA(cudaStreamSynchronize(s.exec.stream));
   });
 }
 
@@ -286,7 +289,6 @@ int anu_backend_primal_update(int64_t n, double tau, double gamma, double halper
     anu::primal_update_kernel<<<anu::grid_n(n), 256, 0, s.exec.stream>>>(
         n, tau, gamma, halpern, x, c, kt_y, lower, upper, anchor, x_out, dx, x_bar);
     ANU_CUDA(cudaGetLastError());
-    ANU_CUDA(cudaStreamSynchronize(s.exec.stream));
   });
 }
 
@@ -301,7 +303,6 @@ int anu_backend_dual_update(int64_t m, int64_t num_equalities, double sigma, dou
         m, num_equalities, sigma, gamma, halpern, y, q, k_x_bar, k_x, anchor_y, anchor_kx, y_out,
         dy, k_out, k_dx);
     ANU_CUDA(cudaGetLastError());
-    ANU_CUDA(cudaStreamSynchronize(s.exec.stream));
   });
 }
 
@@ -310,7 +311,6 @@ int anu_backend_accumulate(int64_t n, double weight, const double* v, double* su
     if (n <= 0) return;
     anu::accumulate64_kernel<<<anu::grid_n(n), 256, 0, s.exec.stream>>>(n, weight, v, sum);
     ANU_CUDA(cudaGetLastError());
-    ANU_CUDA(cudaStreamSynchronize(s.exec.stream));
   });
 }
 
@@ -319,7 +319,6 @@ int anu_backend_scale_into(int64_t n, double weight, const double* sum, double* 
     if (n <= 0) return;
     anu::divide_kernel<<<anu::grid_n(n), 256, 0, s.exec.stream>>>(n, weight, sum, out);
     ANU_CUDA(cudaGetLastError());
-    ANU_CUDA(cudaStreamSynchronize(s.exec.stream));
   });
 }
 

@@ -10,7 +10,7 @@ on the device; `e2e` is the same metric through the C ABI from host arrays
 (create + solve + download inside the timed region).
 
     python bench.py [--gpus N --steps K --warmup W] [--impl reference]
-                    [--workload stack|spmv|packed|adjoint|powerlaw]
+                    [--workload stack|spmv|packed|adjoint|powerlaw|seam]
 
 Two side measurements ride on the stack line:
   * `spmv`: the single-LP iteration (the two fused SpMV kernels) on the
@@ -27,7 +27,9 @@ Two side measurements ride on the stack line:
 `--workload packed` times the packed batch of 256 unequal LPs instead,
 `--workload adjoint` the unrolled-PDHG sensitivities of the 60-case stack, and
 `--workload powerlaw --tolerance T` whole solves of the power-law LP in FP32
-(with refinement) and FP64; each prints its own JSON line.
+(with refinement) and FP64, and `--workload seam` the reference's own
+solve_pdhg on its own CUDA backend against the same solver on this engine's
+kernels (through the LinAlgBackend adapter); each prints its own JSON line.
 
 Under torchrun every rank solves its own copy of the stack (weak scaling, no
 collective on the data path); rank 0 prints one JSON line. `--impl reference`
@@ -399,6 +401,50 @@ def run_powerlaw(args, rank, world, local_rank):
     return out
 
 
+def run_seam(args, rank, world, local_rank):
+    """The reference's own solve_pdhg, unchanged, on the power-law LP and on
+    one refinery case, with the seam's arithmetic on (a) the reference's own
+    cuda_backend.cu and (b) this engine's kernels through the LinAlgBackend
+    adapter. Same solver, same calls, one launch per seam operation: the
+    per-iteration time compares the kernels under the seam. FP64, a fixed
+    number of iterations; the two arms' iterates are compared too."""
+    if rank != 0:
+        return None
+    import torch
+    import oracle
+    from anukulan_b200 import lpgen
+    torch.cuda.set_device(local_rank)
+    kw = dict(tolerance=1e-12, max_iterations=args.seam_iterations, polish_on_exit=0,
+              polish_feasibility=0)
+    out = {"metric": "reference solve_pdhg, us per iteration, by backend", "unit": "us",
+           "higher_is_better": False, "n_gpus": 1, "dtype": "f64",
+           "config": {"workload": "seam", "iterations": args.seam_iterations},
+           "data": "synthetic (seeded generators)"}
+    problems = (("powerlaw_lp", lpgen.power_law_lp()[0]),
+                ("refinery_case_0", lpgen.refinery_stack().case(0)))
+    for name, lp in problems:
+        leg = {"rows": lp.num_rows, "cols": lp.num_cols, "nnz": lp.k.nnz}
+        runs = {}
+        for arm, solve in (("reference_cuda_backend", oracle.ref_cuda_solve),
+                           ("engine_adapter", oracle.ref_b200_solve)):
+            solve(lp, **dict(kw, max_iterations=40))  # context, module load, first uploads
+            r = solve(lp, **kw)
+            runs[arm] = r
+            leg[arm] = {"iterations": r.iterations,
+                        "us_per_iteration": 1e6 * r.phases["iterating"] / max(r.iterations, 1),
+                        "iterating_s": r.phases["iterating"], "checks_s": r.phases["checks"],
+                        "scaling_s": r.phases["scaling"]}
+        a, b = runs["reference_cuda_backend"], runs["engine_adapter"]
+        leg["iterate_rel_diff"] = float(max(
+            np.max(np.abs(a.x - b.x)) / max(1.0, float(np.max(np.abs(a.x)))),
+            np.max(np.abs(a.y - b.y)) / max(1.0, float(np.max(np.abs(a.y))))))
+        leg["speedup"] = (leg["reference_cuda_backend"]["us_per_iteration"]
+                          / leg["engine_adapter"]["us_per_iteration"])
+        out[name] = leg
+    out["value"] = out["powerlaw_lp"]["engine_adapter"]["us_per_iteration"]
+    return out
+
+
 def fp64_single_case(st, device):
     """The stack's cases solved one after another by the engine's plain FP64
     single-case mode (host arrays in, results out, like a solve_pdhg call)."""
@@ -688,7 +734,7 @@ def main(argv=None):
     ap.add_argument("--persistent", action="store_true",
                     help="run each iteration chunk of the stack as one cooperative kernel")
     ap.add_argument("--workload", default="stack",
-                    choices=["stack", "spmv", "packed", "adjoint", "powerlaw"])
+                    choices=["stack", "spmv", "packed", "adjoint", "powerlaw", "seam"])
     ap.add_argument("--tolerance", type=float, default=1e-6,
                     help="--workload powerlaw: relative KKT tolerance")
     ap.add_argument("--time-limit", type=float, default=300.0,
@@ -696,6 +742,8 @@ def main(argv=None):
     ap.add_argument("--packed-workers", type=int, default=0,
                     help="LPs in flight for --workload packed (0: autotune)")
     ap.add_argument("--spmv-iterations", type=int, default=2000)
+    ap.add_argument("--seam-iterations", type=int, default=400,
+                    help="--workload seam: iterations of the reference's solve_pdhg per arm")
     ap.add_argument("--locality", type=int, default=0,
                     help="--workload powerlaw: options.locality_order (relabelled rows/columns)")
     ap.add_argument("--precisions", default="fp32,fp64",
@@ -717,6 +765,8 @@ def main(argv=None):
         out = run_adjoint(args, rank, world, local_rank)
     elif args.workload == "powerlaw":
         out = run_powerlaw(args, rank, world, local_rank)
+    elif args.workload == "seam":
+        out = run_seam(args, rank, world, local_rank)
     elif args.workload == "spmv":
         out = None
         if rank == 0:

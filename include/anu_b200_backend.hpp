@@ -10,8 +10,7 @@
 //   options.backend = &anu_b200::backend();
 //   anukulan::PdhgResult r = anukulan::solve_pdhg(lp, options);
 //
-// anu_b200_cuda_backend.cpp, beside the engine's sources, goes one step
-// further: built in place of anukulan's src/anukulan/cuda_backend.cu, it
+// anukulan_b200/integration/cuda_backend_b200.cpp goes one step further: built in place of anukulan's src/anukulan/cuda_backend.cu, it
 // makes anukulan::cuda_backend() and therefore default_backend() return this
 // adapter, so every caller of solve_pdhg and every test built with
 // ANUKULAN_WITH_CUDA runs on these kernels with no source change.
@@ -20,9 +19,13 @@
 // call, same argument order. Matrices are uploaded once per
 // SparseMatrix::id() (sparse.hpp:51), never keyed by address, and a product
 // on a matrix that was not prepared prepares it first, as the reference's
-// CUDA backend does (cuda_backend.cu:832-834). Every call is complete when it
-// returns. A failed call throws std::runtime_error with the library's
-// message, the reference's error convention (cuda_backend.cu:32-37).
+// CUDA backend does (cuda_backend.cu:832-834). Calls run in order on one
+// library stream; those that return a value or take a host buffer are
+// complete when they return, the pure device operations once queued, as with
+// the reference's CUDA backend. A failed call throws std::runtime_error with
+// the library's message, the reference's error convention
+// (cuda_backend.cu:32-37); a failure inside queued work surfaces at the next
+// call that waits.
 //
 // This route runs one launch per seam call, in FP64. It is the compatibility
 // path; anu_pdhg_solve is the fused fast path.

@@ -308,9 +308,12 @@ int anu_estimate_matrix_norm(const anu_lp* lp, int32_t iterations,
  * library and run the reference's own solve_pdhg on these kernels. Vectors
  * are FP64 device arrays from anu_backend_allocate. Matrices are uploaded by
  * anu_backend_prepare under the caller's identity key (SparseMatrix::id(),
- * src/anukulan/sparse.hpp:51), never by address. All operations run on one
- * library-owned stream and are complete when they return, like the
- * reference's synchronous cudaMemcpy-based backend. */
+ * src/anukulan/sparse.hpp:51), never by address. All operations run in order
+ * on one library-owned stream, a blocking stream (ordered with the legacy
+ * default stream). Those that hand the host a value or read a host buffer
+ * (upload, download, dot, the norms and terms, allocate, prepare) return when
+ * done; fill, copy, multiply, the two updates, accumulate and scale_into
+ * return once queued, as the reference's CUDA backend's kernel launches do. */
 int anu_backend_allocate(int64_t n, double** device_ptr);        /* backend.hpp:50, zeroed */
 int anu_backend_deallocate(double* device_ptr);                  /* backend.hpp:51 */
 int anu_backend_upload(const double* host, double* device_ptr, int64_t n);    /* :52 */
