@@ -15,6 +15,8 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <deque>
+#include <functional>
 #include <map>
 #include <numeric>
 #include <thread>
@@ -927,6 +929,11 @@ struct AdmissionQueue {
   size_t next = 0;
   std::vector<int32_t> slot_index;       // the caller's position of each slot's case, -1: none
   std::vector<CaseResult>* out = nullptr;  // results by the caller's position
+  // Streaming stacks only. deliver: takes each result as its case retires,
+  // in place of *out. refill: asked for more cases when `pending` is used up;
+  // appends to it and returns false when it has none now.
+  std::function<void(int32_t, CaseResult&)> deliver;
+  std::function<bool(AdmissionQueue&)> refill;
 };
 
 // One case's column of a case-interleaved device array (element (row, k) at
@@ -1857,7 +1864,8 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
       cr.r.device_iteration_seconds = device_iter_s;
       cr.r.device_iterations = device_iters;
       if (queue != nullptr) {
-        (*queue->out)[queue->slot_index[k]] = std::move(cr);
+        if (queue->deliver) queue->deliver(queue->slot_index[k], cr);
+        else (*queue->out)[queue->slot_index[k]] = std::move(cr);
         cr = CaseResult{};
         queue->slot_index[k] = -1;
       }
@@ -2379,7 +2387,8 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
         t_checks += phase_end();
         finalize(retired);
         for (int k : retired) {
-          if (queue->next >= queue->pending.size()) break;
+          if (queue->next >= queue->pending.size() && !(queue->refill && queue->refill(*queue)))
+            break;
           const size_t q = queue->next;
           admit(k, queue->pending_index[q], queue->pending[q],
                 q < queue->pending_warm_x.size() ? queue->pending_warm_x[q] : nullptr,
@@ -2480,6 +2489,56 @@ void run_cases_rolling(Problem& problem, const std::vector<const CaseData*>& cas
   }
 }
 
+void run_cases_streaming(Problem& problem, int slots, const anu_pdhg_options& options,
+                         const std::function<const CaseData*(int32_t*)>& next_case,
+                         const std::function<void(int32_t, CaseResult&)>& deliver,
+                         double start_time) {
+  ANU_CUDA(cudaSetDevice(problem.device));
+  PoolScope scope(&problem.pool, problem.stream);
+  AdmissionQueue queue;
+  std::vector<CaseResult> unused;
+  queue.out = &unused;
+  queue.deliver = deliver;
+  queue.refill = [&next_case](AdmissionQueue& q) {
+    int32_t id = -1;
+    const CaseData* d = next_case(&id);
+    if (d == nullptr) return false;
+    q.pending.push_back(d);
+    q.pending_index.push_back(id);
+    q.pending_warm_x.push_back(nullptr);
+    q.pending_warm_y.push_back(nullptr);
+    return true;
+  };
+  std::vector<const CaseData*> first;
+  for (int k = 0; k < slots; ++k) {
+    int32_t id = -1;
+    const CaseData* d = next_case(&id);
+    if (d == nullptr) break;
+    first.push_back(d);
+    queue.slot_index.push_back(id);
+  }
+  if (first.empty()) return;
+  const std::vector<const std::vector<double>*> cold(first.size(), nullptr);
+  std::vector<CaseResult> slot_results;
+  if (problem.precision == ANU_PRECISION_FP32)
+    run_cases_t<float>(problem, first, options, cold, cold, &slot_results, start_time,
+                       problem.unit_scaling, nullptr, nullptr, &queue);
+  else
+    run_cases_t<double>(problem, first, options, cold, cold, &slot_results, start_time,
+                        problem.unit_scaling, nullptr, nullptr, &queue);
+  // Cases taken from the source that the time limit (or a stop request) kept
+  // from ever starting.
+  for (size_t i = queue.next; i < queue.pending.size(); ++i) {
+    CaseResult r;
+    r.r.status = ANU_PDHG_TIME_LIMIT;
+    set_message(&r.r, "not started: the time limit ended the stack first");
+    r.x.assign(problem.n, 0.0);
+    r.y.assign(problem.m, 0.0);
+    r.r.matrix_norm_estimate = problem.matrix_norm;
+    deliver(queue.pending_index[i], r);
+  }
+}
+
 }  // namespace anu
 
 // =============================================================== C ABI
@@ -2533,6 +2592,9 @@ struct anu_pdhg {
 
 struct anu_pdhg_batch {
   std::unique_ptr<anu::Problem> problem;
+  // The base LP's vectors: what a streamed case starts from.
+  std::vector<double> base_c, base_q, base_lower, base_upper;
+  double objective_scale = 1.0, objective_offset = 0.0;
   // A second problem on its own stream (same scaled matrix): larger stacks
   // run as two half-stacks at once, one per problem.
   std::unique_ptr<anu::Problem> twin;
@@ -2757,6 +2819,12 @@ int anu_pdhg_batch_create(const anu_lp* base, int32_t num_cases, const double* c
         !anu::stack_runs_persistent(*h->problem, std::min(num_cases, anu::kMaxCasesPerRun),
                                     *options))
       h->twin = anu::clone_problem(*h->problem);
+    h->base_c.assign(base->c, base->c + n);
+    h->base_q.assign(base->q, base->q + m);
+    h->base_lower.assign(base->lower, base->lower + n);
+    h->base_upper.assign(base->upper, base->upper + n);
+    h->objective_scale = base->objective_scale;
+    h->objective_offset = base->objective_offset;
     h->cases.reserve(num_cases);
     for (int32_t k = 0; k < num_cases; ++k) {
       h->cases.push_back(anu::make_case(
@@ -2772,6 +2840,47 @@ int anu_pdhg_batch_create(const anu_lp* base, int32_t num_cases, const double* c
 
 int anu_pdhg_batch_solve(anu_pdhg_batch* h, double* x, double* y, anu_pdhg_result* results) {
   return anu_pdhg_batch_solve_warm(h, nullptr, nullptr, x, y, results);
+}
+
+int anu_pdhg_batch_stream(anu_pdhg_batch* h, int32_t slots, anu_pdhg_case_source source,
+                          anu_pdhg_case_sink sink, void* user) {
+  return guarded([&] {
+    if (h == nullptr || source == nullptr || sink == nullptr)
+      throw Error(ANU_ERR_INVALID, "null argument");
+    if (slots < 1 || slots > anu::kMaxCasesPerRun)
+      throw Error(ANU_ERR_INVALID, "slots must be 1 to " + std::to_string(anu::kMaxCasesPerRun));
+    const double start = anu::now_seconds();
+    const int32_t n = h->problem->n, m = h->problem->m;
+    // Streamed cases live until the stream ends: admitted slots point at them.
+    std::deque<anu::CaseData> owned;
+    std::vector<double> c, q, lo, up;
+    auto next_case = [&](int32_t* id) -> const anu::CaseData* {
+      c = h->base_c;
+      q = h->base_q;
+      lo = h->base_lower;
+      up = h->base_upper;
+      int32_t case_id = -1;
+      if (source(user, &case_id, c.data(), q.data(), lo.data(), up.data()) == 0) return nullptr;
+      for (int32_t j = 0; j < n; ++j)
+        if (lo[j] > up[j])
+          throw Error(ANU_ERR_INVALID, "empty bound interval in streamed case " +
+                                           std::to_string(case_id));
+      for (int32_t i = 0; i < m; ++i)
+        if (!std::isfinite(q[i]))
+          throw Error(ANU_ERR_INVALID, "rhs is not finite in streamed case " +
+                                           std::to_string(case_id));
+      owned.push_back(anu::make_case(*h->problem, c.data(), q.data(), lo.data(), up.data(),
+                                     h->objective_scale, h->objective_offset));
+      *id = case_id;
+      return &owned.back();
+    };
+    auto deliver = [&](int32_t id, anu::CaseResult& cr) {
+      anu_pdhg_result r;
+      fill_result(*h->problem, cr, h->scaling_seconds, h->norm_seconds, &r);
+      sink(user, id, cr.x.data(), cr.y.data(), &r);
+    };
+    anu::run_cases_streaming(*h->problem, slots, h->options, next_case, deliver, start);
+  });
 }
 
 int anu_pdhg_batch_solve_warm(anu_pdhg_batch* h, const double* warm_x, const double* warm_y,

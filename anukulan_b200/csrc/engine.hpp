@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <functional>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -272,6 +273,17 @@ void run_cases_rolling(Problem& problem, const std::vector<const CaseData*>& cas
                        const std::vector<const std::vector<double>*>& warm_x,
                        const std::vector<const std::vector<double>*>& warm_y,
                        std::vector<CaseResult>* results, double start_time);
+
+// A streaming case stack of at most `slots` cases on `problem`. next_case
+// gives the next case (its id through the argument) or null when it has none
+// now; it is asked for the first cases, and again whenever a slot frees at a
+// termination check and nothing is waiting. deliver takes each case's result
+// as the case retires, on the calling thread, before the freed slot is
+// refilled, so it may decide what next_case hands out. Cases start cold.
+void run_cases_streaming(Problem& problem, int slots, const anu_pdhg_options& options,
+                         const std::function<const CaseData*(int32_t*)>& next_case,
+                         const std::function<void(int32_t, CaseResult&)>& deliver,
+                         double start_time);
 
 // ||K~|| by power iteration on the device, FP64 (pdhg.cpp:223-282).
 double device_matrix_norm(Problem& p, int iterations, double tolerance);

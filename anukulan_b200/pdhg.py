@@ -38,7 +38,7 @@ EXPORTS = (
     "anu_backend_step_size_terms", "anu_backend_convergence_terms",
     "anu_backend_convergence_terms_noalloc",
     "anu_pdhg_batch_create", "anu_pdhg_batch_solve", "anu_pdhg_batch_solve_warm",
-    "anu_pdhg_batch_destroy",
+    "anu_pdhg_batch_destroy", "anu_pdhg_batch_stream",
     "anu_pdhg_packed_create", "anu_pdhg_packed_solve", "anu_pdhg_packed_workers",
     "anu_pdhg_packed_destroy",
     "anu_pdhg_unrolled_create", "anu_pdhg_unrolled_step_sizes", "anu_pdhg_forward_unrolled",
@@ -92,6 +92,8 @@ def lib():
                                              _P(C.c_double), _P(C.c_double),
                                              _P(anu_pdhg_result)])
     d("anu_pdhg_batch_destroy", None, [C.c_void_p])
+    d("anu_pdhg_batch_stream", C.c_int, [C.c_void_p, C.c_int32, CASE_SOURCE, CASE_SINK,
+                                         C.c_void_p])
     d("anu_pdhg_packed_create", C.c_int, [C.c_int32, _P(anu_lp), _P(anu_pdhg_options),
                                           C.c_int32, _P(C.c_void_p)])
     d("anu_pdhg_packed_solve", C.c_int, [C.c_void_p, _P(_P(C.c_double)), _P(_P(C.c_double)),
@@ -236,6 +238,13 @@ def estimate_matrix_norm(lp: StandardLp, iterations: int = 200, tolerance: float
     return out.value
 
 
+# anu_pdhg_case_source / anu_pdhg_case_sink.
+CASE_SOURCE = C.CFUNCTYPE(C.c_int32, C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_double),
+                          C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double))
+CASE_SINK = C.CFUNCTYPE(None, C.c_void_p, C.c_int32, C.POINTER(C.c_double),
+                        C.POINTER(C.c_double), C.POINTER(anu_pdhg_result))
+
+
 class CaseStackSolver:
     """A case stack sharing one matrix (``anu_pdhg_batch_*``)."""
 
@@ -269,6 +278,47 @@ class CaseStackSolver:
             check(lib().anu_pdhg_batch_solve_warm(self._h, f64_ptr(wx), f64_ptr(wy), f64_ptr(x),
                                                   f64_ptr(y), res))
         return [PdhgResult.from_c(res[k], x[k], y[k]) for k in range(K)]
+
+    def stream(self, source, sink, slots: int = 64):
+        """A streaming stack (``anu_pdhg_batch_stream``). `source(case)`
+        fills the next case and returns its id, or returns None when it has
+        none now; `case` has writable arrays c, q, lower and upper holding the
+        base LP's vectors. `sink(case_id, result)` receives each result as its
+        case retires, before the freed slot is refilled."""
+        n, m = self._cl.n, self._cl.m
+        failure = []
+
+        class Case:
+            pass
+
+        def src(_user, case_id, c, q, lower, upper):
+            try:
+                case = Case()
+                case.c = np.ctypeslib.as_array(c, shape=(n,))
+                case.q = np.ctypeslib.as_array(q, shape=(m,))
+                case.lower = np.ctypeslib.as_array(lower, shape=(n,))
+                case.upper = np.ctypeslib.as_array(upper, shape=(n,))
+                k = source(case)
+                if k is None:
+                    return 0
+                case_id[0] = int(k)
+                return 1
+            except BaseException as e:  # no exception may cross the C boundary
+                failure.append(e)
+                return 0
+
+        def snk(_user, case_id, x, y, res):
+            try:
+                sink(int(case_id), PdhgResult.from_c(
+                    res.contents, np.ctypeslib.as_array(x, shape=(n,)).copy(),
+                    np.ctypeslib.as_array(y, shape=(m,)).copy()))
+            except BaseException as e:
+                failure.append(e)
+
+        cb_src, cb_snk = CASE_SOURCE(src), CASE_SINK(snk)
+        check(lib().anu_pdhg_batch_stream(self._h, int(slots), cb_src, cb_snk, None))
+        if failure:
+            raise failure[0]
 
     def close(self):
         if self._h:

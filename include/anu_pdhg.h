@@ -413,6 +413,32 @@ int anu_pdhg_batch_solve_warm(anu_pdhg_batch* handle, const double* warm_x,
                               anu_pdhg_result* results);
 void anu_pdhg_batch_destroy(anu_pdhg_batch* handle);
 
+/* A streaming case stack: cases admitted as the caller produces them and
+ * results handed back as cases retire. The reference has no counterpart;
+ * it is the admit / retire / results cycle of a rolling stack (the cases of
+ * anu_pdhg_batch_create are not used), for callers whose next cases depend on
+ * earlier results, such as the open nodes of branch and bound
+ * (src/anukulan/branch_and_bound.cpp:532-565).
+ *
+ * - source: fills the next case and returns 1, or returns 0 when it has none
+ *   now. Its arrays (c: n, q: m, lower and upper: n) arrive holding the base
+ *   LP's vectors, so it writes only what its case changes; *case_id is the
+ *   caller's label for the case. It is asked for up to `slots` cases at the
+ *   start, which fixes the stack's width, and again whenever a case retires at
+ *   a termination check and no case is waiting.
+ * - sink: receives each case's x (n), y (m) and result when the case retires,
+ *   before its slot is refilled, so it may decide what the source hands out.
+ * - Both run on the calling thread. Every case starts cold and runs the
+ *   iteration it would run alone (its counts start at its admission).
+ * - slots: 1 to 64. The call returns when the source has nothing more and
+ *   every admitted case has retired. */
+typedef int32_t (*anu_pdhg_case_source)(void* user, int32_t* case_id, double* c, double* q,
+                                        double* lower, double* upper);
+typedef void (*anu_pdhg_case_sink)(void* user, int32_t case_id, const double* x,
+                                   const double* y, const anu_pdhg_result* result);
+int anu_pdhg_batch_stream(anu_pdhg_batch* handle, int32_t slots, anu_pdhg_case_source source,
+                          anu_pdhg_case_sink sink, void* user);
+
 /* ------------------------------------------------------ packed batches
  * Independent LPs of different shapes solved together on one GPU. No
  * counterpart in the reference, whose callers loop solve_pdhg over such a
