@@ -202,6 +202,36 @@ def ref_b200_backend_name() -> str:
     return buf.value.decode()
 
 
+def ref_pipeline(model, options=None, use_presolve: bool = True, engine: bool = True, **kw):
+    """anu_b200::solve_model_pdhg (include/anu_b200_pipeline.hpp): the
+    reference's presolve -> standard form -> solve_pdhg -> postsolve on a
+    :class:`Model`, with the PDHG step on the engine (`engine`) or on the
+    reference's cpu_backend(). Returns (rc, result, x, y, info) with info =
+    worst violation, relative row violation, dual exact, presolve status."""
+    lib = ref_b200_lib()
+    fn = getattr(lib, "ref_pipeline_solve")
+    fn.restype = C.c_int
+    a = model.constraints
+    m, n = a.rows, a.cols
+    i32 = lambda arr: np.ascontiguousarray(arr, np.int32)
+    f64 = lambda arr: np.ascontiguousarray(arr, np.float64)
+    keep = [i32(a.start), i32(a.index), f64(a.value), f64(model.objective),
+            f64(model.row_lower), f64(model.row_upper), f64(model.col_lower),
+            f64(model.col_upper)]
+    ip = lambda arr: arr.ctypes.data_as(_P(C.c_int32))
+    o = _opts(options, **kw)
+    x = np.zeros(max(n, 1))
+    y = np.zeros(max(m, 1))
+    info = np.zeros(4)
+    r = anu_pdhg_result()
+    rc = fn(C.c_int32(m), C.c_int32(n), C.c_int32(a.nnz), ip(keep[0]), ip(keep[1]),
+            f64_ptr(keep[2]), f64_ptr(keep[3]), f64_ptr(keep[4]), f64_ptr(keep[5]),
+            f64_ptr(keep[6]), f64_ptr(keep[7]), C.c_int(int(model.maximize)),
+            C.c_double(float(model.objective_offset)), C.byref(o), C.c_int(int(use_presolve)),
+            C.c_int(0 if engine else 1), f64_ptr(x), f64_ptr(y), C.byref(r), f64_ptr(info))
+    return rc, PdhgResult.from_c(r, x[:n].copy(), y[:m].copy()), x[:n].copy(), y[:m].copy(), info
+
+
 def ref_b200_solve(lp: StandardLp, options=None, **kw) -> PdhgResult:
     """The reference's own solve_pdhg, unchanged, with the engine's kernels
     under its LinAlgBackend seam (FP64, one seam call per launch)."""

@@ -1,0 +1,36 @@
+"""The reference's first-order pipeline (presolve -> standard form ->
+solve_pdhg -> postsolve) with its PDHG step on the engine's kernels, through
+anu_b200::solve_model_pdhg and the LinAlgBackend adapter, against the same
+pipeline on the reference's cpu_backend(). The FP64 seam keeps every product
+entry's summation order; only reductions differ, so both reach the same
+status and iteration counts within a few check periods. Relative KKT 1e-8
+bounds the gap against 1 + |primal| + |dual|, about twice the objective, so
+the objective is held to 5e-8 of the HiGHS optimum.
+"""
+import pytest
+
+import oracle
+from anukulan_b200 import lpgen
+from anukulan_b200.abi import OPTIMAL
+from anukulan_b200.model import to_standard_form
+from golden.make_simplex_golden import highs_objective
+
+pytestmark = [
+    pytest.mark.gpu,
+    pytest.mark.skipif(not oracle.have_reference_b200(),
+                       reason="oracle/_ref adapter build absent"),
+]
+
+
+@pytest.mark.parametrize("use_presolve", [True, False])
+def test_pipeline_on_engine_matches_cpu_backend(engine, use_presolve):
+    model, _ = lpgen.refinery_model(24, lpgen.BASE_SEED + 2)
+    optimum = highs_objective(to_standard_form(model).lp)[1]
+    kw = dict(use_presolve=use_presolve, tolerance=1e-8)
+    rc_g, g, xg, yg, ig = oracle.ref_pipeline(model, engine=True, **kw)
+    rc_c, c, xc, yc, ic = oracle.ref_pipeline(model, engine=False, **kw)
+    assert rc_g == rc_c == 0, (g.message, c.message)
+    assert g.status == c.status == OPTIMAL, g.message
+    assert abs(g.iterations - c.iterations) <= 200
+    assert abs(g.objective - optimum) <= 5e-8 * abs(optimum)
+    assert ig[1] <= 1e-7
