@@ -2752,6 +2752,22 @@ int anu_pdhg_solve(const anu_lp* lp, const anu_pdhg_options* options, const doub
   return rc;
 }
 
+int anu_locality_relabel(const anu_lp* lp, int32_t* row_old, int32_t* col_old) {
+  return guarded([&] {
+    if (lp == nullptr || (lp->k.rows > 0 && row_old == nullptr) ||
+        (lp->k.cols > 0 && col_old == nullptr))
+      throw Error(ANU_ERR_INVALID, "null argument");
+    const std::string e = anu::validate_csr(lp->k.rows, lp->k.cols, lp->k.nnz, lp->k.start,
+                                            lp->k.index);
+    if (!e.empty()) throw Error(ANU_ERR_INVALID, "invalid matrix: " + e);
+    if (lp->num_equalities < 0 || lp->num_equalities > lp->k.rows)
+      throw Error(ANU_ERR_INVALID, "num_equalities out of range");
+    const anu::Relabel r = anu::locality_relabel(*lp);
+    for (int32_t i = 0; i < lp->k.rows; ++i) row_old[i] = r.empty() ? i : r.row_old[i];
+    for (int32_t j = 0; j < lp->k.cols; ++j) col_old[j] = r.empty() ? j : r.col_old[j];
+  });
+}
+
 int anu_estimate_matrix_norm(const anu_lp* lp, int32_t iterations, double tolerance,
                              double* norm) {
   return guarded([&] {

@@ -29,7 +29,7 @@ EXPORTS = (
     "anu_pdhg_version", "anu_pdhg_default_options", "anu_last_error", "anu_device_count",
     "anu_release_cached_memory",
     "anu_pdhg_solve", "anu_pdhg_create", "anu_pdhg_run", "anu_pdhg_destroy",
-    "anu_evaluate_residual", "anu_estimate_matrix_norm",
+    "anu_evaluate_residual", "anu_estimate_matrix_norm", "anu_locality_relabel",
     "anu_backend_allocate", "anu_backend_deallocate", "anu_backend_upload",
     "anu_backend_download", "anu_backend_fill", "anu_backend_copy", "anu_backend_prepare",
     "anu_backend_release", "anu_backend_multiply", "anu_backend_dot", "anu_backend_two_norm",
@@ -92,6 +92,7 @@ def lib():
                                              _P(C.c_double), _P(C.c_double),
                                              _P(anu_pdhg_result)])
     d("anu_pdhg_batch_destroy", None, [C.c_void_p])
+    d("anu_locality_relabel", C.c_int, [_P(anu_lp), _P(C.c_int32), _P(C.c_int32)])
     d("anu_pdhg_batch_stream", C.c_int, [C.c_void_p, C.c_int32, CASE_SOURCE, CASE_SINK,
                                          C.c_void_p])
     d("anu_pdhg_packed_create", C.c_int, [C.c_int32, _P(anu_lp), _P(anu_pdhg_options),
@@ -172,6 +173,17 @@ def _options(options: Optional[anu_pdhg_options], kw) -> anu_pdhg_options:
             setattr(o, k, int(v) if isinstance(v, bool) else v)
         return o
     return options
+
+
+def locality_relabel(lp: StandardLp):
+    """``anu_locality_relabel``: (row_old, col_old), the relabelling that
+    options.locality_order applies (new -> original). Host only."""
+    cl = CLp(lp)
+    row_old = np.zeros(max(cl.m, 1), np.int32)
+    col_old = np.zeros(max(cl.n, 1), np.int32)
+    check(lib().anu_locality_relabel(cl.ref(), row_old.ctypes.data_as(C.POINTER(C.c_int32)),
+                                     col_old.ctypes.data_as(C.POINTER(C.c_int32))))
+    return row_old[:cl.m].copy(), col_old[:cl.n].copy()
 
 
 def solve_pdhg(lp: StandardLp, options: Optional[anu_pdhg_options] = None,

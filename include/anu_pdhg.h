@@ -297,6 +297,16 @@ void anu_pdhg_destroy(anu_pdhg* handle);
 int anu_evaluate_residual(const anu_lp* lp, const double* x, const double* y,
                           anu_pdhg_residual* out);
 
+/* The relabelling options.locality_order applies (no counterpart in the
+ * reference), computed on the host without a device: row_old[r] (m entries)
+ * is the original row of relabelled row r, col_old[c] (n entries) the
+ * original column of relabelled column c. Rows are ordered by decreasing
+ * length within the equality block and within the inequality block (ties
+ * keep their order); columns by the first relabelled row they appear in
+ * (ties keep their order, empty columns last). An LP without rows or columns
+ * gets the identity. */
+int anu_locality_relabel(const anu_lp* lp, int32_t* row_old, int32_t* col_old);
+
 /* estimate_matrix_norm, src/anukulan/pdhg.hpp:580 / pdhg.cpp:223-282: power
  * iteration on K'K on the device, FP64. */
 int anu_estimate_matrix_norm(const anu_lp* lp, int32_t iterations,
