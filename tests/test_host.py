@@ -210,3 +210,15 @@ def test_node_relaxation_rule():
     inf = NodeRelaxation(result(abi.PRIMAL_INFEASIBLE, 0.0, 0.0))
     assert inf.proved_infeasible and not inf.optimal
     assert not NodeRelaxation(result(abi.ITERATION_LIMIT, 1.0, 0.0)).optimal
+
+
+def test_node_relaxations_reject_bad_bounds():
+    """Node bounds are (nodes x columns), the same shape for lower and
+    upper; anything else is refused before the engine is asked."""
+    from anukulan_b200.pdhg import solve_node_relaxations
+    lp = lp_cases.standard(lp_cases.wyndor())
+    n = lp.num_cols
+    with pytest.raises(ValueError):
+        solve_node_relaxations(lp, np.zeros((2, n)), np.ones((3, n)))
+    with pytest.raises(ValueError):
+        solve_node_relaxations(lp, np.zeros((2, n + 1)), np.ones((2, n + 1)))
