@@ -3,15 +3,23 @@ solve_pdhg -> postsolve) with its PDHG step on the engine's kernels, through
 anu_b200::solve_model_pdhg and the LinAlgBackend adapter, against the same
 pipeline on the reference's cpu_backend(). The FP64 seam keeps every product
 entry's summation order; only reductions differ, so both reach the same
-status and iteration counts within a few check periods. Relative KKT 1e-8
-bounds the gap against 1 + |primal| + |dual|, about twice the objective, so
-the objective is held to 5e-8 of the HiGHS optimum.
+iteration counts within a few check periods. Relative KKT 1e-8 bounds the
+gap against 1 + |primal| + |dual|, about twice the objective, so the
+objective is held to 5e-8 of the HiGHS optimum.
+
+With presolve, the CLI's rule holds the original model's relative row
+violation to the tolerance. PDHG stops right at the tolerance on the reduced
+model, and on this model the original's violation then lands within a few
+percent of it (8.2e-9 at 1e-8 on the CPU backend), so either backend may end
+OPTIMAL or flagged as a numerical error by that rule. The test holds the
+violation to twice the tolerance and the status to one of the two. Without
+presolve the status is PDHG's own and must be OPTIMAL on both.
 """
 import pytest
 
 import oracle
 from anukulan_b200 import lpgen
-from anukulan_b200.abi import OPTIMAL
+from anukulan_b200.abi import NUMERICAL_ERROR, OPTIMAL
 from anukulan_b200.model import to_standard_form
 from golden.make_simplex_golden import highs_objective
 
@@ -30,7 +38,11 @@ def test_pipeline_on_engine_matches_cpu_backend(engine, use_presolve):
     rc_g, g, xg, yg, ig = oracle.ref_pipeline(model, engine=True, **kw)
     rc_c, c, xc, yc, ic = oracle.ref_pipeline(model, engine=False, **kw)
     assert rc_g == rc_c == 0, (g.message, c.message)
-    assert g.status == c.status == OPTIMAL, g.message
+    if use_presolve:
+        assert g.status in (OPTIMAL, NUMERICAL_ERROR), g.message
+        assert c.status in (OPTIMAL, NUMERICAL_ERROR), c.message
+    else:
+        assert g.status == c.status == OPTIMAL, g.message
     assert abs(g.iterations - c.iterations) <= 200
     assert abs(g.objective - optimum) <= 5e-8 * abs(optimum)
-    assert ig[1] <= 1e-7
+    assert ig[1] <= 2e-8
