@@ -11,6 +11,8 @@ from __future__ import annotations
 
 from typing import Callable, List, Optional
 
+import numpy as np
+
 from .lpgen import CaseStack
 
 
@@ -48,6 +50,38 @@ def solve_stack_sharded(stack: CaseStack, solve: Optional[Callable] = None, grou
     local = solve(sub_stack(stack, mine)) if len(mine) else []
     if len(local) != len(mine):
         raise RuntimeError("the solver returned a result count different from its cases")
+    gathered: List = [None] * world
+    dist.all_gather_object(gathered, list(local), group=group)
+    out: List = []
+    for part in gathered:
+        out.extend(part)
+    return out
+
+
+def solve_nodes_sharded(lp, lower, upper, solve: Optional[Callable] = None, group=None,
+                        **kw) -> List:
+    """Branch-and-bound node relaxations across the ranks of `group`: the
+    nodes' bounds (nodes x columns) are sliced like a case stack, each rank
+    solves its slice as one stack, and one all-gather gives every rank every
+    node's result in node order. `solve` maps (lp, lower, upper) to a list of
+    results (default: pdhg.solve_node_relaxations with `kw` as options)."""
+    import torch.distributed as dist
+    if solve is None:
+        from .pdhg import solve_node_relaxations
+
+        def solve(base, lo, up):
+            return solve_node_relaxations(base, lo, up, **kw)
+    lower = np.atleast_2d(np.asarray(lower, np.float64))
+    upper = np.atleast_2d(np.asarray(upper, np.float64))
+    if lower.shape != upper.shape:
+        raise ValueError("node bounds must have the same shape")
+    world = dist.get_world_size(group)
+    rank = dist.get_rank(group)
+    mine = case_shard(lower.shape[0], rank, world)
+    idx = list(mine)
+    local = solve(lp, lower[idx], upper[idx]) if idx else []
+    if len(local) != len(idx):
+        raise RuntimeError("the solver returned a result count different from its nodes")
     gathered: List = [None] * world
     dist.all_gather_object(gathered, list(local), group=group)
     out: List = []

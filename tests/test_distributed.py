@@ -74,3 +74,41 @@ def test_case_shard_partition():
             assert covered == list(range(n))
     with pytest.raises(ValueError):
         D.case_shard(4, 2, 2)
+
+
+def _node_worker(rank, world, port, num_nodes, out):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        base = _stack(1).base
+        lower = np.tile(base.lower, (num_nodes, 1))
+        upper = np.tile(base.upper, (num_nodes, 1))
+        upper[:, 0] = np.arange(num_nodes)          # node k: column 0 capped at k
+        res = D.solve_nodes_sharded(
+            base, lower, upper, solve=lambda lp, lo, up: [(rank, float(u[0])) for u in up])
+        out.put((rank, res))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("num_nodes", [9, 1])
+def test_sharded_nodes_two_ranks(num_nodes):
+    """Node relaxations shard like a case stack: every rank ends with every
+    node's result once, in node order, each rank having solved its slice."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_node_worker, args=(r, 2, port, num_nodes, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = dict(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for rank in (0, 1):
+        res = got[rank]
+        assert [u for _, u in res] == [float(k) for k in range(num_nodes)]
+        owners = [r for r, _ in res]
+        for r in (0, 1):
+            assert owners.count(r) == len(D.case_shard(num_nodes, r, 2))
