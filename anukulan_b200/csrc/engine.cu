@@ -334,7 +334,8 @@ __global__ void normalize_kernel(int32_t n, const double* __restrict__ in,
                                  const double* __restrict__ sumsq, double* __restrict__ out,
                                  double* __restrict__ estimates, int32_t slot) {
   const double next = sqrt(sumsq[0]);
-  for (int32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n;
+       j += (int64_t)gridDim.x * blockDim.x)
     out[j] = next != 0.0 ? in[j] / next : 0.0;
   if (blockIdx.x == 0 && threadIdx.x == 0) estimates[slot] = next;
 }

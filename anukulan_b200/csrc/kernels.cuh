@@ -801,7 +801,8 @@ __global__ void __launch_bounds__(kThreads) terms_stage1(int32_t len, int32_t K,
   double acc[CPL][NT];
 #pragma unroll
   for (int c = 0; c < CPL; ++c) Terms::init(acc[c]);
-  for (int32_t r = blockIdx.x * kGroups + group; r < len; r += gridDim.x * kGroups) {
+  for (int64_t r = blockIdx.x * (int64_t)kGroups + group; r < len;
+       r += (int64_t)gridDim.x * kGroups) {
 #pragma unroll
     for (int c = 0; c < CPL; ++c) {
       const int32_t cs = lane + c * L;

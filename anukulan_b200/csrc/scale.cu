@@ -25,7 +25,8 @@ namespace {
 
 __global__ void row_norms_kernel(int32_t rows, const int32_t* __restrict__ start,
                                  const double* __restrict__ value, int one, double* __restrict__ out) {
-  for (int32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x) {
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < rows;
+       r += (int64_t)gridDim.x * blockDim.x) {
     double acc = 0.0;
     const int32_t end = start[r + 1];
     for (int32_t e = start[r]; e < end; ++e) {
@@ -39,7 +40,8 @@ __global__ void row_norms_kernel(int32_t rows, const int32_t* __restrict__ start
 __global__ void col_norms_kernel(int32_t cols, const int32_t* __restrict__ tstart,
                                  const int32_t* __restrict__ pos, const double* __restrict__ value,
                                  int one, double* __restrict__ out) {
-  for (int32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < cols; c += gridDim.x * blockDim.x) {
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < cols;
+       c += (int64_t)gridDim.x * blockDim.x) {
     double acc = 0.0;
     const int32_t end = tstart[c + 1];
     for (int32_t t = tstart[c]; t < end; ++t) {
@@ -51,7 +53,8 @@ __global__ void col_norms_kernel(int32_t cols, const int32_t* __restrict__ tstar
 }
 
 __global__ void factors_kernel(int32_t len, const double* __restrict__ norm, double* __restrict__ d) {
-  for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < len; i += gridDim.x * blockDim.x) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < len;
+       i += (int64_t)gridDim.x * blockDim.x) {
     const double v = norm[i];
     d[i] = v > 0.0 ? __ddiv_rn(1.0, __dsqrt_rn(v)) : 1.0;
   }
@@ -61,7 +64,8 @@ __global__ void scale_values_kernel(int32_t nnz, const int32_t* __restrict__ row
                                     const int32_t* __restrict__ index,
                                     const double* __restrict__ d1, const double* __restrict__ d2,
                                     double* __restrict__ value) {
-  for (int32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < nnz; e += gridDim.x * blockDim.x)
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nnz;
+       e += (int64_t)gridDim.x * blockDim.x)
     value[e] = __dmul_rn(__dmul_rn(value[e], d1[row_of[e]]), d2[index[e]]);
 }
 

@@ -370,21 +370,23 @@ int anu_backend_convergence_terms(int64_t n, int64_t m, const double* c,
  * counterpart in the reference.
  *
  * It is for hosts that may not call cudaMalloc: a plugin inside an application
- * that owns the device memory pool, a process whose allocations all go
- * through another runtime's allocator, or code that runs while such an
- * application holds a stream capture. The caller passes inputs and outputs
- * exactly as for anu_backend_convergence_terms and gets the same 7 terms.
+ * that owns the device memory pool, or a process whose allocations all go
+ * through another runtime's allocator. Such a host can hand over its own
+ * input and output arrays, but a library that allocates behind its back
+ * breaks its accounting. The caller passes inputs and outputs exactly as for
+ * anu_backend_convergence_terms and gets the same 7 terms.
  *
  * - Scratch: the partial sums live in one fixed array in the library's device
  *   image, 42,768 bytes, which every GPU that loads the library holds until
  *   the process exits.
- * - Limits: n and m up to 2^31-1. Larger or negative lengths return
- *   ANU_ERR_INVALID with a message.
+ * - Limits: n and m up to 2^31-1 (every loop index is 64-bit). Larger or
+ *   negative lengths return ANU_ERR_INVALID with a message.
  * - Set-up: the first call on each device looks the array up on that device
- *   (cudaGetSymbolAddress). Make that first call before any stream capture
- *   begins.
- * - Stream: work runs on the legacy default stream, and the call returns when
- *   it is done.
+ *   (cudaGetSymbolAddress) and caches the address. Make that first call
+ *   before any stream capture begins.
+ * - Stream: work runs on the legacy default stream, which waits for and
+ *   blocks every stream created without cudaStreamNonBlocking, and the call
+ *   returns when its work is done.
  * - Sharing: every call shares the one array. Calls that overlap on the same
  *   GPU (from several host threads, say) race on it and must be serialised by
  *   the caller. */

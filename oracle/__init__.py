@@ -36,7 +36,9 @@ REF_CUDA_SO = os.path.join(HERE, "_ref", "libanuref_cuda.so")
 REF_B200_SO = os.path.join(HERE, "_ref", "libanuref_b200.so")
 REF_B200_TEST_BACKEND = os.path.join(HERE, "_ref", "test_backend_b200")
 REF_B200_TEST_PDHG = os.path.join(HERE, "_ref", "test_pdhg_b200")
-REF_SRC = "/root/reference/src/anukulan/pdhg.cpp"
+# The reference checkout is named by the caller of build() or by the
+# ANUKULAN_REFERENCE environment variable; nothing here assumes where it is.
+REF_ENV = "ANUKULAN_REFERENCE"
 
 _oracle = None
 _ref = None
@@ -46,15 +48,30 @@ _ref_b200 = None
 _P = C.POINTER
 
 
-def build(with_reference: Optional[bool] = None) -> None:
-    """Builds liboracle.so, and _ref/libanuref.so and _ref/libanuref_cuda.so
-    when the reference sources are present (or `with_reference` is True)."""
+def reference_root(root: Optional[str] = None) -> Optional[str]:
+    """The reference checkout to build from: `root`, else $ANUKULAN_REFERENCE,
+    kept only when it holds the reference's sources (src/anukulan/pdhg.cpp)."""
+    root = root or os.environ.get(REF_ENV) or None
+    if root and os.path.exists(os.path.join(root, "src", "anukulan", "pdhg.cpp")):
+        return os.path.abspath(root)
+    return None
+
+
+def build(with_reference: Optional[bool] = None, root: Optional[str] = None) -> None:
+    """Builds liboracle.so, and the reference builds under _ref/ when a
+    reference checkout is given (`root` or $ANUKULAN_REFERENCE) and holds the
+    sources. `with_reference=False` skips them; True requires them."""
     import subprocess
     subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
-    if with_reference is None:
-        with_reference = os.path.exists(REF_SRC)
-    if with_reference:
-        subprocess.run(["make", "-s", "-j8", "-C", HERE, "ref", "ref_cuda", "ref_b200"], check=True)
+    if with_reference is False:
+        return
+    ref = reference_root(root)
+    if ref is None:
+        if with_reference:
+            raise RuntimeError(f"no reference checkout: pass root= or set {REF_ENV}")
+        return
+    subprocess.run(["make", "-s", "-j8", "-C", HERE, f"REF={ref}", "ref", "ref_cuda", "ref_b200"],
+                   check=True)
 
 
 def _declare(lib, name, restype, argtypes):

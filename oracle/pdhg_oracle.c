@@ -1160,7 +1160,7 @@ static void solve(const olp* original, const anu_pdhg_options* options, const do
           set_message(result, "feasibility polished");
         } else {
           char buf[sizeof(result->message)];
-          snprintf(buf, sizeof(buf), "%s, feasibility polished", result->message);
+          snprintf(buf, sizeof(buf), "%.130s, feasibility polished", result->message);
           set_message(result, buf);
         }
       }
