@@ -18,8 +18,10 @@
 #include <deque>
 #include <functional>
 #include <map>
+#include <memory>
 #include <numeric>
 #include <thread>
+#include <unordered_map>
 #include <utility>
 
 #include "engine.hpp"
@@ -935,6 +937,9 @@ struct AdmissionQueue {
   // appends to it and returns false when it has none now.
   std::function<void(int32_t, CaseResult&)> deliver;
   std::function<bool(AdmissionQueue&)> refill;
+  // Streaming stacks only: hands back a case whose slot has just been
+  // refilled. Until then a retired slot still points at its case's vectors.
+  std::function<void(const CaseData*)> release;
 };
 
 // One case's column of a case-interleaved device array (element (row, k) at
@@ -1878,6 +1883,7 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
   // case-interleaved device array start over as at the start of a solve.
   auto admit = [&](int k, int32_t index, const CaseData* d, const std::vector<double>* wx,
                    const std::vector<double>* wy) {
+    const CaseData* outgoing = cases[k];
     cases[k] = d;
     queue->slot_index[k] = index;
     origin[k] = iteration;
@@ -1977,6 +1983,8 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
     }
     // The staged host columns stay alive until the copies are done.
     ANU_CUDA(cudaStreamSynchronize(st));
+    // Nothing in this run points at the outgoing case any more.
+    if (queue->release && outgoing != nullptr && outgoing != d) queue->release(outgoing);
   };
 
   while ((queue != nullptr || iteration < o.max_iterations) && any_active()) {
@@ -2493,6 +2501,7 @@ void run_cases_rolling(Problem& problem, const std::vector<const CaseData*>& cas
 void run_cases_streaming(Problem& problem, int slots, const anu_pdhg_options& options,
                          const std::function<const CaseData*(int32_t*)>& next_case,
                          const std::function<void(int32_t, CaseResult&)>& deliver,
+                         const std::function<void(const CaseData*)>& release,
                          double start_time) {
   ANU_CUDA(cudaSetDevice(problem.device));
   PoolScope scope(&problem.pool, problem.stream);
@@ -2500,6 +2509,7 @@ void run_cases_streaming(Problem& problem, int slots, const anu_pdhg_options& op
   std::vector<CaseResult> unused;
   queue.out = &unused;
   queue.deliver = deliver;
+  queue.release = release;
   queue.refill = [&next_case](AdmissionQueue& q) {
     int32_t id = -1;
     const CaseData* d = next_case(&id);
@@ -2868,8 +2878,10 @@ int anu_pdhg_batch_stream(anu_pdhg_batch* h, int32_t slots, anu_pdhg_case_source
       throw Error(ANU_ERR_INVALID, "slots must be 1 to " + std::to_string(anu::kMaxCasesPerRun));
     const double start = anu::now_seconds();
     const int32_t n = h->problem->n, m = h->problem->m;
-    // Streamed cases live until the stream ends: admitted slots point at them.
-    std::deque<anu::CaseData> owned;
+    // A streamed case lives until its slot takes the next case (the stack
+    // hands it back then) or the stream ends, so a long stream holds about
+    // `slots` cases on the host, not every case it has seen.
+    std::unordered_map<const anu::CaseData*, std::unique_ptr<anu::CaseData>> owned;
     std::vector<double> c, q, lo, up;
     auto next_case = [&](int32_t* id) -> const anu::CaseData* {
       c = h->base_c;
@@ -2886,17 +2898,21 @@ int anu_pdhg_batch_stream(anu_pdhg_batch* h, int32_t slots, anu_pdhg_case_source
         if (!std::isfinite(q[i]))
           throw Error(ANU_ERR_INVALID, "rhs is not finite in streamed case " +
                                            std::to_string(case_id));
-      owned.push_back(anu::make_case(*h->problem, c.data(), q.data(), lo.data(), up.data(),
-                                     h->objective_scale, h->objective_offset));
+      auto cd = std::make_unique<anu::CaseData>(anu::make_case(
+          *h->problem, c.data(), q.data(), lo.data(), up.data(), h->objective_scale,
+          h->objective_offset));
+      const anu::CaseData* ptr = cd.get();
+      owned.emplace(ptr, std::move(cd));
       *id = case_id;
-      return &owned.back();
+      return ptr;
     };
+    auto release = [&](const anu::CaseData* d) { owned.erase(d); };
     auto deliver = [&](int32_t id, anu::CaseResult& cr) {
       anu_pdhg_result r;
       fill_result(*h->problem, cr, h->scaling_seconds, h->norm_seconds, &r);
       sink(user, id, cr.x.data(), cr.y.data(), &r);
     };
-    anu::run_cases_streaming(*h->problem, slots, h->options, next_case, deliver, start);
+    anu::run_cases_streaming(*h->problem, slots, h->options, next_case, deliver, release, start);
   });
 }
 

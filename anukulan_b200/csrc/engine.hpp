@@ -280,9 +280,12 @@ void run_cases_rolling(Problem& problem, const std::vector<const CaseData*>& cas
 // termination check and nothing is waiting. deliver takes each case's result
 // as the case retires, on the calling thread, before the freed slot is
 // refilled, so it may decide what next_case hands out. Cases start cold.
+// release gets back each case whose slot has taken a new case; the stack no
+// longer reads it.
 void run_cases_streaming(Problem& problem, int slots, const anu_pdhg_options& options,
                          const std::function<const CaseData*(int32_t*)>& next_case,
                          const std::function<void(int32_t, CaseResult&)>& deliver,
+                         const std::function<void(const CaseData*)>& release,
                          double start_time);
 
 // ||K~|| by power iteration on the device, FP64 (pdhg.cpp:223-282).

@@ -209,6 +209,13 @@ def ref_b200_lib():
                  [C.c_void_p, _P(anu_pdhg_options), C.c_int, _P(C.c_double),
                   _P(C.c_double), _P(C.c_double), _P(C.c_double), _P(anu_pdhg_result)])
         _declare(lib, "ref_default_backend_name", C.c_int, [C.c_char_p, C.c_int])
+        _declare(lib, "ref_finish_simplex", C.c_int,
+                 [C.c_void_p, _P(C.c_double), _P(C.c_double), C.c_int, _P(C.c_double),
+                  _P(C.c_double), _P(C.c_double), _P(C.c_int32), _P(C.c_int32),
+                  _P(C.c_int32), _P(C.c_int32)])
+        _declare(lib, "ref_simplex_basis", C.c_int,
+                 [C.c_void_p, _P(C.c_int32), C.c_int32, _P(C.c_int32), C.c_int32,
+                  _P(C.c_int32), _P(C.c_int32), _P(C.c_int32), _P(C.c_int32), _P(C.c_double)])
         _ref_b200 = lib
     return _ref_b200
 
@@ -247,6 +254,145 @@ def ref_pipeline(model, options=None, use_presolve: bool = True, engine: bool = 
             C.c_double(float(model.objective_offset)), C.byref(o), C.c_int(int(use_presolve)),
             C.c_int(0 if engine else 1), f64_ptr(x), f64_ptr(y), C.byref(r), f64_ptr(info))
     return rc, PdhgResult.from_c(r, x[:n].copy(), y[:m].copy()), x[:n].copy(), y[:m].copy(), info
+
+
+SIMPLEX_STATUS_NAMES = {0: "optimal"}
+
+
+def ref_pipeline_crossover(model, options=None, use_presolve: bool = True, engine: bool = True,
+                           crossover_tolerance: float = 1e-4, **kw):
+    """anu_b200::solve_model_crossover (include/anu_b200_pipeline.hpp): the
+    CLI's `simplex --crossover` (app/anukulan_cli.cpp:574-636) on a
+    :class:`Model`, the PDHG seed on the engine (`engine`) or on cpu_backend().
+    Returns (rc, x, info) with info a dict: simplex status (0 optimal),
+    pivots, seeded, fell_back, seeded_pivots, seed_iterations, seed_status,
+    row_violation, objective, candidates, pushed, presolve_status."""
+    lib = ref_b200_lib()
+    fn = getattr(lib, "ref_pipeline_crossover")
+    fn.restype = C.c_int
+    a = model.constraints
+    m, n = a.rows, a.cols
+    i32 = lambda arr: np.ascontiguousarray(arr, np.int32)
+    f64 = lambda arr: np.ascontiguousarray(arr, np.float64)
+    keep = [i32(a.start), i32(a.index), f64(a.value), f64(model.objective),
+            f64(model.row_lower), f64(model.row_upper), f64(model.col_lower),
+            f64(model.col_upper)]
+    ip = lambda arr: arr.ctypes.data_as(_P(C.c_int32))
+    o = _opts(options, **kw)
+    x = np.zeros(max(n, 1))
+    info = np.zeros(12)
+    rc = fn(C.c_int32(m), C.c_int32(n), C.c_int32(a.nnz), ip(keep[0]), ip(keep[1]),
+            f64_ptr(keep[2]), f64_ptr(keep[3]), f64_ptr(keep[4]), f64_ptr(keep[5]),
+            f64_ptr(keep[6]), f64_ptr(keep[7]), C.c_int(int(model.maximize)),
+            C.c_double(float(model.objective_offset)), C.byref(o), C.c_int(int(use_presolve)),
+            C.c_int(0 if engine else 1), C.c_double(crossover_tolerance), f64_ptr(x),
+            f64_ptr(info))
+    names = ("status", "pivots", "seeded", "fell_back", "seeded_pivots", "seed_iterations",
+             "seed_status", "row_violation", "objective", "candidates", "pushed",
+             "presolve_status")
+    d = dict(zip(names, info.tolist()))
+    for k in names:
+        if k not in ("row_violation", "objective"):
+            d[k] = int(d[k])
+    return rc, x[:n].copy(), d
+
+
+def ref_finish_simplex(lp: StandardLp, x, y, dual: bool = False):
+    """anu_b200::finish_with_simplex: crossover_basis at (x, y), the simplex
+    from its basis (the dual simplex when `dual`), the cold solve after a
+    miss. Returns a dict: status (0 optimal), pivots, seeded, fell_back,
+    seeded_pivots, objective, seconds, candidates, pushed, x, y and basis (the
+    simplex's final (basic, status), for ref_simplex_basis)."""
+    cl = CLp(lp)
+    xi = np.ascontiguousarray(x, np.float64)
+    yi = np.ascontiguousarray(y, np.float64)
+    xo = np.zeros(max(cl.n, 1))
+    yo = np.zeros(max(cl.m, 1))
+    info = np.zeros(9)
+    cap_b, cap_s = max(cl.m, 1) + 8, cl.n + cl.m + 8
+    bo = np.zeros(cap_b, np.int32)
+    so = np.zeros(cap_s, np.int32)
+    nb, ns = C.c_int32(cap_b), C.c_int32(cap_s)
+    ip = lambda arr: arr.ctypes.data_as(_P(C.c_int32))
+    rc = ref_b200_lib().ref_finish_simplex(cl.ref(), f64_ptr(xi), f64_ptr(yi), int(dual),
+                                           f64_ptr(xo), f64_ptr(yo), f64_ptr(info), ip(bo),
+                                           C.byref(nb), ip(so), C.byref(ns))
+    if rc != 0:
+        raise RuntimeError(f"ref_finish_simplex returned {rc}")
+    d = dict(zip(("status", "pivots", "seeded", "fell_back", "seeded_pivots", "objective",
+                  "seconds", "candidates", "pushed"), info.tolist()))
+    for k in ("status", "pivots", "seeded", "fell_back", "seeded_pivots", "candidates", "pushed"):
+        d[k] = int(d[k])
+    d["x"] = xo[:cl.n].copy()
+    d["y"] = yo[:cl.m].copy()
+    d["basis"] = (bo[:nb.value].copy(), so[:ns.value].copy())
+    return d
+
+
+def ref_finish_model(model, x, y, use_presolve: bool = False, dual: bool = False,
+                     seeded_pivot_limit: int = 0):
+    """anu_b200::finish_model_with_simplex: a :class:`Model` finished exactly
+    from a first-order point of its unpresolved standard form (x: columns, y:
+    standard-form rows). Returns (rc, x_model, info) with info a dict: status
+    (0 optimal), pivots, seeded, fell_back, seeded_pivots, objective (model),
+    seconds, candidates, pushed, row_violation, presolve_status."""
+    lib = ref_b200_lib()
+    fn = getattr(lib, "ref_finish_model")
+    fn.restype = C.c_int
+    a = model.constraints
+    m, n = a.rows, a.cols
+    i32 = lambda arr: np.ascontiguousarray(arr, np.int32)
+    f64 = lambda arr: np.ascontiguousarray(arr, np.float64)
+    keep = [i32(a.start), i32(a.index), f64(a.value), f64(model.objective),
+            f64(model.row_lower), f64(model.row_upper), f64(model.col_lower),
+            f64(model.col_upper), f64(x), f64(y)]
+    ip = lambda arr: arr.ctypes.data_as(_P(C.c_int32))
+    xo = np.zeros(max(n, 1))
+    info = np.zeros(11)
+    rc = fn(C.c_int32(m), C.c_int32(n), C.c_int32(a.nnz), ip(keep[0]), ip(keep[1]),
+            f64_ptr(keep[2]), f64_ptr(keep[3]), f64_ptr(keep[4]), f64_ptr(keep[5]),
+            f64_ptr(keep[6]), f64_ptr(keep[7]), C.c_int(int(model.maximize)),
+            C.c_double(float(model.objective_offset)), f64_ptr(keep[8]), f64_ptr(keep[9]),
+            C.c_int32(len(keep[9])), C.c_int(int(use_presolve)), C.c_int(int(dual)),
+            C.c_int32(int(seeded_pivot_limit)), f64_ptr(xo), f64_ptr(info))
+    names = ("status", "pivots", "seeded", "fell_back", "seeded_pivots", "objective",
+             "seconds", "candidates", "pushed", "row_violation", "presolve_status")
+    d = dict(zip(names, info.tolist()))
+    for k in ("status", "pivots", "seeded", "fell_back", "seeded_pivots", "candidates",
+              "pushed", "presolve_status"):
+        d[k] = int(d[k])
+    return rc, xo[:n].copy(), d
+
+
+def ref_simplex_basis(lp: StandardLp, basis=None):
+    """One member of the reference's `family --from-first` (dual simplex,
+    app/anukulan_cli.cpp:1065-1230): solve_lp from `basis` = (basic, status),
+    or cold when None. Returns (info, final basis) with info a dict: status
+    (0 optimal), pivots, objective, seconds."""
+    cl = CLp(lp)
+    cap_b = max(cl.m, 1) + 8
+    cap_s = cl.n + cl.m + 8
+    bo = np.zeros(cap_b, np.int32)
+    so = np.zeros(cap_s, np.int32)
+    nb = C.c_int32(cap_b)
+    ns = C.c_int32(cap_s)
+    info = np.zeros(4)
+    ip = lambda arr: None if arr is None else arr.ctypes.data_as(_P(C.c_int32))
+    if basis is None:
+        bi = si = None
+        lb = ls = 0
+    else:
+        bi = np.ascontiguousarray(basis[0], np.int32)
+        si = np.ascontiguousarray(basis[1], np.int32)
+        lb, ls = len(bi), len(si)
+    rc = ref_b200_lib().ref_simplex_basis(cl.ref(), ip(bi), lb, ip(si), ls, ip(bo),
+                                          C.byref(nb), ip(so), C.byref(ns), f64_ptr(info))
+    if rc != 0:
+        raise RuntimeError(f"ref_simplex_basis returned {rc}")
+    d = dict(zip(("status", "pivots", "objective", "seconds"), info.tolist()))
+    d["status"] = int(d["status"])
+    d["pivots"] = int(d["pivots"])
+    return d, (bo[:nb.value].copy(), so[:ns.value].copy())
 
 
 def ref_b200_solve(lp: StandardLp, options=None, **kw) -> PdhgResult:
