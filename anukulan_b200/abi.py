@@ -56,7 +56,7 @@ class anu_pdhg_options(C.Structure):
         ("detect_infeasibility", i32), ("infeasibility_tolerance", f64),
         ("termination", i32), ("known_matrix_norm", f64), ("initial_step_size", f64),
         ("initial_primal_weight", f64), ("verbose", i32), ("log_frequency", i32),
-        ("stop", C.POINTER(i32)),
+        ("stop", C.POINTER(C.c_uint8)),
         ("precision", i32), ("refinement", i32), ("device", i32), ("use_graphs", i32),
         ("profile", i32), ("split_stacks", i32), ("persistent_chunks", i32),
         ("locality_order", i32), ("scaling_on_device", i32),

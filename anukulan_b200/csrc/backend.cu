@@ -10,16 +10,26 @@
 // device operations (fill, copy, the products, the updates, accumulate,
 // scale_into) return once queued, as the reference's CUDA backend's kernel
 // launches do (cuda_backend.cu:530-559, 832-858).
+#include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <map>
 #include <memory>
 #include <mutex>
+#include <string>
+#include <utility>
+#include <vector>
 
 #include "engine.hpp"
 
 namespace anu {
 namespace {
+
+struct Timing {
+  double seconds = 0.0;
+  long long calls = 0;
+};
 
 struct BackendState {
   std::mutex lock;
@@ -28,6 +38,11 @@ struct BackendState {
   DevBuf<double> partial;
   DevBuf<double> out;
   bool ready = false;
+  // Profiling (LinAlgBackend::set_profiling, backend.hpp:213): per seam
+  // operation, the device time of the work it queued and how often it ran.
+  bool profiling = false;
+  cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+  std::map<std::string, Timing> timings;
 };
 
 BackendState& state() {
@@ -48,6 +63,74 @@ void ensure(BackendState& s) {
   ANU_CUDA(cudaStreamCreateWithFlags(&s.exec.stream, cudaStreamDefault));
   s.out.alloc(16);
   s.ready = true;
+}
+
+// Times the device work one seam operation queues on the library stream:
+// an event before it, an event after it and a wait for the second. With
+// profiling off it does nothing, so the ordinary path pays one branch. The
+// wait serialises the stream, so a profiled run is slower than a plain one;
+// the shares are what it is for.
+class Timed {
+ public:
+  Timed(BackendState& s, const char* name) : s_(s), name_(name) {
+    if (s_.profiling) on_ = cudaEventRecord(s_.ev_start, s_.exec.stream) == cudaSuccess;
+  }
+  Timed(const Timed&) = delete;
+  Timed& operator=(const Timed&) = delete;
+  ~Timed() {
+    if (!on_) return;
+    float ms = 0.0f;
+    if (cudaEventRecord(s_.ev_stop, s_.exec.stream) != cudaSuccess ||
+        cudaEventSynchronize(s_.ev_stop) != cudaSuccess ||
+        cudaEventElapsedTime(&ms, s_.ev_start, s_.ev_stop) != cudaSuccess)
+      return;  // a failure in the queued work surfaces at the next waiting call
+    Timing& t = s_.timings[name_];
+    t.seconds += static_cast<double>(ms) * 1e-3;
+    t.calls += 1;
+  }
+
+ private:
+  BackendState& s_;
+  std::string name_;
+  bool on_ = false;
+};
+
+std::string profile_report(const BackendState& s) {
+  if (s.timings.empty()) return {};
+  std::vector<std::pair<std::string, Timing>> rows(s.timings.begin(), s.timings.end());
+  std::sort(rows.begin(), rows.end(),
+            [](const auto& a, const auto& b) { return a.second.seconds > b.second.seconds; });
+  double total = 0.0;
+  long long calls = 0;
+  for (const auto& r : rows) {
+    total += r.second.seconds;
+    calls += r.second.calls;
+  }
+  std::string out;
+  char line[256];
+  std::snprintf(line, sizeof(line), "%-26s %12s %9s %12s %10s\n", "operation", "seconds",
+                "share", "calls", "us each");
+  out += line;
+  for (const auto& [name, t] : rows) {
+    std::snprintf(line, sizeof(line), "%-26s %12.6f %8.1f%% %12lld %10.2f\n", name.c_str(),
+                  t.seconds, total > 0.0 ? 100.0 * t.seconds / total : 0.0, t.calls,
+                  t.calls > 0 ? 1e6 * t.seconds / static_cast<double>(t.calls) : 0.0);
+    out += line;
+  }
+  std::snprintf(line, sizeof(line), "%-26s %12.6f %8.1f%% %12lld\n", "total on the device",
+                total, 100.0, calls);
+  out += line;
+  if (!s.matrices.empty()) {
+    out += "\nprepared matrices (row-block schedule of the product kernel):\n";
+    for (const auto& [id, d] : s.matrices) {
+      std::snprintf(line, sizeof(line),
+                    "  id %-12llu %9d rows %10d nonzeros %7.2f per row %8d row blocks\n",
+                    static_cast<unsigned long long>(id), d->rows, d->nnz,
+                    d->rows > 0 ? static_cast<double>(d->nnz) / d->rows : 0.0, d->num_blocks);
+      out += line;
+    }
+  }
+  return out;
 }
 
 template <class F>
@@ -223,6 +306,7 @@ int anu_backend_download(const double* dev, double* host, int64_t n) {
 int anu_backend_fill(double* dev, int64_t n, double value) {
   return anu::guard([&](BackendState& s) {
     if (n <= 0) return;
+    anu::Timed t(s, "fill");
     anu::fill_kernel<<<anu::grid_n(n), 256, 0, s.exec.stream>>>(n, value, dev);
     ANU_CUDA(cudaGetLastError());
   });
@@ -231,6 +315,7 @@ int anu_backend_fill(double* dev, int64_t n, double value) {
 int anu_backend_copy(const double* source, double* target, int64_t n) {
   return anu::guard([&](BackendState& s) {
     if (n <= 0) return;
+    anu::Timed t(s, "copy");
     ANU_CUDA(cudaMemcpyAsync(target, source, sizeof(double) * n, cudaMemcpyDeviceToDevice,
                              s.exec.stream));
   });
@@ -257,16 +342,23 @@ int anu_backend_multiply(uint64_t id, const double* x, double* y) {
   return anu::guard([&](BackendState& s) {
     auto it = s.matrices.find(id);
     if (it == s.matrices.end()) throw Error(ANU_ERR_INVALID, "matrix was not prepared");
+    anu::Timed t(s, "multiply");
     anu::product<double, double, double>(s.exec, *it->second, x, 1, anu::StoreEpi<double>{1, y});
   });
 }
 
 int anu_backend_dot(const double* a, const double* b, int64_t n, double* out) {
-  return anu::guard([&](BackendState& s) { *out = anu::reduce_scalar_dot(s, a, b, n); });
+  return anu::guard([&](BackendState& s) {
+    anu::Timed t(s, "dot");
+    *out = anu::reduce_scalar_dot(s, a, b, n);
+  });
 }
 
 int anu_backend_two_norm(const double* a, int64_t n, double* out) {
-  return anu::guard([&](BackendState& s) { *out = std::sqrt(anu::reduce_scalar_dot(s, a, a, n)); });
+  return anu::guard([&](BackendState& s) {
+    anu::Timed t(s, "two norm");
+    *out = std::sqrt(anu::reduce_scalar_dot(s, a, a, n));
+  });
 }
 
 int anu_backend_inf_norm(const double* a, int64_t n, double* out) {
@@ -274,6 +366,7 @@ int anu_backend_inf_norm(const double* a, int64_t n, double* out) {
     anu::check_len(n);
     *out = 0.0;
     if (n == 0) return;
+    anu::Timed t(s, "inf norm");
     anu::reduce_terms(s.exec, static_cast<int32_t>(n), 1, anu::MaxAbsTerms{a}, s.partial, s.out.p, 1, 0);
     ANU_CUDA(cudaMemcpyAsync(out, s.out.p, sizeof(double), cudaMemcpyDeviceToHost, s.exec.stream));
     ANU_CUDA(cudaStreamSynchronize(s.exec.stream));
@@ -286,6 +379,7 @@ int anu_backend_primal_update(int64_t n, double tau, double gamma, double halper
                               double* dx, double* x_bar) {
   return anu::guard([&](BackendState& s) {
     if (n <= 0) return;
+    anu::Timed t(s, "primal update");
     anu::primal_update_kernel<<<anu::grid_n(n), 256, 0, s.exec.stream>>>(
         n, tau, gamma, halpern, x, c, kt_y, lower, upper, anchor, x_out, dx, x_bar);
     ANU_CUDA(cudaGetLastError());
@@ -299,6 +393,7 @@ int anu_backend_dual_update(int64_t m, int64_t num_equalities, double sigma, dou
                             double* k_dx) {
   return anu::guard([&](BackendState& s) {
     if (m <= 0) return;
+    anu::Timed t(s, "dual update");
     anu::dual_update_kernel<<<anu::grid_n(m), 256, 0, s.exec.stream>>>(
         m, num_equalities, sigma, gamma, halpern, y, q, k_x_bar, k_x, anchor_y, anchor_kx, y_out,
         dy, k_out, k_dx);
@@ -309,6 +404,7 @@ int anu_backend_dual_update(int64_t m, int64_t num_equalities, double sigma, dou
 int anu_backend_accumulate(int64_t n, double weight, const double* v, double* sum) {
   return anu::guard([&](BackendState& s) {
     if (n <= 0) return;
+    anu::Timed t(s, "accumulate");
     anu::accumulate64_kernel<<<anu::grid_n(n), 256, 0, s.exec.stream>>>(n, weight, v, sum);
     ANU_CUDA(cudaGetLastError());
   });
@@ -317,6 +413,7 @@ int anu_backend_accumulate(int64_t n, double weight, const double* v, double* su
 int anu_backend_scale_into(int64_t n, double weight, const double* sum, double* out) {
   return anu::guard([&](BackendState& s) {
     if (n <= 0) return;
+    anu::Timed t(s, "scale into");
     anu::divide_kernel<<<anu::grid_n(n), 256, 0, s.exec.stream>>>(n, weight, sum, out);
     ANU_CUDA(cudaGetLastError());
   });
@@ -325,6 +422,7 @@ int anu_backend_scale_into(int64_t n, double weight, const double* sum, double* 
 int anu_backend_weighted_norm_squared(int64_t n, int64_t m, const double* dx, const double* dy,
                                       double omega, double* out) {
   return anu::guard([&](BackendState& s) {
+    anu::Timed t(s, "weighted norm");
     const double a = anu::reduce_scalar_dot(s, dx, dx, n);
     const double b = anu::reduce_scalar_dot(s, dy, dy, m);
     *out = omega * a + b / omega;
@@ -335,6 +433,7 @@ int anu_backend_step_size_terms(int64_t n, int64_t m, const double* dx, const do
                                 const double* k_dx, double omega, double* interaction,
                                 double* movement) {
   return anu::guard([&](BackendState& s) {
+    anu::Timed t(s, "step-size terms");
     *interaction = std::fabs(anu::reduce_scalar_dot(s, dy, k_dx, m));
     const double a = anu::reduce_scalar_dot(s, dx, dx, n);
     const double b = anu::reduce_scalar_dot(s, dy, dy, m);
@@ -351,6 +450,7 @@ int anu_backend_convergence_terms(int64_t n, int64_t m, const double* c, const d
     anu::check_len(n);
     anu::check_len(m);
     if (s.out.n < 18) s.out.alloc(18);
+    anu::Timed t(s, "convergence terms");
     anu::RowCheckTerms<double, double, double> rt{1, static_cast<int32_t>(num_equalities), k_x,
                                                   y, nullptr, nullptr, nullptr, nullptr, q,
                                                   nullptr, row_scale};
@@ -370,6 +470,29 @@ int anu_backend_convergence_terms(int64_t n, int64_t m, const double* c, const d
     out[4] = h[10];
     out[5] = h[11];
     out[6] = h[12];
+  });
+}
+
+int anu_backend_set_profiling(int32_t on) {
+  return anu::guard([&](BackendState& s) {
+    if (on && s.ev_start == nullptr) {
+      ANU_CUDA(cudaEventCreate(&s.ev_start));
+      ANU_CUDA(cudaEventCreate(&s.ev_stop));
+    }
+    s.profiling = on != 0;
+    if (!s.profiling) s.timings.clear();
+  });
+}
+
+int anu_backend_profile_report(char* buf, int32_t size, int32_t* length) {
+  return anu::guard([&](BackendState& s) {
+    const std::string r = anu::profile_report(s);
+    if (length != nullptr) *length = static_cast<int32_t>(r.size());
+    if (buf != nullptr && size > 0) {
+      const size_t k = std::min(r.size(), static_cast<size_t>(size - 1));
+      std::memcpy(buf, r.data(), k);
+      buf[k] = '\0';
+    }
   });
 }
 

@@ -2287,7 +2287,7 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
                     candidate_kkt[k], S[k].eta, S[k].omega);
     }
     const bool out_of_time = now_seconds() - start_time > o.time_limit_seconds ||
-                             (o.stop != nullptr && *o.stop != 0);
+                             (o.stop != nullptr && __atomic_load_n(o.stop, __ATOMIC_ACQUIRE) != 0);
     std::fill(adopt_mask.begin(), adopt_mask.end(), 0);
     if (out_of_time) {
       for (int k = 0; k < K; ++k) {

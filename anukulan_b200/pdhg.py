@@ -36,7 +36,8 @@ EXPORTS = (
     "anu_backend_inf_norm", "anu_backend_primal_update", "anu_backend_dual_update",
     "anu_backend_accumulate", "anu_backend_scale_into", "anu_backend_weighted_norm_squared",
     "anu_backend_step_size_terms", "anu_backend_convergence_terms",
-    "anu_backend_convergence_terms_noalloc",
+    "anu_backend_convergence_terms_noalloc", "anu_backend_set_profiling",
+    "anu_backend_profile_report",
     "anu_pdhg_batch_create", "anu_pdhg_batch_solve", "anu_pdhg_batch_solve_warm",
     "anu_pdhg_batch_destroy", "anu_pdhg_batch_stream",
     "anu_pdhg_packed_create", "anu_pdhg_packed_solve", "anu_pdhg_packed_workers",
@@ -132,8 +133,24 @@ def lib():
       + [_P(dbl)])
     d("anu_backend_convergence_terms_noalloc", C.c_int,
       [i64, i64] + [vp] * 6 + [i64] + [vp] * 4 + [_P(dbl)])
+    d("anu_backend_set_profiling", C.c_int, [C.c_int32])
+    d("anu_backend_profile_report", C.c_int, [C.c_char_p, C.c_int32, _P(C.c_int32)])
     _lib = L
     return L
+
+
+def backend_set_profiling(on: bool) -> None:
+    """LinAlgBackend::set_profiling on the seam (backend.hpp:213)."""
+    check(lib().anu_backend_set_profiling(1 if on else 0))
+
+
+def backend_profile_report() -> str:
+    """LinAlgBackend::profile_report of the seam (backend.hpp:214)."""
+    n = C.c_int32(0)
+    check(lib().anu_backend_profile_report(None, 0, C.byref(n)))
+    buf = C.create_string_buffer(n.value + 1)
+    check(lib().anu_backend_profile_report(buf, n.value + 1, C.byref(n)))
+    return buf.value.decode()
 
 
 def check(rc: int) -> None:

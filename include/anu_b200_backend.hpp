@@ -34,6 +34,7 @@
 #include <cstdint>
 #include <stdexcept>
 #include <string>
+#include <vector>
 
 #include "anu_pdhg.h"
 #include "anukulan/backend.hpp"
@@ -154,6 +155,18 @@ class Backend final : public anukulan::LinAlgBackend {
     out->dual_inf = t[4];
     out->bound_term = t[5];
     out->c_dot_x = t[6];
+  }
+
+  // backend.hpp:213-214: the library times each seam operation's device work
+  // with CUDA events while profiling is on (anu_backend_set_profiling) and
+  // reports the table the CLI's --profile prints.
+  void set_profiling(bool on) const override { check(anu_backend_set_profiling(on ? 1 : 0)); }
+  std::string profile_report() const override {
+    int32_t length = 0;
+    check(anu_backend_profile_report(nullptr, 0, &length));
+    std::vector<char> buf(static_cast<std::size_t>(length) + 1, '\0');
+    check(anu_backend_profile_report(buf.data(), static_cast<int32_t>(buf.size()), &length));
+    return std::string(buf.data());
   }
 
  private:

@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define ANU_PDHG_ABI_VERSION 1
+#define ANU_PDHG_ABI_VERSION 2
 
 /* Return codes. */
 enum {
@@ -139,9 +139,15 @@ typedef struct anu_pdhg_options {
   double initial_primal_weight;           /* 0: derive it */
   int32_t verbose;                        /* 0 */
   int32_t log_frequency;                  /* 5000 */
-  /* PdhgOptions::stop: when *stop becomes nonzero the solve ends at the next
-   * check with ANU_PDHG_TIME_LIMIT. NULL: no cancellation. */
-  const volatile int32_t* stop;
+  /* PdhgOptions::stop (pdhg.hpp:414, a const std::atomic<bool>*): a one-byte
+   * flag that another thread may set at any time. The engine reads it with
+   * an acquire load at every termination check; once it is nonzero the
+   * solve (every case still running, for a case stack) ends at that check
+   * with ANU_PDHG_TIME_LIMIT, as a stop request ends the reference's solve.
+   * A std::atomic<bool>, which is one lock-free byte holding a bool, binds
+   * as reinterpret_cast<const volatile uint8_t*>(ptr). NULL: no
+   * cancellation. */
+  const volatile uint8_t* stop;
 
   /* --- engine additions, no counterpart in PdhgOptions --- */
   int32_t precision;            /* ANU_PRECISION_FP64 (default) or _FP32 */
@@ -365,6 +371,18 @@ int anu_backend_convergence_terms(int64_t n, int64_t m, const double* c,
                                   const double* x, const double* k_x,
                                   const double* y, const double* kt_y,
                                   double* out);                   /* backend.hpp:198-202 */
+
+/* LinAlgBackend::set_profiling (backend.hpp:213): on = 1 times the device
+ * work of every seam operation above with CUDA events on the library stream,
+ * waiting for each, so a profiled run is slower than a plain one and its
+ * shares are what it is for; 0 stops and clears the timings. */
+int anu_backend_set_profiling(int32_t on);
+/* LinAlgBackend::profile_report (backend.hpp:214): one line per operation
+ * (device seconds, share, calls, microseconds per call), the total, and the
+ * prepared matrices with their product schedules. Writes at most size-1
+ * characters and a NUL into buf (NULL: nothing); *length (may be NULL) gets
+ * the report's full length. Empty when nothing was timed. */
+int anu_backend_profile_report(char* buf, int32_t size, int32_t* length);
 
 /* anu_backend_convergence_terms without any device allocation. There is no
  * counterpart in the reference.

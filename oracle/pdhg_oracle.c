@@ -1038,7 +1038,7 @@ static void solve(const olp* original, const anu_pdhg_options* options, const do
              eta, omega);
     }
     if (now_seconds() - start_time > options->time_limit_seconds ||
-        (options->stop != NULL && *options->stop != 0)) {
+        (options->stop != NULL && __atomic_load_n(options->stop, __ATOMIC_ACQUIRE) != 0)) {
       status = ANU_PDHG_TIME_LIMIT;
       ++iteration;
       ADOPT_CANDIDATE();

@@ -102,3 +102,32 @@ def test_reference_solver_on_engine_full_solves(engine):
         assert oracle.ref_residual(case, g.x, g.y).converged(1e-6)
         if known is not None:
             assert abs(g.objective - known) <= 1e-5 * abs(known)
+
+
+def test_adapter_profile_report(engine):
+    """set_profiling / profile_report (backend.hpp:213-214), which the CLI's
+    --profile prints: with profiling on, the reference's solve_pdhg through
+    the adapter leaves a report of the seam operations it ran, the products
+    and the two updates among them, whose shares add up to the total; off,
+    the report is empty."""
+    lp, _ = lpgen.random_lp(300, 450, 8, seed=20261203)
+    engine.backend_set_profiling(True)
+    try:
+        r = oracle.ref_b200_solve(lp, tolerance=1e-6)
+        report = engine.backend_profile_report()
+    finally:
+        engine.backend_set_profiling(False)
+    assert r.status == OPTIMAL
+    rows = {}
+    for line in report.splitlines()[1:]:
+        if not line.strip() or line.startswith("total"):
+            break
+        name, rest = line[:26].strip(), line[26:].split()
+        rows[name] = (float(rest[0]), float(rest[1].rstrip("%")), int(rest[2]))
+    for op in ("multiply", "primal update", "dual update", "convergence terms"):
+        assert op in rows and rows[op][0] > 0.0 and rows[op][2] > 0, (op, report)
+    # Two products per iteration at least.
+    assert rows["multiply"][2] >= 2 * r.iterations
+    assert abs(sum(v[1] for v in rows.values()) - 100.0) < 0.5
+    assert "prepared matrices" in report
+    assert engine.backend_profile_report() == ""
