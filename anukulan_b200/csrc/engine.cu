@@ -2749,6 +2749,35 @@ int anu_pdhg_run(anu_pdhg* h, const double* warm_x, const double* warm_y, double
   });
 }
 
+int anu_pdhg_set_case(anu_pdhg* h, const double* c, const double* q, const double* lower,
+                      const double* upper) {
+  return guarded([&] {
+    if (h == nullptr) throw Error(ANU_ERR_INVALID, "null argument");
+    const anu::Problem& p = *h->problem;
+    const anu::Relabel& r = h->relabel;
+    // Each given vector in the problem's order; a NULL one keeps the case's.
+    auto order = [&](const double* v, const std::vector<int32_t>& old, int32_t len,
+                     const std::vector<double>& keep) {
+      if (v == nullptr) return keep;
+      if (r.empty()) return std::vector<double>(v, v + len);
+      return anu::take(v, old);
+    };
+    const std::vector<double> cc = order(c, r.col_old, p.n, h->data.c);
+    const std::vector<double> qq = order(q, r.row_old, p.m, h->data.q);
+    const std::vector<double> lo = order(lower, r.col_old, p.n, h->data.lower);
+    const std::vector<double> up = order(upper, r.col_old, p.n, h->data.upper);
+    for (int32_t j = 0; j < p.n; ++j) {
+      if (!std::isfinite(cc[j])) throw Error(ANU_ERR_INVALID, "objective is not finite");
+      if (lo[j] > up[j] || std::isnan(lo[j]) || std::isnan(up[j]))
+        throw Error(ANU_ERR_INVALID, "empty or NaN bound interval");
+    }
+    for (int32_t i = 0; i < p.m; ++i)
+      if (!std::isfinite(qq[i])) throw Error(ANU_ERR_INVALID, "rhs is not finite");
+    h->data = anu::make_case(p, cc.data(), qq.data(), lo.data(), up.data(),
+                             h->data.objective_scale, h->data.objective_offset);
+  });
+}
+
 void anu_pdhg_destroy(anu_pdhg* h) { delete h; }
 
 int anu_pdhg_solve(const anu_lp* lp, const anu_pdhg_options* options, const double* warm_x,

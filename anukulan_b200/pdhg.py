@@ -28,7 +28,7 @@ _lib = None
 EXPORTS = (
     "anu_pdhg_version", "anu_pdhg_default_options", "anu_last_error", "anu_device_count",
     "anu_release_cached_memory",
-    "anu_pdhg_solve", "anu_pdhg_create", "anu_pdhg_run", "anu_pdhg_destroy",
+    "anu_pdhg_solve", "anu_pdhg_create", "anu_pdhg_run", "anu_pdhg_set_case", "anu_pdhg_destroy",
     "anu_evaluate_residual", "anu_estimate_matrix_norm", "anu_locality_relabel",
     "anu_backend_allocate", "anu_backend_deallocate", "anu_backend_upload",
     "anu_backend_download", "anu_backend_fill", "anu_backend_copy", "anu_backend_prepare",
@@ -79,6 +79,7 @@ def lib():
     d("anu_pdhg_create", C.c_int, [_P(anu_lp), _P(anu_pdhg_options), _P(C.c_void_p)])
     d("anu_pdhg_run", C.c_int, [C.c_void_p, _P(C.c_double), _P(C.c_double), _P(C.c_double),
                                 _P(C.c_double), _P(anu_pdhg_result)])
+    d("anu_pdhg_set_case", C.c_int, [C.c_void_p] + [_P(C.c_double)] * 4)
     d("anu_pdhg_destroy", None, [C.c_void_p])
     d("anu_evaluate_residual", C.c_int, [_P(anu_lp), _P(C.c_double), _P(C.c_double),
                                          _P(anu_pdhg_residual)])
@@ -237,6 +238,16 @@ class PdhgHandle:
         check(lib().anu_pdhg_run(self._h, f64_ptr(wx), f64_ptr(wy), f64_ptr(x), f64_ptr(y),
                                  C.byref(r)))
         return PdhgResult.from_c(r, x, y)
+
+    def set_case(self, c=None, q=None, lower=None, upper=None) -> None:
+        """``anu_pdhg_set_case``: another LP with the same matrix (None keeps
+        a vector); the scaled matrix and ||K|| are kept."""
+        keep = [None if v is None else np.ascontiguousarray(v, np.float64)
+                for v in (c, q, lower, upper)]
+        for v, size in zip(keep, (self._cl.n, self._cl.m, self._cl.n, self._cl.n)):
+            if v is not None and v.shape != (size,):
+                raise ValueError("case vector of the wrong length")
+        check(lib().anu_pdhg_set_case(self._h, *[f64_ptr(v) for v in keep]))
 
     def close(self):
         if self._h:

@@ -55,6 +55,8 @@ sys.path.insert(0, ROOT)
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM = 6650.0
 TOL = 1e-6
+# Side legs of the default stack line, in the order they run.
+SIDE_LEGS = ("spmv", "fp64_single_case", "stream", "exact_stack", "adjoint", "packed", "powerlaw")
 # DRAM bytes (read + write) per fused seg_kernel launch of 30 cases (one
 # half of the split stack), mean of the primal and dual kernels, from one
 # cold-cache ncu capture (profiles/seg_kernel_refinery_stack.md): 3.04 MB
@@ -198,29 +200,26 @@ def spmv_leg(iterations, device, peak, only=None):
     return out
 
 
-def run_packed(args, rank, world, local_rank):
+def packed_leg(local_rank, steps, warmup, workers=0, cpu=True, cpu_sample=32):
     """The packed batch: 256 independent LPs, rows log-uniform in
     [500, 50,000], 1.5x as many columns, 8 nonzeros per column, FP32 with
     FP64 checks and refinement to relative KKT 1e-6. A step solves the whole
-    batch. Rank 0 only (the batch does not shard here)."""
-    if rank != 0:
-        return None
+    batch, timed with CUDA events."""
     import torch
     from anukulan_b200 import lpgen, pdhg
     from anukulan_b200.abi import OPTIMAL, PRECISION_FP32, make_options
-    torch.cuda.set_device(local_rank)
     batch = lpgen.packed_batch()
     lps = [lp for lp, _ in batch]
     opts = make_options(tolerance=TOL, precision=PRECISION_FP32, device=local_rank)
     t0 = time.perf_counter()
-    solver = pdhg.PackedBatchSolver(lps, opts, workers=args.packed_workers)
+    solver = pdhg.PackedBatchSolver(lps, opts, workers=workers)
     create_s = time.perf_counter() - t0
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         solver.solve()
     clocks = ClockSampler(local_rank)
     clocks.start()
     step_ms, solved, iters = [], 0, 0
-    for _ in range(args.steps):
+    for _ in range(steps):
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
@@ -232,32 +231,30 @@ def run_packed(args, rank, world, local_rank):
         solved += sum(int(r.status == OPTIMAL) for r in res)
         iters += sum(r.iterations for r in res)
     clk = clocks.stop()
-    workers = solver.workers
+    used = solver.workers
     solver.close()
     total = float(np.sum(step_ms))
     nnz = sum(lp.k.nnz for lp in lps)
     out = {
-        "metric": "LP solves/s to relative KKT 1e-6 (packed batch of unequal LPs, FP32 + FP64 checks)",
-        "value": solved / (total / 1e3), "unit": "solves/s", "n_gpus": 1, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": total / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (seeded generator, 256 LPs of the random known-optimum construction)",
+        "value": solved / (total / 1e3), "unit": "solves/s", "steps": steps, "warmup": warmup,
+        "ms_per_step": total / steps,
         "config": {"workload": "packed_batch", "lps": len(lps),
                    "rows_total": int(sum(lp.num_rows for lp in lps)), "nnz_total": int(nnz),
                    "rows_range": [int(min(lp.num_rows for lp in lps)),
                                   int(max(lp.num_rows for lp in lps))],
-                   "tolerance": TOL, "workers": workers},
-        "cases_optimal": solved, "cases_attempted": len(lps) * args.steps,
+                   "tolerance": TOL, "workers": used},
+        "cases_optimal": solved, "cases_attempted": len(lps) * steps,
         "iterations_per_second": iters / (total / 1e3),
         "step_ms": [round(v, 1) for v in step_ms], "create_seconds": create_s, "clocks": clk,
     }
-    if args.cpu_baseline:
+    if cpu:
         # The reference's CPU PDHG on a uniform random sample of the batch,
         # one LP per host thread.
         import oracle
         from concurrent.futures import ThreadPoolExecutor
         rng = np.random.default_rng(0)
-        sample = [lps[i] for i in rng.choice(len(lps), size=min(32, len(lps)), replace=False)]
+        sample = [lps[i] for i in rng.choice(len(lps), size=min(cpu_sample, len(lps)),
+                                             replace=False)]
         threads = os.cpu_count() or 1
         use_ref = oracle.have_reference()
         fn = (lambda lp: oracle.ref_solve(lp, tolerance=TOL)) if use_ref else \
@@ -273,17 +270,32 @@ def run_packed(args, rank, world, local_rank):
     return out
 
 
-def run_adjoint(args, rank, world, local_rank):
+def run_packed(args, rank, world, local_rank):
+    """--workload packed: the packed batch as the line's own workload. Rank 0
+    only (the batch does not shard here)."""
+    if rank != 0:
+        return None
+    import torch
+    torch.cuda.set_device(local_rank)
+    leg = packed_leg(local_rank, args.steps, args.warmup, args.packed_workers, args.cpu_baseline)
+    out = {
+        "metric": "LP solves/s to relative KKT 1e-6 (packed batch of unequal LPs, FP32 + FP64 checks)",
+        "n_gpus": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded generator, 256 LPs of the random known-optimum construction)",
+    }
+    out.update(leg)
+    return out
+
+
+def adjoint_leg(local_rank, steps, warmup, cpu=True):
     """Sensitivities through the unrolled program: the 60-case refinery stack,
     2,000 FP32 iterations with checkpoints every 100, loss c_hat'x_T per
     case with c_hat = c (1 + 0.05 N(0,1)). A step is one forward pass (x_T
     and the losses) and one backward pass (dL/dc, dL/dq for every case)."""
-    if rank != 0:
-        return None
     import torch
     from anukulan_b200 import lpgen, pdhg
     from anukulan_b200.abi import PRECISION_FP32, make_options
-    torch.cuda.set_device(local_rank)
     stack, c_hat = lpgen.adjoint_case()
     ratio = c_hat / np.where(stack.base.c != 0, stack.base.c, 1.0)
     loss = stack.c * ratio
@@ -291,13 +303,13 @@ def run_adjoint(args, rank, world, local_rank):
     opts = make_options(precision=PRECISION_FP32, device=local_rank)
     u = pdhg.UnrolledPdhg(stack.base, stack.c, stack.q, stack.lower, stack.upper,
                           iterations=T, checkpoint_every=R, options=opts)
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         x, _ = u.forward()
         u.backward(loss)
     clocks = ClockSampler(local_rank)
     clocks.start()
     step_ms = []
-    for _ in range(args.steps):
+    for _ in range(steps):
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
@@ -313,17 +325,14 @@ def run_adjoint(args, rank, world, local_rank):
     total = float(np.sum(step_ms))
     K = stack.num_cases
     out = {
-        "metric": "unrolled-PDHG sensitivities/s (dL/dc, dL/dq per case, 2,000 FP32 iterations)",
-        "value": K * args.steps / (total / 1e3), "unit": "case gradients/s", "n_gpus": 1,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (seeded generator, refinery-shaped 60-case stack)",
+        "value": K * steps / (total / 1e3), "unit": "case gradients/s", "steps": steps,
+        "warmup": warmup, "ms_per_step": total / steps,
         "config": {"workload": "unrolled_adjoint", "cases": K, "iterations": T,
                    "checkpoint_every": R, "rows": stack.base.num_rows,
                    "cols": stack.base.num_cols},
         "step_ms": [round(v, 2) for v in step_ms], "clocks": clk,
     }
-    if args.cpu_baseline:
+    if cpu:
         # The float64 numpy restatement of the same program and reverse mode,
         # one case on one host thread.
         from oracle import unrolled as U
@@ -334,6 +343,22 @@ def run_adjoint(args, rank, world, local_rank):
         out["cpu_baseline"] = {"value": 1.0 / dt, "unit": "case gradients/s", "cores": 1,
                                "kind": "port",
                                "sample": f"case 0, forward + reverse in numpy/scipy FP64, {dt:.2f} s"}
+    return out
+
+
+def run_adjoint(args, rank, world, local_rank):
+    """--workload adjoint: the unrolled adjoint as the line's own workload."""
+    if rank != 0:
+        return None
+    import torch
+    torch.cuda.set_device(local_rank)
+    leg = adjoint_leg(local_rank, args.steps, args.warmup, args.cpu_baseline)
+    out = {
+        "metric": "unrolled-PDHG sensitivities/s (dL/dc, dL/dq per case, 2,000 FP32 iterations)",
+        "n_gpus": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded generator, refinery-shaped 60-case stack)",
+    }
+    out.update(leg)
     return out
 
 
@@ -362,41 +387,85 @@ def stream_leg(st, opts, copies=4):
             "mode": "rolling stack: retired slots admit waiting cases at termination checks"}
 
 
-def run_powerlaw(args, rank, world, local_rank):
-    """Whole solves of the 200,000 x 300,000 power-law LP to --tolerance: FP64
-    iterates against FP32 iterates with FP64 checks and refinement. A step
-    is one solve in each precision (no warm-up: each solve is long)."""
-    if rank != 0:
-        return None
-    import torch
+def powerlaw_leg(local_rank, tolerance, precisions, locality, time_limit, peak,
+                 cpu=True, cpu_iterations=2000):
+    """Whole solves of the 200,000 x 300,000 power-law LP to `tolerance`, one
+    per precision (FP32 iterates with FP64 checks and refinement; FP64), no
+    warm-up: each solve is long. Per solve: seconds, iterations, the device
+    time per iteration and its fraction of the HBM roofline (algorithmic
+    bytes of one iteration), the residuals and the objective's distance from
+    the planted optimum c'x0."""
     from anukulan_b200 import lpgen, pdhg
     from anukulan_b200.abi import PRECISION_FP32, PRECISION_FP64, make_options
-    torch.cuda.set_device(local_rank)
     lp, objective = lpgen.power_law_lp()
-    out = {"metric": f"power-law LP solve to relative KKT {args.tolerance:g}",
-           "unit": "seconds", "higher_is_better": False, "n_gpus": 1,
-           "config": {"workload": "powerlaw_lp", "rows": lp.num_rows, "cols": lp.num_cols,
-                      "nnz": lp.k.nnz, "tolerance": args.tolerance,
-                      "locality_order": args.locality},
-           "data": "synthetic (seeded generator, planted optimum c'x0)"}
-    wanted = args.precisions.split(",")
-    for name, prec in (("fp32", PRECISION_FP32), ("fp64", PRECISION_FP64)):
-        if name not in wanted:
+    nnz, m, n = lp.k.nnz, lp.num_rows, lp.num_cols
+    out = {"config": {"workload": "powerlaw_lp", "rows": m, "cols": n, "nnz": nnz,
+                      "tolerance": tolerance, "locality_order": locality}}
+    for name, prec, size in (("fp32", PRECISION_FP32, 4), ("fp64", PRECISION_FP64, 8)):
+        if name not in precisions:
             continue
-        opts = make_options(tolerance=args.tolerance, precision=prec, device=local_rank,
-                            max_iterations=5_000_000, time_limit_seconds=args.time_limit,
-                            profile=1, locality_order=args.locality)
+        opts = make_options(tolerance=tolerance, precision=prec, device=local_rank,
+                            max_iterations=5_000_000, time_limit_seconds=time_limit,
+                            profile=1, locality_order=locality)
+        clocks = ClockSampler(local_rank)
+        clocks.start()
         t0 = time.perf_counter()
         r = pdhg.solve_pdhg(lp, opts)
         dt = time.perf_counter() - t0
+        clk = clocks.stop()
+        us = 1e6 * r.device_iteration_seconds / max(r.device_iterations, 1)
+        bytes_it = algorithmic_bytes_per_iteration(nnz, m, n, 1, size, size)
+        achieved = bytes_it / (us * 1e-6) / 1e9 if r.device_iterations else None
         out[name] = {"status": r.status, "iterations": r.iterations, "seconds": dt,
+                     "solves_per_second": 1.0 / dt,
+                     "iterations_per_second": r.iterations / dt,
                      "restarts": r.restarts, "polished": bool(r.polished),
                      "relative_primal": r.residual.relative_primal,
                      "relative_dual": r.residual.relative_dual,
                      "relative_gap": r.residual.relative_gap,
                      "objective_error": abs(r.objective - objective) / abs(objective),
-                     "us_per_iteration_device": 1e6 * r.device_iteration_seconds
-                     / max(r.device_iterations, 1)}
+                     "setup_ms": {k: round(r.phases[k] * 1e3, 2)
+                                  for k in ("scaling", "matrix_norm")},
+                     "us_per_iteration_device": us,
+                     "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak,
+                                  "unit": "GB/s", "frac": achieved / peak if achieved else None,
+                                  "algorithmic_bytes_per_iteration": bytes_it},
+                     "clocks": clk}
+    if cpu:
+        # The reference's CPU PDHG (threaded_cpu_backend with the reference's
+        # own default thread count) run for a bounded number of iterations:
+        # its time per iteration, and that time over the engine's iteration
+        # count as a projection of its whole solve.
+        import oracle
+        if oracle.have_reference():
+            r = oracle.ref_solve(lp, threads=-1, tolerance=tolerance,
+                                 max_iterations=cpu_iterations, time_limit_seconds=600.0)
+            per_it = r.phases["iterating"] / max(r.iterations, 1)
+            first = out.get(precisions[0], {})
+            out["cpu_baseline"] = {
+                "value": 1.0 / per_it, "unit": "iterations/s",
+                "cores": int(oracle.ref_lib().ref_default_thread_count()), "kind": "reference",
+                "sample": f"{r.iterations} iterations of solve_pdhg on threaded_cpu_backend, "
+                          f"{r.phases['iterating']:.1f} s iterating, "
+                          f"{r.phases['scaling'] + r.phases['matrix_norm']:.1f} s set-up",
+                "projected_solve_seconds": per_it * first.get("iterations", 0)}
+    return out
+
+
+def run_powerlaw(args, rank, world, local_rank):
+    """--workload powerlaw: whole solves of the power-law LP as the line's
+    own workload, to --tolerance."""
+    if rank != 0:
+        return None
+    import torch
+    torch.cuda.set_device(local_rank)
+    peak, kind = hbm_peak()
+    wanted = args.precisions.split(",")
+    out = {"metric": f"power-law LP solve to relative KKT {args.tolerance:g}",
+           "unit": "seconds", "higher_is_better": False, "n_gpus": 1,
+           "data": "synthetic (seeded generator, planted optimum c'x0)", "peak_source": kind}
+    out.update(powerlaw_leg(local_rank, args.tolerance, wanted, args.locality, args.time_limit,
+                            peak, args.cpu_baseline))
     out["value"] = out[wanted[0]]["seconds"]
     return out
 
@@ -445,9 +514,84 @@ def run_seam(args, rank, world, local_rank):
     return out
 
 
+def exact_stack_leg(st, device):
+    """The case stack answered exactly, the reference's stated design for
+    case stacks (README.md:81-86): the engine bounds every case at once (the
+    FP32 stack to relative KKT 1e-6), the engine's point for the base LP goes
+    through the reference's crossover_basis and simplex, and every case is
+    finished by the reference's warm dual simplex from that basis, on all
+    host threads (a case whose warm start misses is finished from its own
+    engine point). Beside it, the reference's family --from-first
+    (app/anukulan_cli.cpp:1065-1230): a cold dual simplex on the base, then
+    every case warm from its basis, on the same threads. Crossover and the
+    simplex are the reference's host code, built from its sources."""
+    import oracle
+    from concurrent.futures import ThreadPoolExecutor
+    from anukulan_b200 import pdhg
+    from anukulan_b200.abi import OPTIMAL, PRECISION_FP32
+    if not oracle.have_reference_b200():
+        return {"unavailable": "oracle/_ref adapter build absent"}
+    threads = os.cpu_count() or 1
+    K = st.num_cases
+    cases = [st.case(k) for k in range(K)]
+    pdhg.solve_pdhg(st.base, tolerance=TOL, precision=PRECISION_FP32, device=device)  # warm-up
+
+    def warm_all(basis):
+        def one(k):
+            d, _ = oracle.ref_simplex_basis(cases[k], basis)
+            return d
+        with ThreadPoolExecutor(max_workers=threads) as ex:
+            return list(ex.map(one, range(K)))
+
+    t0 = time.perf_counter()
+    bounds = pdhg.solve_case_stack(st, tolerance=TOL, precision=PRECISION_FP32, device=device)
+    t1 = time.perf_counter()
+    base = pdhg.solve_pdhg(st.base, tolerance=TOL, precision=PRECISION_FP32, device=device)
+    t2 = time.perf_counter()
+    fin = oracle.ref_finish_simplex(st.base, base.x, base.y)
+    t3 = time.perf_counter()
+    warm = warm_all(fin["basis"])
+    misses = [k for k, d in enumerate(warm) if d["status"] != 0]
+    for k in misses:
+        own = oracle.ref_finish_simplex(cases[k], bounds[k].x, bounds[k].y)
+        warm[k] = {"status": own["status"], "objective": own["objective"], "pivots": own["pivots"]}
+    t4 = time.perf_counter()
+    r0 = time.perf_counter()
+    ref_base, ref_basis = oracle.ref_simplex_basis(st.base)
+    ref_warm = warm_all(ref_basis)
+    r1 = time.perf_counter()
+    exact = sum(int(d["status"] == 0) for d in warm)
+    agree = sum(int(a["status"] == 0 and b["status"] == 0 and
+                    abs(a["objective"] - b["objective"]) <= 1e-9 * max(1.0, abs(b["objective"])))
+                for a, b in zip(warm, ref_warm))
+    bound_err = max(abs(bounds[k].objective - ref_warm[k]["objective"])
+                    / max(1.0, abs(ref_warm[k]["objective"])) for k in range(K))
+    return {
+        "value": exact / (t4 - t0), "unit": "exact solves/s", "cases": K, "exact": exact,
+        "agree_with_reference_1e-9": agree, "threads": threads,
+        "seconds": {"engine_stack_bounds": t1 - t0, "engine_base_point": t2 - t1,
+                    "crossover_and_base_simplex": t3 - t2, "warm_dual_simplex": t4 - t3,
+                    "total": t4 - t0},
+        "base_pivots": {"from_crossover": fin["pivots"], "cold": ref_base["pivots"]},
+        "warm_pivots_median": float(np.median([d["pivots"] for d in warm])),
+        "warm_misses": len(misses),
+        "bounds_all_optimal": all(r.status == OPTIMAL for r in bounds),
+        "bound_objective_max_rel_error": bound_err,
+        "reference_family_from_first": {
+            "value": sum(int(d["status"] == 0) for d in ref_warm) / (r1 - r0),
+            "unit": "exact solves/s", "seconds": r1 - r0,
+            "cold_base_seconds": ref_base["seconds"],
+            "mode": "cold dual simplex on the base, every case warm from its basis, "
+                    f"{threads} host threads"},
+    }
+
+
 def fp64_single_case(st, device):
     """The stack's cases solved one after another by the engine's plain FP64
-    single-case mode (host arrays in, results out, like a solve_pdhg call)."""
+    single-case mode, host arrays in and results out: (a) a fresh
+    anu_pdhg_solve per case, (b) one handle whose scaled matrix and ||K|| are
+    kept, each case swapped in by anu_pdhg_set_case (the reference's backends
+    keep a prepared matrix per SparseMatrix::id() the same way)."""
     from anukulan_b200 import pdhg
     from anukulan_b200.abi import OPTIMAL, PRECISION_FP64, make_options
     opts = make_options(tolerance=TOL, precision=PRECISION_FP64, device=device)
@@ -460,9 +604,19 @@ def fp64_single_case(st, device):
         ok += int(r.status == OPTIMAL)
         iters += r.iterations
     dt = time.perf_counter() - t0
-    return {"value": ok / dt, "unit": "solves/s", "cases": st.num_cases, "optimal": ok,
-            "seconds": dt, "iterations_per_second": iters / dt,
-            "mode": "engine FP64, one case per solve, no batching"}
+    t1 = time.perf_counter()
+    h = pdhg.PdhgHandle(st.base, opts)
+    ok_h = 0
+    for k in range(st.num_cases):
+        h.set_case(st.c[k], st.q[k], st.lower[k], st.upper[k])
+        ok_h += int(h.run().status == OPTIMAL)
+    h.close()
+    dt_h = time.perf_counter() - t1
+    return {"value": ok_h / dt_h, "unit": "solves/s", "cases": st.num_cases, "optimal": ok_h,
+            "seconds": dt_h, "iterations_per_second": iters / dt_h,
+            "mode": "engine FP64, one case per run on one handle (matrix prepared once)",
+            "fresh_solve_per_case": {"value": ok / dt, "unit": "solves/s", "seconds": dt,
+                                     "mode": "engine FP64, anu_pdhg_solve per case"}}
 
 
 # -------------------------------------------------------------- our arm
@@ -611,12 +765,25 @@ def run_engine(args, rank, world, local_rank):
                          "launch_seconds": per_launch_s},
             "clocks": clk,
         }
-        if args.side:
-            out["spmv"] = spmv_leg(args.spmv_iterations, local_rank, peak)
-            out["fp64_single_case"] = fp64_single_case(st, local_rank)
-            out["stream"] = stream_leg(st, opts)
         if args.cpu_baseline:
             out["cpu_baseline"] = cpu_baseline(st, seconds=args.cpu_seconds)
+        legs = set(args.side_legs.split(",")) if args.side else set()
+        if "spmv" in legs:
+            out["spmv"] = spmv_leg(args.spmv_iterations, local_rank, peak)
+        if "fp64_single_case" in legs:
+            out["fp64_single_case"] = fp64_single_case(st, local_rank)
+        if "stream" in legs:
+            out["stream"] = stream_leg(st, opts)
+        if "exact_stack" in legs:
+            out["exact_stack"] = exact_stack_leg(st, local_rank)
+        if "adjoint" in legs:
+            out["adjoint"] = adjoint_leg(local_rank, steps=3, warmup=2, cpu=args.cpu_baseline)
+        if "packed" in legs:
+            out["packed"] = packed_leg(local_rank, steps=1, warmup=1, workers=args.packed_workers,
+                                       cpu=args.cpu_baseline, cpu_sample=16)
+        if "powerlaw" in legs:
+            out["powerlaw"] = powerlaw_leg(local_rank, TOL, ["fp32", "fp64"], 1, 300.0, peak,
+                                           cpu=args.cpu_baseline)
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
@@ -768,7 +935,9 @@ def main(argv=None):
                     help="comma list of spmv legs to run with --workload spmv "
                          "(fp32, fp64, fp32_relabelled, fp64_relabelled; default all)")
     ap.add_argument("--no-side", dest="side", action="store_false",
-                    help="skip the spmv and fp64 single-case side measurements")
+                    help="skip every side leg of the stack line")
+    ap.add_argument("--side-legs", default=",".join(SIDE_LEGS),
+                    help="comma list of the stack line's side legs: " + ", ".join(SIDE_LEGS))
     args = ap.parse_args(argv)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -295,6 +295,16 @@ int anu_pdhg_create(const anu_lp* lp, const anu_pdhg_options* options,
                     anu_pdhg** handle);
 int anu_pdhg_run(anu_pdhg* handle, const double* warm_x, const double* warm_y,
                  double* x, double* y, anu_pdhg_result* result);
+/* Replaces the handle's objective, right-hand side and bounds (n, m, n, n
+ * entries, the caller's order; NULL keeps that vector) and keeps its scaled
+ * matrix, product schedules and ||K~||, so the next anu_pdhg_run solves
+ * another LP with the same matrix without the set-up: the reference's
+ * backends keep a prepared matrix per SparseMatrix::id() the same way
+ * (src/anukulan/cuda_backend.cu:561-588). Scaling factors depend on the
+ * matrix alone, so the run is the one a fresh anu_pdhg_solve of that LP would
+ * make, bit for bit in FP64. */
+int anu_pdhg_set_case(anu_pdhg* handle, const double* c, const double* q,
+                      const double* lower, const double* upper);
 void anu_pdhg_destroy(anu_pdhg* handle);
 
 /* evaluate_residual, src/anukulan/pdhg.hpp:548 / pdhg.cpp:112-174: the FP64
