@@ -638,10 +638,30 @@ def run_engine(args, rank, world, local_rank):
                         split_stacks=0 if args.no_split else 1,
                         persistent_chunks=1 if args.persistent else 0)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    # Under torchrun the workload is the stack taken `world` times, sharded by
+    # case across the ranks (anukulan_b200.distributed): each rank solves its
+    # contiguous slice on its own GPU and one all-gather of the results gives
+    # every rank every case's answer. One rank: the stack itself, no gather.
+    full = st
+    if dist is not None:
+        from anukulan_b200 import distributed as D
+        from anukulan_b200.lpgen import CaseStack
+        full = CaseStack(st.base, st.names * world, np.tile(st.c, (world, 1)),
+                         np.tile(st.q, (world, 1)), np.tile(st.lower, (world, 1)),
+                         np.tile(st.upper, (world, 1)))
+        st = D.sub_stack(full, D.case_shard(full.num_cases, rank, world))
+        cfg = dict(cfg, cases=full.num_cases)
 
     def barrier():
         if dist is not None:
             dist.barrier()
+
+    def solve_all(local_solver):
+        """This rank's slice, then (several ranks) the results of every case."""
+        if dist is None:
+            return local_solver.solve(), local_solver.solve
+        res = D.solve_stack_sharded(full, solve=lambda _: local_solver.solve())
+        return res, None
 
     # value: data resident (handle created once), one solve per step
     solver = pdhg.CaseStackSolver(st.base, st.c, st.q, st.lower, st.upper, opts)
@@ -664,7 +684,7 @@ def run_engine(args, rank, world, local_rank):
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record()
-        res = solver.solve()
+        res, _ = solve_all(solver)
         e1.record()
         torch.cuda.synchronize()
         step_ms.append(e0.elapsed_time(e1))
@@ -689,7 +709,7 @@ def run_engine(args, rank, world, local_rank):
         h0 = time.perf_counter()
         s2 = pdhg.CaseStackSolver(st.base, st.c, st.q, st.lower, st.upper, opts)
         h1 = time.perf_counter()
-        r2 = s2.solve()
+        r2, _ = solve_all(s2)
         h2 = time.perf_counter()
         s2.close()
         h3 = time.perf_counter()
@@ -704,12 +724,9 @@ def run_engine(args, rank, world, local_rank):
         t = torch.tensor([total_ms, total_e2e], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms, total_e2e = float(t[0]), float(t[1])
-        s = torch.tensor([solved], device="cuda", dtype=torch.float64)
-        dist.all_reduce(s)
-        solved_all = int(s[0])
-    else:
-        solved_all = solved
-    cases_all = st.num_cases * args.steps * world
+    # After the gather every rank holds every case's result.
+    solved_all = solved
+    cases_all = full.num_cases * args.steps
     out = None
     if rank == 0:
         peak, peak_kind = hbm_peak()
@@ -738,7 +755,9 @@ def run_engine(args, rank, world, local_rank):
             "vs_baseline": None,
             "dtype": "f32",
             "data": "synthetic (seeded generator, refinery-shaped 60-case stack)",
-            "config": dict(cfg, parallelism=f"case stacks replicated per GPU x{world}"),
+            "config": dict(cfg, parallelism=(f"cases sharded over {world} GPUs, one result "
+                                             f"all-gather per step" if world > 1
+                                             else "one GPU")),
             "cases_optimal": solved_all,
             "cases_attempted": cases_all,
             "iterations_per_solve": total_iterations / args.steps,
@@ -746,7 +765,7 @@ def run_engine(args, rank, world, local_rank):
             "phases_ms_median": {k: round(1e3 * float(np.median([ph[k] for ph in phases])), 2)
                                  for k in phases[0]},
             "e2e": {"value": solved_all / (total_e2e / 1e3), "unit": "solves/s",
-                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                    "h2d_bytes_per_step": int(h2d) * world, "d2h_bytes_per_step": int(d2h) * world,
                     "parts_ms_median": ({k: round(1e3 * float(np.median([p[i] for p in e2e_parts])), 2)
                                          for i, k in enumerate(("create", "solve", "close"))}
                                         if e2e_parts else None),
