@@ -337,8 +337,17 @@ __device__ __forceinline__ Acc block_sum(Acc v, Acc* scratch) {
 // short rows match it bit for bit. Longer rows are listed in row order and
 // taken by whole warps (lane-strided partial sums, then a fixed shuffle
 // tree). A row longer than the block has a CTA to itself.
+//
+// The products sit in shared memory with one pad word after every 32
+// (prod_slot). A row's owner thread reads its products consecutively, so in
+// a block of equal-length rows the 32 threads of a warp read at a stride of
+// the row length: for 8-nonzero rows, unpadded, that is 4 distinct banks and
+// an 8-way conflict on every step of the sum. Padded, the warp's reads fall
+// in 32 distinct banks. Only the addresses change, not the order of a sum.
 constexpr int kSerialRow = 32;
 constexpr int kPerThread = kBlockNnz / kRowThreads;
+constexpr int kProdSlots = kBlockNnz + kBlockNnz / 32;
+__device__ __forceinline__ int prod_slot(int k) { return k + (k >> 5); }
 static_assert(kBlockRows <= kRowThreads, "one epilogue row per thread");
 static_assert(kBlockNnz >= kRowThreads, "block_sum scratch");
 
@@ -346,7 +355,7 @@ template <class V, class X, class Acc, class Epi>
 __global__ void __launch_bounds__(kRowThreads)
     rows_kernel(CsrView<V> a, const X* __restrict__ x, Epi epi) {
   constexpr int kWarps = kRowThreads / 32;
-  __shared__ Acc prod[kBlockNnz];
+  __shared__ Acc prod[kProdSlots];
   __shared__ Acc rowsum[kBlockRows];
   __shared__ int32_t long_rows[kBlockRows];
   __shared__ int32_t warp_long[kWarps];
@@ -412,12 +421,12 @@ __global__ void __launch_bounds__(kRowThreads)
     xv[q] = col[q] >= 0 ? static_cast<Acc>(x[col[q]]) : static_cast<Acc>(0);
 #pragma unroll
   for (int q = 0; q < kPerThread; ++q)
-    if (col[q] >= 0) prod[q * kRowThreads + t] = mul(static_cast<Acc>(val[q]), xv[q]);
+    if (col[q] >= 0) prod[prod_slot(q * kRowThreads + t)] = mul(static_cast<Acc>(val[q]), xv[q]);
   __syncthreads();
   const bool is_long = has_row && re - rb > kSerialRow;
   if (has_row && !is_long) {
     Acc s = 0;
-    for (int32_t k = rb; k < re; ++k) s = add(s, prod[k]);
+    for (int32_t k = rb; k < re; ++k) s = add(s, prod[prod_slot(k)]);
     rowsum[t] = s;
   }
   const int warp = t / 32;
@@ -439,7 +448,7 @@ __global__ void __launch_bounds__(kRowThreads)
     const int32_t b = a.start[r0 + row] - nz0;
     const int32_t e = a.start[r0 + row + 1] - nz0;
     Acc s = 0;
-    for (int32_t k = b + lane; k < e; k += 32) s = add(s, prod[k]);
+    for (int32_t k = b + lane; k < e; k += 32) s = add(s, prod[prod_slot(k)]);
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) s = add(s, __shfl_down_sync(0xffffffffu, s, off));
     if (lane == 0) rowsum[row] = s;
