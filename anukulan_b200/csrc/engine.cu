@@ -85,6 +85,10 @@ void DevCsr::upload(const HostCsr& a, bool with_fp32, cudaStream_t s, int32_t se
     if (nnz > 0)
       ANU_CUDA(cudaMemcpyAsync(v32.p, f.data(), sizeof(float) * nnz, cudaMemcpyHostToDevice, s));
   }
+  // Every row exactly kEllWidth long: ell_kernel takes the single-LP product.
+  bool uniform = rows > 0 && nnz == kEllWidth * rows;
+  for (int32_t r = 0; uniform && r <= rows; ++r) uniform = a.start[r] == kEllWidth * r;
+  uniform_len = uniform ? kEllWidth : 0;
   const std::vector<RowBlock> b = row_blocks(a, kBlockNnz, kBlockRows);
   num_blocks = static_cast<int32_t>(b.size());
   blocks.alloc(std::max<size_t>(b.size(), 1));
@@ -112,12 +116,12 @@ void DevCsr::upload(const HostCsr& a, bool with_fp32, cudaStream_t s, int32_t se
 template <>
 CsrView<double> DevCsr::view<double>() const {
   return {rows, cols, start.p, index.p, v64.p, blocks.p, num_blocks,
-          seg_begin.p, row_seg.p, cta_row.p, cta_seg.p, num_ctas, seg_per_cta};
+          seg_begin.p, row_seg.p, cta_row.p, cta_seg.p, num_ctas, seg_per_cta, uniform_len};
 }
 template <>
 CsrView<float> DevCsr::view<float>() const {
   return {rows, cols, start.p, index.p, v32.p, blocks.p, num_blocks,
-          seg_begin.p, row_seg.p, cta_row.p, cta_seg.p, num_ctas, seg_per_cta};
+          seg_begin.p, row_seg.p, cta_row.p, cta_seg.p, num_ctas, seg_per_cta, uniform_len};
 }
 
 Problem::~Problem() {

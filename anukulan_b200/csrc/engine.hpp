@@ -160,6 +160,7 @@ struct DevCsr {
   DevBuf<int32_t> seg_begin, row_seg, cta_row, cta_seg;
   int32_t num_ctas = 0;
   int32_t seg_per_cta = kSegPerCta;
+  int32_t uniform_len = 0;  // kEllWidth when every row has that many nonzeros
   // seg_nnz, seg_per_cta: the segment schedule's shape (at most
   // kSegPerCtaMax segments per CTA).
   void upload(const HostCsr& a, bool with_fp32, cudaStream_t s, int32_t seg_nnz = kSegNnz,

@@ -113,6 +113,9 @@ struct CsrView {
   const int32_t* __restrict__ cta_seg;
   int32_t num_ctas;
   int32_t seg_per_cta;
+  // kEllWidth when every row holds exactly that many nonzeros (start[r] =
+  // kEllWidth * r), so ell_kernel can take the product; 0 otherwise.
+  int32_t uniform_len;
 };
 
 // ------------------------------------------------------- per-case state
@@ -455,6 +458,86 @@ __global__ void __launch_bounds__(kRowThreads)
   }
   __syncthreads();
   if (has_row) epi.finish(r0 + t, 0, rowsum[t], pre);
+}
+
+// ------------------------------------------------------------ ell_kernel
+
+// One LP, a matrix whose rows all hold exactly kEllWidth nonzeros (the
+// transpose of an LP with that many nonzeros per column, such as K~' of the
+// power-law LP). Row r's nonzeros sit at kEllWidth * r, so one thread per row
+// loads its indices and values with 128-bit loads straight into registers
+// (before the PDL wait: they do not depend on the previous launch), issues
+// its kEllWidth gathers together, and sums the products left to right from
+// zero in registers with explicitly rounded multiplies and adds - the order
+// and roundings of rows_kernel's short-row path and of the reference, so the
+// result is the same bit for bit. No shared memory, no barrier.
+constexpr int kEllWidth = 8;
+
+__device__ __forceinline__ float strict_mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float strict_add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double strict_mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double strict_add(double a, double b) { return __dadd_rn(a, b); }
+
+template <class V>
+__device__ __forceinline__ void load_ell_row(const int32_t* __restrict__ index,
+                                             const V* __restrict__ value, int32_t r,
+                                             int32_t (&col)[kEllWidth], V (&val)[kEllWidth]) {
+  static_assert(kEllWidth % 4 == 0, "whole 16-byte vectors per row");
+  const int4* ip = reinterpret_cast<const int4*>(index + static_cast<size_t>(r) * kEllWidth);
+#pragma unroll
+  for (int v = 0; v < kEllWidth / 4; ++v) {
+    const int4 c = __ldg(ip + v);
+    col[4 * v] = c.x;
+    col[4 * v + 1] = c.y;
+    col[4 * v + 2] = c.z;
+    col[4 * v + 3] = c.w;
+  }
+  if constexpr (sizeof(V) == 4) {
+    const float4* vp = reinterpret_cast<const float4*>(value + static_cast<size_t>(r) * kEllWidth);
+#pragma unroll
+    for (int v = 0; v < kEllWidth / 4; ++v) {
+      const float4 w = __ldg(vp + v);
+      val[4 * v] = w.x;
+      val[4 * v + 1] = w.y;
+      val[4 * v + 2] = w.z;
+      val[4 * v + 3] = w.w;
+    }
+  } else {
+    const double2* vp =
+        reinterpret_cast<const double2*>(value + static_cast<size_t>(r) * kEllWidth);
+#pragma unroll
+    for (int v = 0; v < kEllWidth / 2; ++v) {
+      const double2 w = __ldg(vp + v);
+      val[2 * v] = w.x;
+      val[2 * v + 1] = w.y;
+    }
+  }
+}
+
+template <class V, class X, class Acc, class Epi>
+__global__ void __launch_bounds__(kRowThreads)
+    ell_kernel(CsrView<V> a, const X* __restrict__ x, Epi epi) {
+  const int32_t r = static_cast<int32_t>(blockIdx.x) * kRowThreads + static_cast<int32_t>(threadIdx.x);
+  const bool has_row = r < a.rows;
+  int32_t col[kEllWidth];
+  V val[kEllWidth];
+  typename Epi::Pre pre{};
+  if (has_row) {
+    load_ell_row(a.index, a.value, r, col, val);
+    pre = epi.prefetch(r, 0);
+  }
+  // ---- the gathers read the previous launch's output
+  pdl_wait();
+  pdl_launch();
+  if (!has_row) return;
+  Acc xv[kEllWidth];
+#pragma unroll
+  for (int q = 0; q < kEllWidth; ++q) xv[q] = static_cast<Acc>(x[col[q]]);
+  Acc s = 0;
+#pragma unroll
+  for (int q = 0; q < kEllWidth; ++q)
+    s = strict_add(s, strict_mul(static_cast<Acc>(val[q]), xv[q]));
+  epi.finish(r, 0, s, pre);
 }
 
 // ------------------------------------------------------------ seg_kernel

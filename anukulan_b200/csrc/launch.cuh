@@ -91,7 +91,19 @@ template <class V, class X, class Acc, class Epi, class Mat>
 void product(Exec& p, const Mat& a, const X* x, int K, const Epi& epi, bool pdl = false) {
   if (a.rows == 0) return;
   cudaStream_t s = p.stream;
-  if (K == 1) {
+  if (K == 1 && a.uniform_len == kEllWidth) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((a.rows + kRowThreads - 1) / kRowThreads);
+    cfg.blockDim = dim3(kRowThreads);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = pdl ? 1 : 0;
+    cuda_check(cudaLaunchKernelEx(&cfg, ell_kernel<V, X, Acc, Epi>, a.template view<V>(), x, epi),
+               "ell_kernel launch");
+  } else if (K == 1) {
     rows_kernel_setup<V, X, Acc, Epi>(s);
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(a.num_blocks);
