@@ -796,6 +796,10 @@ def run_engine(args, rank, world, local_rank):
         if args.cpu_baseline:
             out["cpu_baseline"] = cpu_baseline(st, seconds=args.cpu_seconds)
         legs = set(args.side_legs.split(",")) if args.side else set()
+        if world > 1:
+            # The other ranks would wait at the closing barrier, holding their
+            # GPUs; the side legs are single-GPU measurements, taken at N=1.
+            legs = set()
         if "spmv" in legs:
             out["spmv"] = spmv_leg(args.spmv_iterations, local_rank, peak)
         if "fp64_single_case" in legs:
