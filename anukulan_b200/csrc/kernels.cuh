@@ -26,6 +26,8 @@
 // (src/anukulan/backend.cpp:60-111 runs without contraction on x86-64).
 #pragma once
 
+#include <type_traits>
+#include <utility>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -184,6 +186,8 @@ struct PrimalEpi {
   struct Pre {
     T x, c, lo, hi, anchor, sum;
   };
+  // A retired case's lanes neither gather nor step.
+  __device__ __forceinline__ bool live(int32_t k) const { return p[k].active != 0; }
   __device__ __forceinline__ Pre prefetch(int32_t j, int32_t k) const {
     Pre r{};
     const StepParams& P = p[k];
@@ -255,6 +259,8 @@ struct DualEpi {
   struct Pre {
     T y, q, kx, anchor_y, anchor_kx, floor_v, sum;
   };
+  // A retired case's lanes neither gather nor step.
+  __device__ __forceinline__ bool live(int32_t k) const { return p[k].active != 0; }
   __device__ __forceinline__ Pre prefetch(int32_t i, int32_t k) const {
     Pre r{};
     const StepParams& P = p[k];
@@ -542,6 +548,18 @@ __global__ void __launch_bounds__(kRowThreads)
 
 // ------------------------------------------------------------ seg_kernel
 
+// Whether the lanes of case k take part in a product: an epilogue that can
+// retire cases says so through live(k); any other takes every case.
+template <class E, class = void>
+struct HasLive : std::false_type {};
+template <class E>
+struct HasLive<E, std::void_t<decltype(std::declval<const E&>().live(0))>> : std::true_type {};
+template <class E>
+__device__ __forceinline__ bool case_live(const E& e, int32_t k) {
+  if constexpr (HasLive<E>::value) return e.live(k);
+  else return true;
+}
+
 // The case-stack product in segments. A CTA owns a run of rows and their
 // segments; each group of L lanes takes one segment at a time: the group
 // loads the segment's indices and values once (one coalesced load), then
@@ -594,8 +612,15 @@ __global__ void __launch_bounds__(kMaxThreads)
   pdl_wait();
   pdl_launch();
   Acc acc[CPL];
+  // Retired cases skip their gathers too, not only their epilogue: near the
+  // end of a stack most lanes belong to retired cases.
+  bool live[CPL];
 #pragma unroll
-  for (int c = 0; c < CPL; ++c) acc[c] = 0;
+  for (int c = 0; c < CPL; ++c) {
+    acc[c] = 0;
+    const int32_t cs = lane + c * L;
+    live[c] = cs < K && case_live(epi, cs);
+  }
   const int32_t warp_len = __reduce_max_sync(0xffffffffu, static_cast<unsigned>(len));
   for (int32_t base = 0; base < warp_len; base += L) {
     int32_t idx = idx0;
@@ -616,10 +641,8 @@ __global__ void __launch_bounds__(kMaxThreads)
       if (base + t < len) {
         const X* xc = x + (size_t)col * K;
 #pragma unroll
-        for (int c = 0; c < CPL; ++c) {
-          const int32_t cs = lane + c * L;
-          if (cs < K) acc[c] = madd(acc[c], v, static_cast<Acc>(xc[cs]));
-        }
+        for (int c = 0; c < CPL; ++c)
+          if (live[c]) acc[c] = madd(acc[c], v, static_cast<Acc>(xc[lane + c * L]));
       }
     }
   }
