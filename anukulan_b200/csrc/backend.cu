@@ -43,6 +43,10 @@ struct BackendState {
   bool profiling = false;
   cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
   std::map<std::string, Timing> timings;
+  // Matrices prepared while profiling was on, described when prepared: the
+  // reference's solve_pdhg releases its matrices before it returns, which is
+  // before a caller asks for the report.
+  std::map<uint64_t, std::string> profiled_matrices;
 };
 
 BackendState& state() {
@@ -120,17 +124,24 @@ std::string profile_report(const BackendState& s) {
   std::snprintf(line, sizeof(line), "%-26s %12.6f %8.1f%% %12lld\n", "total on the device",
                 total, 100.0, calls);
   out += line;
-  if (!s.matrices.empty()) {
-    out += "\nprepared matrices (row-block schedule of the product kernel):\n";
-    for (const auto& [id, d] : s.matrices) {
-      std::snprintf(line, sizeof(line),
-                    "  id %-12llu %9d rows %10d nonzeros %7.2f per row %8d row blocks\n",
-                    static_cast<unsigned long long>(id), d->rows, d->nnz,
-                    d->rows > 0 ? static_cast<double>(d->nnz) / d->rows : 0.0, d->num_blocks);
-      out += line;
-    }
+  if (!s.profiled_matrices.empty()) {
+    out += "\nmatrices prepared while profiling (schedule of the product kernel):\n";
+    for (const auto& m : s.profiled_matrices) out += m.second;
   }
   return out;
+}
+
+std::string describe_matrix(uint64_t id, const DevCsr& d) {
+  char line[256];
+  if (d.uniform_len > 0)
+    std::snprintf(line, sizeof(line), "  id %-12llu %9d rows %10d nonzeros %7.2f per row  ell, %d per row\n",
+                  static_cast<unsigned long long>(id), d.rows, d.nnz,
+                  d.rows > 0 ? static_cast<double>(d.nnz) / d.rows : 0.0, d.uniform_len);
+  else
+    std::snprintf(line, sizeof(line), "  id %-12llu %9d rows %10d nonzeros %7.2f per row  %d row blocks\n",
+                  static_cast<unsigned long long>(id), d.rows, d.nnz,
+                  d.rows > 0 ? static_cast<double>(d.nnz) / d.rows : 0.0, d.num_blocks);
+  return line;
 }
 
 template <class F>
@@ -330,6 +341,7 @@ int anu_backend_prepare(uint64_t id, const anu_csr* a) {
     const anu::HostCsr h = anu::copy_csr(a->rows, a->cols, a->nnz, a->start, a->index, a->value);
     auto d = std::make_unique<anu::DevCsr>();
     d->upload(h, false, s.exec.stream);
+    if (s.profiling) s.profiled_matrices[id] = anu::describe_matrix(id, *d);
     s.matrices[id] = std::move(d);
   });
 }
@@ -480,7 +492,10 @@ int anu_backend_set_profiling(int32_t on) {
       ANU_CUDA(cudaEventCreate(&s.ev_stop));
     }
     s.profiling = on != 0;
-    if (!s.profiling) s.timings.clear();
+    if (!s.profiling) {
+      s.timings.clear();
+      s.profiled_matrices.clear();
+    }
   });
 }
 

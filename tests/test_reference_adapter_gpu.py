@@ -129,5 +129,8 @@ def test_adapter_profile_report(engine):
     # Two products per iteration at least.
     assert rows["multiply"][2] >= 2 * r.iterations
     assert abs(sum(v[1] for v in rows.values()) - 100.0) < 0.5
-    assert "prepared matrices" in report
+    # The matrices solve_pdhg prepared (K and K'), described although the
+    # solve has released them.
+    assert "matrices prepared while profiling" in report
+    assert report.count(" rows ") >= 2
     assert engine.backend_profile_report() == ""

@@ -15,11 +15,13 @@ import time
 import pytest
 
 from anukulan_b200 import lpgen
-from anukulan_b200.abi import PRECISION_FP32, TIME_LIMIT
+from anukulan_b200.abi import TIME_LIMIT
 
 pytestmark = pytest.mark.gpu
 
-# A tolerance the refinery LP cannot reach, so only the flag ends the run.
+# A tolerance FP64 iterates cannot reach on the refinery LP, so only the flag
+# ends the run. (FP32 iterates with re-centring refinement can: their FP64
+# base point reaches machine precision there, so these tests run in FP64.)
 RUN = dict(tolerance=1e-15, gap_tolerance=1e-15, max_iterations=50_000_000,
            time_limit_seconds=120.0, polish_feasibility=False)
 
@@ -55,7 +57,7 @@ def test_stop_flag_ends_a_case_stack(engine):
     st = lpgen.refinery_stack()
     sub = lpgen.CaseStack(st.base, st.names[:8], st.c[:8], st.q[:8], st.lower[:8], st.upper[:8])
     res, seconds = _run_and_stop(
-        lambda stop: engine.solve_case_stack(sub, stop=stop, precision=PRECISION_FP32, **RUN))
+        lambda stop: engine.solve_case_stack(sub, stop=stop, **RUN))
     assert len(res) == 8
     for r in res:
         assert r.status == TIME_LIMIT, r.message
