@@ -608,19 +608,21 @@ __global__ void __launch_bounds__(kMaxThreads)
     const int32_t t = threadIdx.x + q * threads;
     if (t < items) pre[q] = epi.prefetch(r0 + t / K, t % K);
   }
+  // Retired cases skip their gathers too, not only their epilogue: near the
+  // end of a stack most lanes belong to retired cases. The per-case flags are
+  // written before the chunk, so they are read before the wait.
+  bool live[CPL];
+#pragma unroll
+  for (int c = 0; c < CPL; ++c) {
+    const int32_t cs = lane + c * L;
+    live[c] = cs < K && case_live(epi, cs);
+  }
   // ---- the gather reads the previous launch's output.
   pdl_wait();
   pdl_launch();
   Acc acc[CPL];
-  // Retired cases skip their gathers too, not only their epilogue: near the
-  // end of a stack most lanes belong to retired cases.
-  bool live[CPL];
 #pragma unroll
-  for (int c = 0; c < CPL; ++c) {
-    acc[c] = 0;
-    const int32_t cs = lane + c * L;
-    live[c] = cs < K && case_live(epi, cs);
-  }
+  for (int c = 0; c < CPL; ++c) acc[c] = 0;
   const int32_t warp_len = __reduce_max_sync(0xffffffffu, static_cast<unsigned>(len));
   for (int32_t base = 0; base < warp_len; base += L) {
     int32_t idx = idx0;
