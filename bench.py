@@ -297,7 +297,7 @@ def run_packed(args, rank, world, local_rank):
     return out
 
 
-def adjoint_leg(local_rank, steps, warmup, cpu=True):
+def adjoint_leg(local_rank, steps, warmup, cpu=True, unrolled_steps=2000):
     """Sensitivities through the unrolled program: the 60-case refinery stack,
     2,000 FP32 iterations with checkpoints every 100, loss c_hat'x_T per
     case with c_hat = c (1 + 0.05 N(0,1)). A step is one forward pass (x_T
@@ -308,7 +308,7 @@ def adjoint_leg(local_rank, steps, warmup, cpu=True):
     stack, c_hat = lpgen.adjoint_case()
     ratio = c_hat / np.where(stack.base.c != 0, stack.base.c, 1.0)
     loss = stack.c * ratio
-    T, R = 2000, 100
+    T, R = unrolled_steps, 100
     opts = make_options(precision=PRECISION_FP32, device=local_rank)
     u = pdhg.UnrolledPdhg(stack.base, stack.c, stack.q, stack.lower, stack.upper,
                           iterations=T, checkpoint_every=R, options=opts)
@@ -361,9 +361,9 @@ def run_adjoint(args, rank, world, local_rank):
         return None
     import torch
     torch.cuda.set_device(local_rank)
-    leg = adjoint_leg(local_rank, args.steps, args.warmup, args.cpu_baseline)
+    leg = adjoint_leg(local_rank, args.steps, args.warmup, args.cpu_baseline, args.unrolled_steps)
     out = {
-        "metric": "unrolled-PDHG sensitivities/s (dL/dc, dL/dq per case, 2,000 FP32 iterations)",
+        "metric": f"unrolled-PDHG sensitivities/s (dL/dc, dL/dq per case, {args.unrolled_steps:,} FP32 iterations)",
         "n_gpus": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic (seeded generator, refinery-shaped 60-case stack)",
     }
@@ -954,6 +954,8 @@ def main(argv=None):
                     help="--workload powerlaw: relative KKT tolerance")
     ap.add_argument("--time-limit", type=float, default=300.0,
                     help="--workload powerlaw: seconds per solve")
+    ap.add_argument("--unrolled-steps", type=int, default=2000,
+                    help="--workload adjoint: unrolled PDHG steps (profiling runs use fewer)")
     ap.add_argument("--packed-workers", type=int, default=0,
                     help="LPs in flight for --workload packed (0: autotune)")
     ap.add_argument("--spmv-iterations", type=int, default=2000)

