@@ -957,6 +957,20 @@ void upload_slot(cudaStream_t s, T* dst, int32_t len, int K, int k, const std::v
                              len, cudaMemcpyHostToDevice, s));
 }
 
+// Keeps the cases `keep` (in that order) of a case-interleaved array of
+// `len` rows and K cases, as an array of keep.size() cases. Unallocated
+// arrays stay unallocated.
+template <class T>
+void keep_cases(cudaStream_t s, DevBuf<T>& buf, int32_t len, int K, const std::vector<int>& keep) {
+  if (buf.p == nullptr || len <= 0) return;
+  const int K2 = static_cast<int>(keep.size());
+  DevBuf<T> kept(static_cast<size_t>(len) * K2);
+  for (int j = 0; j < K2; ++j)
+    ANU_CUDA(cudaMemcpy2DAsync(kept.p + j, sizeof(T) * K2, buf.p + keep[j], sizeof(T) * K,
+                               sizeof(T), len, cudaMemcpyDeviceToDevice, s));
+  buf = std::move(kept);
+}
+
 template <class T>
 void zero_slot(cudaStream_t s, T* dst, int32_t len, int K, int k) {
   if (len == 0 || dst == nullptr) return;
@@ -1085,7 +1099,9 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
                  AdmissionQueue* queue) {
   // The case in each slot; a rolling stack replaces retired ones.
   std::vector<const CaseData*> cases(initial_cases);
-  const int K = static_cast<int>(cases.size());
+  // Slots of the stack; a stack whose last cases run on alone is compacted
+  // to fewer slots (compact() below), so K can shrink during the run.
+  int K = static_cast<int>(cases.size());
   const int32_t n = p.n, m = p.m;
   results->assign(K, CaseResult{});
   if (K == 0) return;
@@ -1245,8 +1261,8 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
     oq[k] = &cases[k]->q;
     if (!cases[k]->ylo.empty()) any_ylo = true;
   }
-  const size_t NK = static_cast<size_t>(std::max(n, 1)) * K;
-  const size_t MK = static_cast<size_t>(std::max(m, 1)) * K;
+  size_t NK = static_cast<size_t>(std::max(n, 1)) * K;
+  size_t MK = static_cast<size_t>(std::max(m, 1)) * K;
   upload_interleaved(st, w.x, n, K, vx);
   upload_interleaved(st, w.y, m, K, vy);
   upload_interleaved(st, w.c, n, K, vc);
@@ -1690,6 +1706,10 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
   };
 
   std::vector<CaseResult>* R_ptr = results;
+  // The caller's slot of each current slot: results stay in the caller's
+  // order when the stack is compacted.
+  std::vector<int> orig(K);
+  std::iota(orig.begin(), orig.end(), 0);
   // Refinement at a check: fold every active case's FP32 offset into its FP64
   // base and re-form the correction LP from the FP64 residual there.
   auto recenter = [&]() {
@@ -1732,13 +1752,13 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
       p.launches += 3;
     });
     for (int k = 0; k < K; ++k)
-      if (mk[k]) ++R_ptr->at(k).r.refinement_rounds;
+      if (mk[k]) ++R_ptr->at(orig[k]).r.refinement_rounds;
   };
 
   int32_t iteration = 0;
   std::vector<CaseResult>& R = *results;
   for (int k = 0; k < K; ++k) {
-    R[k].r.matrix_norm_estimate = p.matrix_norm;
+    R[orig[k]].r.matrix_norm_estimate = p.matrix_norm;
   }
   double t_setup = phase_end();
   double t_iter = 0.0, t_checks = 0.0, t_polish = 0.0;
@@ -1783,7 +1803,7 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
     std::vector<int> exit_polish;
     for (int k : ks) {
       CaseState& c = S[k];
-      CaseResult& cr = R[k];
+      CaseResult& cr = R[orig[k]];
       if (c.have_polished) {
         cr.x = c.polished_x;
         cr.y = c.polished_y;
@@ -1827,7 +1847,7 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
       t_polish += phase_end();
       for (size_t i = 0; i < exits.size(); ++i) {
         const int k = exits[i];
-        CaseResult& cr = R[k];
+        CaseResult& cr = R[orig[k]];
         ++cr.r.polish_attempts;
         cr.r.polish_iterations += spent[i];
         const anu_pdhg_residual& cur = cr.r.residual;
@@ -1857,7 +1877,7 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
     }
     t_checks += phase_end();
     for (int k : ks) {
-      CaseResult& cr = R[k];
+      CaseResult& cr = R[orig[k]];
       double cx = 0.0;
       for (int32_t j = 0; j < n; ++j) cx += cases[k]->c[j] * cr.x[j];
       cr.r.objective = cases[k]->objective_scale * cx + cases[k]->objective_offset;
@@ -1906,8 +1926,8 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
     if (o.initial_primal_weight > 0.0) omega = o.initial_primal_weight;
     S[k].eta = eta;
     S[k].omega = omega;
-    R[k] = CaseResult{};
-    R[k].r.matrix_norm_estimate = p.matrix_norm;
+    R[orig[k]] = CaseResult{};
+    R[orig[k]].r.matrix_norm_estimate = p.matrix_norm;
     vc[k] = &d->cs;
     vl[k] = &d->ls;
     vu[k] = &d->us;
@@ -1989,6 +2009,60 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
     ANU_CUDA(cudaStreamSynchronize(st));
     // Nothing in this run points at the outgoing case any more.
     if (queue->release && outgoing != nullptr && outgoing != d) queue->release(outgoing);
+  };
+
+  // The lockstep tail. A stack's cases retire at different iterations, and
+  // its last case often runs on alone for half of the stack's time while the
+  // launches still carry every slot. Once at most 1/kTailRatio of the slots
+  // are active, the retired cases are finalized and every per-case array is
+  // compacted to the active cases, so the products run narrower launches (a
+  // single case takes the single-LP kernels). Each case's state moves with
+  // it unchanged. FP32 stacks only: FP64 stacks stay in their layout, whose
+  // results equal separate solves bit for bit. Not for rolling stacks (their
+  // slots take new cases) or polishing sub-stacks.
+  constexpr int kTailRatio = 8;
+  const bool compact_tail = !fp64 && queue == nullptr && !persistent && !slow && !sub_run &&
+                            K >= kTailRatio;
+  auto compact = [&]() {
+    std::vector<int> keep, drop;
+    for (int k = 0; k < K; ++k) (S[k].active ? keep : drop).push_back(k);
+    finalize(drop);
+    const int K2 = static_cast<int>(keep.size());
+    for (DevBuf<T>* b : {&w.x, &w.x_bar, &w.anchor_x, &w.dx, &w.c, &w.lo, &w.hi, &w.x_next,
+                         &w.sum_x, &w.avg_x, &w.x_restart, &w.x_prev})
+      keep_cases(st, *b, n, K, keep);
+    for (DevBuf<T>* b : {&w.y, &w.kx, &w.anchor_y, &w.anchor_kx, &w.dy, &w.q, &w.k_dx, &w.y_next,
+                         &w.k_next, &w.sum_y, &w.avg_y, &w.y_restart, &w.y_prev, &w.ylo})
+      keep_cases(st, *b, m, K, keep);
+    for (DevBuf<double>* b : {&w.kty64, &w.ktdy64, &w.c0, &w.lo0, &w.hi0, &w.los, &w.his, &w.xb,
+                              &w.x_comb, &w.c0s, &w.l0s, &w.u0s})
+      keep_cases(st, *b, n, K, keep);
+    for (DevBuf<double>* b : {&w.kx64, &w.q0, &w.qs, &w.yb, &w.y_comb, &w.q0s, &w.kshift})
+      keep_cases(st, *b, m, K, keep);
+    keep_cases(st, w.sum_weight, 1, K, keep);
+    auto pick = [&](auto& v) {
+      std::remove_reference_t<decltype(v)> kept;
+      for (int k : keep) kept.push_back(std::move(v[k]));
+      v = std::move(kept);
+    };
+    pick(S);
+    pick(origin);
+    pick(cases);
+    pick(orig);
+    for (auto* v : {&vx, &vy, &vc, &vl, &vu, &vq, &oc, &ol, &ou, &oq}) pick(*v);
+    K = K2;
+    w.K = K2;
+    NK = static_cast<size_t>(std::max(n, 1)) * K;
+    MK = static_cast<size_t>(std::max(m, 1)) * K;
+    ylo_ptr = any_ylo ? w.ylo.p : nullptr;
+    // Graphs hold the old layout's pointers and widths.
+    for (auto& g : w.graphs) cudaGraphExecDestroy(g.second);
+    w.graphs.clear();
+    for (auto* r : {&w.check_replay, &w.recenter_replay}) {
+      if (r->exec) cudaGraphExecDestroy(r->exec);
+      *r = typename Workspace<T>::Replay{};
+    }
+    ANU_CUDA(cudaStreamSynchronize(st));
   };
 
   while ((queue != nullptr || iteration < o.max_iterations) && any_active()) {
@@ -2106,7 +2180,7 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
           c.halpern_k >= o.halpern_minimum_epoch) {
         if (c.movement <= c.epoch_start_movement / 7.389056098930650) {
           c.anchor_needs_reset = true;
-          ++R[0].r.restarts;
+          ++R[orig[0]].r.restarts;
         }
       }
     }
@@ -2160,7 +2234,7 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
         const bool bad = tc[7] > 0.0 || tc[kRowTerms + 8] > 0.0 || !(scale > 0.0);
         if (!bad && (tc[8] - tc[kRowTerms + 7]) / scale > o.infeasibility_tolerance) {
           c.status = ANU_PDHG_PRIMAL_INFEASIBLE;
-          set_message(&R[k].r, "Farkas certificate found in the dual iterate difference");
+          set_message(&R[orig[k]].r, "Farkas certificate found in the dual iterate difference");
           c.final_iteration = it_idx + 1 - origin[k];
           c.active = false;
           continue;
@@ -2183,7 +2257,7 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
       rr[k] = r;
       if (!std::isfinite(r.primal_residual) || !std::isfinite(r.dual_residual)) {
         c.status = ANU_PDHG_NUMERICAL_ERROR;
-        set_message(&R[k].r, "iterates stopped being finite");
+        set_message(&R[orig[k]].r, "iterates stopped being finite");
         c.final_iteration = it_idx + 1 - origin[k];
         adopt_mask[k] = c.use_average;
         c.active = false;
@@ -2266,18 +2340,18 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
       for (size_t i = 0; i < polish_cases.size(); ++i) {
         const int k = polish_cases[i];
         CaseState& c = S[k];
-        ++R[k].r.polish_attempts;
-        R[k].r.polish_iterations += spent[i];
+        ++R[orig[k]].r.polish_attempts;
+        R[orig[k]].r.polish_iterations += spent[i];
         if (converged(pr[i], tolerance, o.absolute_tolerance, inf_norm, gap_tolerance)) {
           c.polished_x = px[i];
           c.polished_y = py[i];
-          R[k].xs = pxs[i];
-          R[k].ys = pys[i];
+          R[orig[k]].xs = pxs[i];
+          R[orig[k]].ys = pys[i];
           c.polished_residual = pr[i];
           c.have_polished = true;
-          R[k].r.polished = 1;
+          R[orig[k]].r.polished = 1;
           c.status = ANU_PDHG_OPTIMAL;
-          set_message(&R[k].r, "converged after feasibility polishing");
+          set_message(&R[orig[k]].r, "converged after feasibility polishing");
           c.final_iteration = it_idx + 1 - origin[k];
           c.active = false;
         }
@@ -2370,7 +2444,7 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
                                            : &h_kkt.p[static_cast<size_t>(k) * kKktTerms];
           c.kkt_at_restart = kkt_value(kt, c.omega);
         }
-        ++R[k].r.restarts;
+        ++R[orig[k]].r.restarts;
       }
       if (!o.pid_primal_weight) {
         masked_copy<T, T>(p, n, K, w.mask.p, w.x_restart.p, w.x_prev.p);
@@ -2411,6 +2485,14 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
       }
     }
     t_checks += phase_end();
+    if (compact_tail) {
+      int active = 0;
+      for (int k = 0; k < K; ++k) active += S[k].active ? 1 : 0;
+      if (active > 0 && active * kTailRatio <= K) {
+        compact();
+        t_checks += phase_end();
+      }
+    }
   }
   if (persistent) {
     ANU_CUDA(cudaStreamSynchronize(st));

@@ -305,6 +305,36 @@ def test_case_stack_objectives_within_1e6_of_simplex(engine, stack, precision):
         assert abs(r.objective - ref_obj) <= 1e-6 * abs(ref_obj), (k, r.objective, ref_obj)
 
 
+def test_case_stack_tail_compaction(engine, stack):
+    # An FP32 stack compacts its per-case arrays to the active cases once at
+    # most an eighth of its slots are active: 64 cases (the 60, then cases
+    # 0-3 again) go to 8 slots and then to the one case still running, which
+    # then takes the single-LP kernels. Every case must come back in its own
+    # slot with its own answer: the objective of its simplex golden to 1e-6,
+    # the duplicates equal to their originals, every returned point converged
+    # in FP64 (sampled), and the hardest case - the one that finishes in the
+    # compacted layout - within two check periods of its separate solve.
+    g = np.load(SIMPLEX)["refinery/objective"]
+    idx = list(range(60)) + [0, 1, 2, 3]
+    sub = _rolling(stack, idx)
+    res = engine.solve_case_stack(sub, tolerance=1e-6, gap_tolerance=5e-7,
+                                  precision=PRECISION_FP32, split_stacks=0)
+    assert len(res) == 64
+    for slot, (k, r) in enumerate(zip(idx, res)):
+        assert r.status == OPTIMAL, (slot, r.message)
+        assert abs(r.objective - g[k]) <= 1e-6 * abs(g[k]), (slot, r.objective, g[k])
+    for dup in range(4):
+        assert res[60 + dup].iterations == res[dup].iterations
+        assert abs(res[60 + dup].objective - res[dup].objective) <= 1e-9 * abs(res[dup].objective)
+    hard = int(np.argmax([r.iterations for r in res]))
+    for slot in (hard, 5, 33, 47):
+        rr = oracle.oracle_residual(stack.case(idx[slot]), res[slot].x, res[slot].y)
+        assert rr.converged(1e-6), (slot, rr)
+    alone = engine.solve_pdhg(stack.case(idx[hard]), tolerance=1e-6, gap_tolerance=5e-7,
+                              precision=PRECISION_FP32)
+    assert abs(alone.iterations - res[hard].iterations) <= 80, (alone.iterations, res[hard].iterations)
+
+
 @pytest.mark.parametrize("precision", [0, PRECISION_FP32])
 def test_case_stack_graphs_bit_identical(engine, stack, precision):
     # Iteration chunks, termination checks and re-centrings replayed as CUDA
