@@ -2013,16 +2013,18 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
 
   // The lockstep tail. A stack's cases retire at different iterations, and
   // its last case often runs on alone for half of the stack's time while the
-  // launches still carry every slot. Once at most 1/kTailRatio of the slots
-  // are active, the retired cases are finalized and every per-case array is
-  // compacted to the active cases, so the products run narrower launches (a
-  // single case takes the single-LP kernels). Each case's state moves with
-  // it unchanged. FP32 stacks only: FP64 stacks stay in their layout, whose
-  // results equal separate solves bit for bit. Not for rolling stacks (their
-  // slots take new cases) or polishing sub-stacks.
-  constexpr int kTailRatio = 8;
+  // launches still carry every slot. When a single case is left, the retired
+  // cases are finalized and every per-case array is compacted to that case,
+  // which then runs the single-LP kernels. Its state moves with it unchanged.
+  // Only a single case gains: the stack kernel's lane groups narrow with the
+  // case count, and a few cases walk each segment in more dependent rounds
+  // than many do. FP32 stacks of at least kTailStack cases only: FP64 stacks
+  // stay in their layout, whose results equal separate solves bit for bit.
+  // Not for rolling stacks (their slots take new cases) or polishing
+  // sub-stacks.
+  constexpr int kTailStack = 8;
   const bool compact_tail = !fp64 && queue == nullptr && !persistent && !slow && !sub_run &&
-                            K >= kTailRatio;
+                            K >= kTailStack;
   auto compact = [&]() {
     std::vector<int> keep, drop;
     for (int k = 0; k < K; ++k) (S[k].active ? keep : drop).push_back(k);
@@ -2488,7 +2490,7 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
     if (compact_tail) {
       int active = 0;
       for (int k = 0; k < K; ++k) active += S[k].active ? 1 : 0;
-      if (active > 0 && active * kTailRatio <= K) {
+      if (active == 1 && K > 1) {
         compact();
         t_checks += phase_end();
       }

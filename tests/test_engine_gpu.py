@@ -306,10 +306,9 @@ def test_case_stack_objectives_within_1e6_of_simplex(engine, stack, precision):
 
 
 def test_case_stack_tail_compaction(engine, stack):
-    # An FP32 stack compacts its per-case arrays to the active cases once at
-    # most an eighth of its slots are active: 64 cases (the 60, then cases
-    # 0-3 again) go to 8 slots and then to the one case still running, which
-    # then takes the single-LP kernels. Every case must come back in its own
+    # An FP32 stack compacts its per-case arrays to its last running case,
+    # which then takes the single-LP kernels: 64 cases (the 60, then cases
+    # 0-3 again), one stack. Every case must come back in its own
     # slot with its own answer: the objective of its simplex golden to 1e-6,
     # the duplicates equal to their originals, every returned point converged
     # in FP64 (sampled), and the hardest case - the one that finishes in the
