@@ -430,14 +430,23 @@ def test_cached_blocks_reused_across_solvers(engine, stack):
 def test_persistent_chunks_match_graphs(engine, stack, precision):
     # One cooperative launch per chunk runs the same arithmetic in the same
     # order as the two launches per iteration of the graphs: identical
-    # iterates, iteration counts and restarts, case by case.
+    # iterates, iteration counts and restarts, case by case. In FP32 the
+    # graph path hands the stack's last running case to the single-LP
+    # kernels once it runs alone (tail compaction; the persistent path does
+    # not), so that one case's FP32 sums round differently from there on:
+    # same status, iterations and restarts, iterates equal to rounding.
     kw = dict(tolerance=1e-6, precision=precision, split_stacks=0)
     persistent = engine.solve_case_stack(stack, persistent_chunks=1, **kw)
     graphs = engine.solve_case_stack(stack, persistent_chunks=0, **kw)
+    last = int(np.argmax([r.iterations for r in graphs]))
     for k, (a, b) in enumerate(zip(persistent, graphs)):
         assert a.status == b.status == OPTIMAL, (k, a.message)
         assert a.iterations == b.iterations and a.restarts == b.restarts, k
-        assert np.array_equal(a.x, b.x) and np.array_equal(a.y, b.y), k
+        if precision == PRECISION_FP32 and k == last:
+            np.testing.assert_allclose(a.x, b.x, rtol=1e-6, atol=1e-6 * np.abs(b.x).max())
+            np.testing.assert_allclose(a.y, b.y, rtol=1e-6, atol=1e-6 * np.abs(b.y).max())
+        else:
+            assert np.array_equal(a.x, b.x) and np.array_equal(a.y, b.y), k
     assert persistent[0].kernel_launches < graphs[0].kernel_launches
 
 
