@@ -1543,13 +1543,19 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
   // With profiling, the chunk's events are read once the stream has passed
   // them (at the next read-back), so timing adds no wait of its own.
   int pending_timed = 0;
+  // Only chunks at the stack's full width count: after tail compaction the
+  // last case's single-LP chunks would mix another kernel into the mean.
+  const int full_width = K;
+  int pending_width = 0;
   auto collect_chunk_time = [&]() {
     if (!o.profile || pending_timed == 0) return;
     ANU_CUDA(cudaEventSynchronize(ev_end));
     float ms = 0.0f;
     ANU_CUDA(cudaEventElapsedTime(&ms, ev_begin, ev_end));
-    device_iter_s += 1e-3 * ms;
-    device_iters += pending_timed;
+    if (pending_width == full_width) {
+      device_iter_s += 1e-3 * ms;
+      device_iters += pending_timed;
+    }
     pending_timed = 0;
   };
   auto run_chunk = [&](int len, bool check_at_end) {
@@ -1559,6 +1565,7 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
     if (o.profile) {
       ANU_CUDA(cudaEventRecord(ev_end, st));
       pending_timed = len;
+      pending_width = K;
     }
   };
 

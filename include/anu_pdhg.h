@@ -247,7 +247,9 @@ typedef struct anu_pdhg_result {
   int32_t kernel_launches;   /* kernels this solve launched (graph nodes included) */
   /* With options.profile: device time of the iteration chunks (CUDA events
    * on the engine stream) and the iterations they ran, summed over every
-   * case run this result shares (a case stack runs its cases together). */
+   * case run this result shares (a case stack runs its cases together). A
+   * stack whose last case was handed to the single-LP kernels counts its
+   * full-width chunks only. */
   double device_iteration_seconds;
   int64_t device_iterations;
   char message[160];
