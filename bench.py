@@ -672,6 +672,9 @@ def run_engine(args, rank, world, local_rank):
         res = D.solve_stack_sharded(full, solve=lambda _: local_solver.solve())
         return res, None
 
+    # The engine runs a stack of 16 or more cases as two half-stacks of
+    # alternate cases.
+    split_run = st.num_cases >= 16 and not args.no_split and not args.persistent
     # value: data resident (handle created once), one solve per step
     solver = pdhg.CaseStackSolver(st.base, st.c, st.q, st.lower, st.upper, opts)
     for _ in range(args.warmup):
@@ -701,7 +704,13 @@ def run_engine(args, rank, world, local_rank):
         solved += sum(1 for r in res if r.status == OPTIMAL)
         dev_iter_s += res[0].device_iteration_seconds
         dev_iters += res[0].device_iterations
-        launches += res[0].kernel_launches
+        # Each result counts its own half-stack's launches up to the moment it
+        # was finalized; the last one of each half has them all. Under torchrun
+        # the results are every rank's slice, in rank order.
+        for r0 in range(0, len(res), st.num_cases):
+            mine = res[r0:r0 + st.num_cases]
+            halves = (mine[0::2], mine[1::2]) if (split_run and len(mine) > 1) else (mine,)
+            launches += sum(max(r.kernel_launches for r in h) for h in halves if h)
         total_iterations += max(r.iterations for r in res)
     clk = clocks.stop()
     solver.close()
