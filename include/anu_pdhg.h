@@ -434,7 +434,11 @@ int anu_backend_convergence_terms_noalloc(int64_t n, int64_t m, const double* c,
  * runs as one SpMM-shaped iteration over case-interleaved vectors: every
  * nonzero of the matrix read serves all active cases. Each case keeps its own
  * step size, primal weight, restarts and termination; a case that terminates
- * is retired, and its lanes skip their updates from then on.
+ * is retired, and its lanes skip their gathers and updates from then on. In
+ * FP32, a stack of 8 or more cases whose last case runs on alone moves that
+ * case, state unchanged, to the single-LP kernels, which are quicker for one
+ * case; its FP32 sums then round as a single solve's do. FP64 stacks keep
+ * their layout.
  *
  * Case arrays are case-major: c[k*n + j], q[k*m + i], and so on. A NULL case
  * array means every case uses the base LP's vector. */
