@@ -60,7 +60,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
             if src.endswith(".cu"):
                 cmd = [nvcc()] + ARCH + NVCC_FLAGS + ["-c", src, "-o", obj]
             else:
-                cmd = [nvcc(), "-x", "c++"] + NVCC_FLAGS + ["-c", src, "-o", obj]
+                cmd = [nvcc(), "-x", "c++"] + ARCH + NVCC_FLAGS + ["-c", src, "-o", obj]
             jobs.append(cmd)
 
     def run(cmd):

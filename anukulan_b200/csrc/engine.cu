@@ -829,12 +829,6 @@ struct CaseState {
   ResidualScales scales{};
 };
 
-double worst_relative(const anu_pdhg_residual& r, bool inf) {
-  double w = std::fmax(r.relative_primal, std::fmax(r.relative_dual, r.relative_gap));
-  if (inf) w = std::fmax(w, std::fmax(r.relative_primal_inf, r.relative_dual_inf));
-  return w;
-}
-
 int32_t polish_budget(const anu_pdhg_options& o, int32_t at_iteration) {
   int32_t budget = static_cast<int32_t>(o.polish_iteration_factor * static_cast<double>(at_iteration + 1));
   budget = std::max(budget, o.polish_minimum_iterations);
