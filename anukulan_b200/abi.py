@@ -59,7 +59,7 @@ class anu_pdhg_options(C.Structure):
         ("stop", C.POINTER(C.c_uint8)),
         ("precision", i32), ("refinement", i32), ("device", i32), ("use_graphs", i32),
         ("profile", i32), ("split_stacks", i32), ("persistent_chunks", i32),
-        ("locality_order", i32), ("scaling_on_device", i32),
+        ("locality_order", i32), ("scaling_on_device", i32), ("tile_threads", i32),
     ]
 
 
@@ -86,6 +86,8 @@ class anu_pdhg_result(C.Structure):
         ("col_spread_before", f64), ("col_spread_after", f64),
         ("refinement_rounds", i32), ("kernel_launches", i32),
         ("device_iteration_seconds", f64), ("device_iterations", C.c_int64),
+        ("row_product_threads", i32), ("column_product_threads", i32),
+        ("tile_trial_seconds", f64),
         ("message", C.c_char * 160),
     ]
 
@@ -106,7 +108,7 @@ DEFAULTS = dict(
     known_matrix_norm=0.0, initial_step_size=0.0, initial_primal_weight=0.0,
     verbose=0, log_frequency=5000, precision=0, refinement=1,
     device=0, use_graphs=1, profile=0, split_stacks=1,
-    persistent_chunks=0, locality_order=0, scaling_on_device=1,
+    persistent_chunks=0, locality_order=0, scaling_on_device=1, tile_threads=0,
 )
 
 
@@ -203,6 +205,11 @@ class PdhgResult:
     device_iteration_seconds: float
     device_iterations: int
     message: str
+    # Single-LP product tiles (CTA sizes) of K~ x and K~' y, and the time of
+    # the trial solves that chose them (0 when the option fixed them).
+    row_product_threads: int = 128
+    column_product_threads: int = 128
+    tile_trial_seconds: float = 0.0
 
     @property
     def status_name(self) -> str:
@@ -219,7 +226,8 @@ class PdhgResult:
             (r.row_spread_before, r.row_spread_after, r.col_spread_before,
              r.col_spread_after),
             r.refinement_rounds, r.kernel_launches, r.device_iteration_seconds,
-            r.device_iterations, r.message.decode(errors="replace"))
+            r.device_iterations, r.message.decode(errors="replace"),
+            r.row_product_threads, r.column_product_threads, r.tile_trial_seconds)
 
 
 def _ptr(a: np.ndarray, ctype):

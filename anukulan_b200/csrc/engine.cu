@@ -89,15 +89,19 @@ void DevCsr::upload(const HostCsr& a, bool with_fp32, cudaStream_t s, int32_t se
   bool uniform = rows > 0 && nnz == kEllWidth * rows;
   for (int32_t r = 0; uniform && r <= rows; ++r) uniform = a.start[r] == kEllWidth * r;
   uniform_len = uniform ? kEllWidth : 0;
-  const std::vector<RowBlock> b = row_blocks(a, kBlockNnz, kBlockRows);
-  num_blocks = static_cast<int32_t>(b.size());
-  blocks.alloc(std::max<size_t>(b.size(), 1));
-  std::vector<RowBlockDev> bd(b.size());
-  for (size_t i = 0; i < b.size(); ++i)
-    bd[i] = {b[i].row_begin, b[i].row_end, a.start[b[i].row_begin], a.start[b[i].row_end]};
-  if (!bd.empty())
-    ANU_CUDA(cudaMemcpyAsync(blocks.p, bd.data(), sizeof(RowBlockDev) * bd.size(),
-                             cudaMemcpyHostToDevice, s));
+  for (int i = 0; i < 2; ++i) {
+    const int32_t threads = kTileThreads[i];
+    const std::vector<RowBlock> b = row_blocks(a, threads * kPerThread, threads, kLongRow);
+    std::vector<RowBlockDev> bd(b.size());
+    for (size_t j = 0; j < b.size(); ++j)
+      bd[j] = {b[j].row_begin, b[j].row_end, a.start[b[j].row_begin], a.start[b[j].row_end]};
+    tile_num_blocks[i] = static_cast<int32_t>(bd.size());
+    tile_blocks[i].alloc(std::max<size_t>(bd.size(), 1));
+    if (!bd.empty())
+      ANU_CUDA(cudaMemcpyAsync(tile_blocks[i].p, bd.data(), sizeof(RowBlockDev) * bd.size(),
+                               cudaMemcpyHostToDevice, s));
+  }
+  set_tile(kRowThreads);
   const SegmentSchedule sch = segment_schedule(a, seg_nnz, seg_per, kSegRows);
   seg_per_cta = seg_per;
   num_ctas = static_cast<int32_t>(sch.cta_row.size()) - 1;
@@ -113,15 +117,25 @@ void DevCsr::upload(const HostCsr& a, bool with_fp32, cudaStream_t s, int32_t se
   ANU_CUDA(cudaStreamSynchronize(s));
 }
 
+void DevCsr::set_tile(int32_t threads) {
+  const int i = threads == kTileThreads[1] ? 1 : 0;
+  if (threads != kTileThreads[i]) throw Error(ANU_ERR_INVALID, "tile size must be 128 or 256 threads");
+  blocks = tile_blocks[i].p;
+  num_blocks = tile_num_blocks[i];
+  tile_threads = threads;
+}
+
 template <>
 CsrView<double> DevCsr::view<double>() const {
-  return {rows, cols, start.p, index.p, v64.p, blocks.p, num_blocks,
-          seg_begin.p, row_seg.p, cta_row.p, cta_seg.p, num_ctas, seg_per_cta, uniform_len};
+  return {rows, cols, start.p, index.p, v64.p, blocks, num_blocks,
+          seg_begin.p, row_seg.p, cta_row.p, cta_seg.p, num_ctas, seg_per_cta, uniform_len,
+          tile_threads};
 }
 template <>
 CsrView<float> DevCsr::view<float>() const {
-  return {rows, cols, start.p, index.p, v32.p, blocks.p, num_blocks,
-          seg_begin.p, row_seg.p, cta_row.p, cta_seg.p, num_ctas, seg_per_cta, uniform_len};
+  return {rows, cols, start.p, index.p, v32.p, blocks, num_blocks,
+          seg_begin.p, row_seg.p, cta_row.p, cta_seg.p, num_ctas, seg_per_cta, uniform_len,
+          tile_threads};
 }
 
 Problem::~Problem() {
@@ -464,6 +478,64 @@ void validate_options(const anu_pdhg_options& o) {
     throw Error(ANU_ERR_INVALID, "unknown precision");
   if (o.ruiz_iterations < 0) throw Error(ANU_ERR_INVALID, "ruiz_iterations < 0");
   if (o.termination < 0 || o.termination > 2) throw Error(ANU_ERR_INVALID, "unknown termination");
+  if (o.tile_threads != 0 && o.tile_threads != kTileThreads[0] && o.tile_threads != kTileThreads[1])
+    throw Error(ANU_ERR_INVALID, "tile_threads must be 0 (tuned), 128 or 256");
+}
+
+// ------------------------------------------------------ product tiles
+
+// The single-LP product tile of each matrix of `p`: options.tile_threads
+// when set. Otherwise, for a single LP of at least kTuneNnz nonzeros (`trial`
+// is its case), short solves of that LP run for each pair of tiles (one for
+// K~, one for K~') and the pair with the least device time per iteration
+// stays if it beats the default pair by kTuneMargin; smaller LPs keep
+// kRowThreads, where the trials would cost more than they save. Every tile sums every row in the same order (a row longer than
+// kLongRow always takes a CTA of its own and a fixed-width sum), so the
+// choice changes timing only, never a result; the trial results are
+// discarded. Returns whether trial solves ran.
+bool choose_tiles(Problem& p, const anu_pdhg_options& o, const CaseData* trial) {
+  const int32_t fixed = o.tile_threads != 0 ? o.tile_threads : kRowThreads;
+  p.dk.set_tile(fixed);
+  p.dkt.set_tile(fixed);
+  if (o.tile_threads != 0 || trial == nullptr || !o.use_graphs || o.persistent_chunks ||
+      p.k.nnz() < kTuneNnz)
+    return false;
+  anu_pdhg_options t = o;
+  t.max_iterations = kTuneChunks * o.termination_check_frequency;
+  t.tolerance = 0.0;  // runs the whole budget
+  t.profile = 1;
+  t.verbose = 0;
+  t.polish_feasibility = 0;
+  t.polish_on_exit = 0;
+  const int64_t launches = p.launches;
+  const std::vector<const std::vector<double>*> none(1, nullptr);
+  auto per_iteration = [&](int32_t dk_threads, int32_t dkt_threads) {
+    p.dk.set_tile(dk_threads);
+    p.dkt.set_tile(dkt_threads);
+    std::vector<CaseResult> res;
+    run_cases(p, {trial}, t, none, none, &res, now_seconds());
+    const anu_pdhg_result& r = res[0].r;
+    return r.device_iterations > 0 ? r.device_iteration_seconds / r.device_iterations : INFINITY;
+  };
+  per_iteration(kRowThreads, kRowThreads);  // untimed: first touch of the pool and caches
+  // Each pair twice, the second round in reverse order, keeping its faster
+  // time: one trial varies by a percent or two, drift cancels.
+  constexpr int kPairs = 4;
+  double sec[kPairs];
+  for (int rep = 0; rep < 2; ++rep)
+    for (int k = 0; k < kPairs; ++k) {
+      const int i = rep == 0 ? k : kPairs - 1 - k;
+      const double t_i = per_iteration(kTileThreads[i / 2], kTileThreads[i % 2]);
+      sec[i] = rep == 0 ? t_i : std::min(sec[i], t_i);
+    }
+  // Pair 0 is the default; another pair must beat it by kTuneMargin.
+  int best = 0;
+  for (int i = 1; i < kPairs; ++i)
+    if (sec[i] < sec[best] && sec[i] < (1.0 - kTuneMargin) * sec[0]) best = i;
+  p.dk.set_tile(kTileThreads[best / 2]);
+  p.dkt.set_tile(kTileThreads[best % 2]);
+  p.launches = launches;  // the trial launches belong to no solve
+  return true;
 }
 
 // ------------------------------------------------ locality relabelling
@@ -635,6 +707,8 @@ std::unique_ptr<Problem> clone_problem(const Problem& src) {
   p->seg_per_cta = src.seg_per_cta;
   p->dk.upload(p->k, fp32, p->stream, p->seg_nnz, p->seg_per_cta);
   p->dkt.upload(p->kt, fp32, p->stream, p->seg_nnz, p->seg_per_cta);
+  p->dk.set_tile(src.dk.tile_threads);
+  p->dkt.set_tile(src.dkt.tile_threads);
   p->row_scale.alloc(std::max(p->m, 1));
   p->col_scale.alloc(std::max(p->n, 1));
   if (p->m > 0)
@@ -1481,10 +1555,27 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
     for (cudaEvent_t* e : {&fk.fork, &fk.xcomb, &fk.ycomb, &fk.join})
       ANU_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
   }
+  // With profiling, a chunk is timed from just before its launch (after any
+  // graph capture, which is host work) to its end.
+  cudaEvent_t ev_begin = nullptr, ev_end = nullptr;
+  double device_iter_s = 0.0;
+  int64_t device_iters = 0;
+  if (o.profile) {
+    ANU_CUDA(cudaEventCreate(&ev_begin));
+    ANU_CUDA(cudaEventCreate(&ev_end));
+  }
+  struct EventGuard {
+    cudaEvent_t a, b;
+    ~EventGuard() {
+      if (a) cudaEventDestroy(a);
+      if (b) cudaEventDestroy(b);
+    }
+  } event_guard{ev_begin, ev_end};
   auto run_chunk_body = [&](int len, bool check_at_end) {
     const uint32_t base_flags = averaging ? kAccumulate : 0u;
     if (persistent) {
       if (!coop_lock.owns_lock()) coop_lock.lock();
+      if (o.profile) ANU_CUDA(cudaEventRecord(ev_begin, st));
       PrimalEpi<T> pe{K, 0, 0u, w.params.p, w.w_table.p, w.x.p, w.x.p, w.c.p, w.lo.p, w.hi.p,
                       w.x_bar.p, w.anchor_x.p, w.dx.p, w.sum_x.p};
       DualEpi<T> de{K, 0, 0u, p.num_eq, w.params.p, w.w_table.p, w.y.p, w.y.p, w.q.p, w.kx.p,
@@ -1513,27 +1604,15 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
         p.launches = before;  // counted when launched
         found = w.graphs.emplace(key, exec).first;
       }
+      if (o.profile) ANU_CUDA(cudaEventRecord(ev_begin, st));
       ANU_CUDA(cudaGraphLaunch(found->second, st));
       p.launches += 2 * len;
     } else {
+      if (o.profile) ANU_CUDA(cudaEventRecord(ev_begin, st));
       for (int it = 0; it < len; ++it)
         launch_iteration(it, base_flags | ((check_at_end && it == len - 1) ? kWriteDelta : 0u));
     }
   };
-  cudaEvent_t ev_begin = nullptr, ev_end = nullptr;
-  double device_iter_s = 0.0;
-  int64_t device_iters = 0;
-  if (o.profile) {
-    ANU_CUDA(cudaEventCreate(&ev_begin));
-    ANU_CUDA(cudaEventCreate(&ev_end));
-  }
-  struct EventGuard {
-    cudaEvent_t a, b;
-    ~EventGuard() {
-      if (a) cudaEventDestroy(a);
-      if (b) cudaEventDestroy(b);
-    }
-  } event_guard{ev_begin, ev_end};
   // With profiling, the chunk's events are read once the stream has passed
   // them (at the next read-back), so timing adds no wait of its own.
   int pending_timed = 0;
@@ -1554,7 +1633,6 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
   };
   auto run_chunk = [&](int len, bool check_at_end) {
     collect_chunk_time();
-    if (o.profile) ANU_CUDA(cudaEventRecord(ev_begin, st));
     run_chunk_body(len, check_at_end);
     if (o.profile) {
       ANU_CUDA(cudaEventRecord(ev_end, st));
@@ -2675,6 +2753,8 @@ void fill_result(const anu::Problem& p, const anu::CaseResult& cr, double scalin
   out->col_spread_before = p.scaling.col_spread_before;
   out->col_spread_after = p.scaling.col_spread_after;
   out->matrix_norm_estimate = p.matrix_norm;
+  out->row_product_threads = p.dk.tile_threads;
+  out->column_product_threads = p.dkt.tile_threads;
 }
 
 }  // namespace
@@ -2688,6 +2768,7 @@ struct anu_pdhg {
   anu_pdhg_options options;
   double scaling_seconds = 0.0;
   double norm_seconds = 0.0;
+  double trial_seconds = 0.0;  // the product tiles' trial solves
 };
 
 struct anu_pdhg_batch {
@@ -2759,6 +2840,7 @@ void anu_pdhg_default_options(anu_pdhg_options* o) {
   o->persistent_chunks = 0;
   o->locality_order = 0;
   o->scaling_on_device = 1;
+  o->tile_threads = 0;
 }
 
 int anu_last_error(char* buf, int32_t size) { return anu::copy_last_error(buf, size); }
@@ -2800,6 +2882,9 @@ int anu_pdhg_create(const anu_lp* lp, const anu_pdhg_options* options, anu_pdhg*
       h->data = anu::make_case(*h->problem, c.data(), q.data(), lo.data(), up.data(),
                                lp->objective_scale, lp->objective_offset);
     }
+    const double trial_start = anu::now_seconds();
+    if (anu::choose_tiles(*h->problem, *options, &h->data))
+      h->trial_seconds = anu::now_seconds() - trial_start;
     *handle = h.release();
   });
 }
@@ -2826,6 +2911,7 @@ int anu_pdhg_run(anu_pdhg* h, const double* warm_x, const double* warm_y, double
     std::vector<anu::CaseResult> res;
     anu::run_cases(*h->problem, {&h->data}, h->options, vwx, vwy, &res, start);
     fill_result(*h->problem, res[0], h->scaling_seconds, h->norm_seconds, result);
+    result->tile_trial_seconds = h->trial_seconds;
     if (r.empty()) {
       if (x) std::copy(res[0].x.begin(), res[0].x.end(), x);
       if (y) std::copy(res[0].y.begin(), res[0].y.end(), y);
@@ -2958,6 +3044,7 @@ int anu_pdhg_batch_create(const anu_lp* base, int32_t num_cases, const double* c
     auto h = std::make_unique<anu_pdhg_batch>();
     h->options = *options;
     h->problem = anu::make_problem(*base, *options, &h->scaling_seconds, &h->norm_seconds);
+    anu::choose_tiles(*h->problem, *options, nullptr);
     // A stack that runs persistent chunks is one stack: its chunk kernel
     // fills the device on its own, and two of them may not overlap.
     if (options->split_stacks && num_cases >= anu::kSplitStack &&

@@ -155,16 +155,24 @@ struct DevCsr {
   DevBuf<int32_t> start, index;
   DevBuf<double> v64;
   DevBuf<float> v32;
-  DevBuf<RowBlockDev> blocks;
+  // The single-LP product's row-block schedule for each tile size of
+  // kTileThreads, both built at upload. tile_threads selects one; blocks and
+  // num_blocks are the selected schedule.
+  DevBuf<RowBlockDev> tile_blocks[2];
+  int32_t tile_num_blocks[2] = {0, 0};
+  const RowBlockDev* blocks = nullptr;
   int32_t num_blocks = 0;
   DevBuf<int32_t> seg_begin, row_seg, cta_row, cta_seg;
   int32_t num_ctas = 0;
   int32_t seg_per_cta = kSegPerCta;
   int32_t uniform_len = 0;  // kEllWidth when every row has that many nonzeros
+  int32_t tile_threads = kRowThreads;  // CTA size of the single-LP product
   // seg_nnz, seg_per_cta: the segment schedule's shape (at most
   // kSegPerCtaMax segments per CTA).
   void upload(const HostCsr& a, bool with_fp32, cudaStream_t s, int32_t seg_nnz = kSegNnz,
               int32_t seg_per_cta = kSegPerCta);
+  // Selects the single-LP product tile of `threads` (one of kTileThreads).
+  void set_tile(int32_t threads);
   template <class V>
   CsrView<V> view() const;
 };
@@ -288,6 +296,15 @@ void run_cases_streaming(Problem& problem, int slots, const anu_pdhg_options& op
                          const std::function<void(int32_t, CaseResult&)>& deliver,
                          const std::function<void(const CaseData*)>& release,
                          double start_time);
+
+// Picks each matrix's single-LP product tile: options.tile_threads, or, when
+// it is 0 and `trial` (the LP's case) is given for a large enough LP, the
+// pair that runs short trial solves of it fastest. Results do not depend on
+// the choice. Returns whether trial solves ran.
+constexpr int64_t kTuneNnz = int64_t(1) << 20;
+constexpr int kTuneChunks = 4;
+constexpr double kTuneMargin = 0.01;
+bool choose_tiles(Problem& p, const anu_pdhg_options& o, const CaseData* trial);
 
 // ||K~|| by power iteration on the device, FP64 (pdhg.cpp:223-282).
 double device_matrix_norm(Problem& p, int iterations, double tolerance);

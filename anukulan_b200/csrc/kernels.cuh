@@ -118,6 +118,9 @@ struct CsrView {
   // kEllWidth when every row holds exactly that many nonzeros (start[r] =
   // kEllWidth * r), so ell_kernel can take the product; 0 otherwise.
   int32_t uniform_len;
+  // CTA size of the single-LP product (one of kTileThreads); `blocks` is
+  // the row-block schedule for it.
+  int32_t tile_threads;
 };
 
 // ------------------------------------------------------- per-case state
@@ -355,18 +358,37 @@ __device__ __forceinline__ Acc block_sum(Acc v, Acc* scratch) {
 // in 32 distinct banks. Only the addresses change, not the order of a sum.
 constexpr int kSerialRow = 32;
 constexpr int kPerThread = kBlockNnz / kRowThreads;
-constexpr int kProdSlots = kBlockNnz + kBlockNnz / 32;
+// A row longer than kLongRow takes a CTA to itself and is summed over
+// kLongWidth virtual lanes (lane v adds nonzeros v, v + kLongWidth, ... in
+// order), then by a fixed tree over those lanes. Both are constants, not the
+// CTA size, so every tile size (kTileThreads) sums every row the same way.
+constexpr int kLongRow = kBlockNnz;
+constexpr int kLongWidth = kRowThreads;
 __device__ __forceinline__ int prod_slot(int k) { return k + (k >> 5); }
 static_assert(kBlockRows <= kRowThreads, "one epilogue row per thread");
 static_assert(kBlockNnz >= kRowThreads, "block_sum scratch");
 
-template <class V, class X, class Acc, class Epi>
-__global__ void __launch_bounds__(kRowThreads)
+// The CTA sizes the single-LP kernels are built for. A tile of T threads
+// holds up to T * kPerThread nonzeros in at most T rows (rows_kernel), or T
+// rows (ell_kernel). The tuner picks one per matrix at set-up.
+constexpr int kTileThreads[] = {128, 256};
+
+template <int kThreads>
+struct RowTile {
+  static_assert(kThreads >= kLongWidth, "the long-row sum needs kLongWidth threads");
+  static constexpr int kNnz = kThreads * kPerThread;
+  static constexpr int kRows = kThreads;
+  static constexpr int kSlots = kNnz + kNnz / 32;
+};
+
+template <class V, class X, class Acc, class Epi, int kThreads = kRowThreads>
+__global__ void __launch_bounds__(kThreads)
     rows_kernel(CsrView<V> a, const X* __restrict__ x, Epi epi) {
-  constexpr int kWarps = kRowThreads / 32;
-  __shared__ Acc prod[kProdSlots];
-  __shared__ Acc rowsum[kBlockRows];
-  __shared__ int32_t long_rows[kBlockRows];
+  using Tile = RowTile<kThreads>;
+  constexpr int kWarps = kThreads / 32;
+  __shared__ Acc prod[Tile::kSlots];
+  __shared__ Acc rowsum[Tile::kRows];
+  __shared__ int32_t long_rows[Tile::kRows];
   __shared__ int32_t warp_long[kWarps];
   const RowBlockDev blk = a.blocks[blockIdx.x];
   const int32_t r0 = blk.row_begin;
@@ -374,34 +396,41 @@ __global__ void __launch_bounds__(kRowThreads)
   const int32_t nz0 = blk.nz_begin;
   const int32_t nnz = blk.nz_end - nz0;
   const int t = threadIdx.x;
-  if (nnz > kBlockNnz) {
-    // One long row: strided partial sums (k = t, t + kRowThreads, ...), then
-    // a fixed-order tree over the CTA.
+  if (nrows == 1 && nnz > kLongRow) {
+    // One long row: strided partial sums over kLongWidth virtual lanes, then
+    // a fixed-order tree over them.
     typename Epi::Pre pre{};
     if (t == 0) pre = epi.prefetch(r0, 0);
     pdl_wait();
     pdl_launch();
     Acc s = 0;
     const int32_t end = nz0 + nnz;
-    for (int32_t base = nz0; base < end; base += kRowThreads * kPerThread) {
-      int32_t col[kPerThread];
-      Acc val[kPerThread];
+    if (t < kLongWidth) {
+      for (int32_t base = nz0; base < end; base += kLongWidth * kPerThread) {
+        int32_t col[kPerThread];
+        Acc val[kPerThread];
 #pragma unroll
-      for (int q = 0; q < kPerThread; ++q) {
-        const int32_t k = base + q * kRowThreads + t;
-        col[q] = k < end ? a.index[k] : -1;
-        val[q] = k < end ? static_cast<Acc>(a.value[k]) : static_cast<Acc>(0);
+        for (int q = 0; q < kPerThread; ++q) {
+          const int32_t k = base + q * kLongWidth + t;
+          col[q] = k < end ? a.index[k] : -1;
+          val[q] = k < end ? static_cast<Acc>(a.value[k]) : static_cast<Acc>(0);
+        }
+        Acc xv[kPerThread];
+#pragma unroll
+        for (int q = 0; q < kPerThread; ++q)
+          xv[q] = col[q] >= 0 ? static_cast<Acc>(x[col[q]]) : static_cast<Acc>(0);
+#pragma unroll
+        for (int q = 0; q < kPerThread; ++q)
+          if (col[q] >= 0) s = madd(s, val[q], xv[q]);
       }
-      Acc xv[kPerThread];
-#pragma unroll
-      for (int q = 0; q < kPerThread; ++q)
-        xv[q] = col[q] >= 0 ? static_cast<Acc>(x[col[q]]) : static_cast<Acc>(0);
-#pragma unroll
-      for (int q = 0; q < kPerThread; ++q)
-        if (col[q] >= 0) s = madd(s, val[q], xv[q]);
+      prod[t] = s;
     }
-    s = block_sum<kRowThreads>(s, prod);
-    if (t == 0) epi.finish(r0, 0, s, pre);
+    __syncthreads();
+    for (int w = kLongWidth / 2; w > 0; w >>= 1) {
+      if (t < w) prod[t] = add(prod[t], prod[t + w]);
+      __syncthreads();
+    }
+    if (t == 0) epi.finish(r0, 0, prod[0], pre);
     return;
   }
   // ---- independent of the previous launch
@@ -409,7 +438,7 @@ __global__ void __launch_bounds__(kRowThreads)
   V val[kPerThread];
 #pragma unroll
   for (int q = 0; q < kPerThread; ++q) {
-    const int32_t k = q * kRowThreads + t;
+    const int32_t k = q * kThreads + t;
     col[q] = k < nnz ? a.index[nz0 + k] : -1;
     val[q] = k < nnz ? a.value[nz0 + k] : static_cast<V>(0);
   }
@@ -430,7 +459,7 @@ __global__ void __launch_bounds__(kRowThreads)
     xv[q] = col[q] >= 0 ? static_cast<Acc>(x[col[q]]) : static_cast<Acc>(0);
 #pragma unroll
   for (int q = 0; q < kPerThread; ++q)
-    if (col[q] >= 0) prod[prod_slot(q * kRowThreads + t)] = mul(static_cast<Acc>(val[q]), xv[q]);
+    if (col[q] >= 0) prod[prod_slot(q * kThreads + t)] = mul(static_cast<Acc>(val[q]), xv[q]);
   __syncthreads();
   const bool is_long = has_row && re - rb > kSerialRow;
   if (has_row && !is_long) {
@@ -520,10 +549,10 @@ __device__ __forceinline__ void load_ell_row(const int32_t* __restrict__ index,
   }
 }
 
-template <class V, class X, class Acc, class Epi>
-__global__ void __launch_bounds__(kRowThreads)
+template <class V, class X, class Acc, class Epi, int kThreads = kRowThreads>
+__global__ void __launch_bounds__(kThreads)
     ell_kernel(CsrView<V> a, const X* __restrict__ x, Epi epi) {
-  const int32_t r = static_cast<int32_t>(blockIdx.x) * kRowThreads + static_cast<int32_t>(threadIdx.x);
+  const int32_t r = static_cast<int32_t>(blockIdx.x) * kThreads + static_cast<int32_t>(threadIdx.x);
   const bool has_row = r < a.rows;
   int32_t col[kEllWidth];
   V val[kEllWidth];

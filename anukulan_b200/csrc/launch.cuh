@@ -63,7 +63,7 @@ void prefer_register_bound_carveout(F kernel, int threads) {
 
 // Applied at the first launch of each instantiation that is not being
 // captured into a graph (no attribute calls inside a capture).
-template <class V, class X, class Acc, class Epi>
+template <class V, class X, class Acc, class Epi, int kThreads = kRowThreads>
 void rows_kernel_setup(cudaStream_t s) {
   static std::atomic<bool> done{false};
   if (done.load(std::memory_order_acquire)) return;
@@ -73,17 +73,47 @@ void rows_kernel_setup(cudaStream_t s) {
     return;
   }
   if (status != cudaStreamCaptureStatusNone) return;
-  prefer_register_bound_carveout(rows_kernel<V, X, Acc, Epi>, kRowThreads);
+  prefer_register_bound_carveout(rows_kernel<V, X, Acc, Epi, kThreads>, kThreads);
   done.store(true, std::memory_order_release);
 }
 
-// The carveout hint for the single-LP iteration kernels of precision T. Their
-// first launches are usually inside a graph capture, where rows_kernel_setup
-// leaves them alone, so the problem set-up applies it beforehand.
+// The carveout hint for the single-LP iteration kernels of precision T, at
+// every tile size. Their first launches are usually inside a graph capture,
+// where rows_kernel_setup leaves them alone, so the problem set-up applies
+// it beforehand.
 template <class T>
 void prepare_iteration_kernels(cudaStream_t s) {
-  rows_kernel_setup<T, T, T, PrimalEpi<T>>(s);
-  rows_kernel_setup<T, T, T, DualEpi<T>>(s);
+  rows_kernel_setup<T, T, T, PrimalEpi<T>, kTileThreads[0]>(s);
+  rows_kernel_setup<T, T, T, DualEpi<T>, kTileThreads[0]>(s);
+  rows_kernel_setup<T, T, T, PrimalEpi<T>, kTileThreads[1]>(s);
+  rows_kernel_setup<T, T, T, DualEpi<T>, kTileThreads[1]>(s);
+}
+
+// One single-LP product launch at tile size kThreads: ell_kernel for a
+// matrix of uniform 8-nonzero rows, rows_kernel on the row-block schedule
+// otherwise.
+template <int kThreads, class V, class X, class Acc, class Epi, class Mat>
+void single_product(cudaStream_t s, const Mat& a, const X* x, const Epi& epi, bool pdl) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.blockDim = dim3(kThreads);
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl ? 1 : 0;
+  if (a.uniform_len == kEllWidth) {
+    cfg.gridDim = dim3((a.rows + kThreads - 1) / kThreads);
+    cuda_check(cudaLaunchKernelEx(&cfg, ell_kernel<V, X, Acc, Epi, kThreads>,
+                                  a.template view<V>(), x, epi),
+               "ell_kernel launch");
+  } else {
+    rows_kernel_setup<V, X, Acc, Epi, kThreads>(s);
+    cfg.gridDim = dim3(a.num_blocks);
+    cuda_check(cudaLaunchKernelEx(&cfg, rows_kernel<V, X, Acc, Epi, kThreads>,
+                                  a.template view<V>(), x, epi),
+               "rows_kernel launch");
+  }
 }
 
 // y = A x (any epilogue) for K cases.
@@ -91,31 +121,11 @@ template <class V, class X, class Acc, class Epi, class Mat>
 void product(Exec& p, const Mat& a, const X* x, int K, const Epi& epi, bool pdl = false) {
   if (a.rows == 0) return;
   cudaStream_t s = p.stream;
-  if (K == 1 && a.uniform_len == kEllWidth) {
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3((a.rows + kRowThreads - 1) / kRowThreads);
-    cfg.blockDim = dim3(kRowThreads);
-    cfg.stream = s;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = pdl ? 1 : 0;
-    cuda_check(cudaLaunchKernelEx(&cfg, ell_kernel<V, X, Acc, Epi>, a.template view<V>(), x, epi),
-               "ell_kernel launch");
-  } else if (K == 1) {
-    rows_kernel_setup<V, X, Acc, Epi>(s);
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(a.num_blocks);
-    cfg.blockDim = dim3(kRowThreads);
-    cfg.stream = s;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = pdl ? 1 : 0;
-    cuda_check(cudaLaunchKernelEx(&cfg, rows_kernel<V, X, Acc, Epi>, a.template view<V>(), x, epi),
-               "rows_kernel launch");
+  if (K == 1) {
+    if (a.tile_threads == kTileThreads[1])
+      single_product<kTileThreads[1], V, X, Acc>(s, a, x, epi, pdl);
+    else
+      single_product<kTileThreads[0], V, X, Acc>(s, a, x, epi, pdl);
   } else {
 #define ANU_CASES(L_, CPL_)                                                              \
   do {                                                                                   \

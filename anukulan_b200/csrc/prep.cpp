@@ -158,12 +158,13 @@ void scale_vectors(const ScalingSweeps& sw, int32_t m, int32_t n, double* c, dou
   }
 }
 
-std::vector<RowBlock> row_blocks(const HostCsr& a, int32_t block_nnz, int32_t block_rows) {
+std::vector<RowBlock> row_blocks(const HostCsr& a, int32_t block_nnz, int32_t block_rows,
+                                 int32_t long_row) {
   std::vector<RowBlock> blocks;
   int32_t r = 0;
   while (r < a.rows) {
     const int32_t len = a.start[r + 1] - a.start[r];
-    if (len > block_nnz) {
+    if (len > long_row || len > block_nnz) {
       blocks.push_back({r, r + 1});
       ++r;
       continue;
@@ -172,7 +173,7 @@ std::vector<RowBlock> row_blocks(const HostCsr& a, int32_t block_nnz, int32_t bl
     int32_t nnz = 0;
     while (r < a.rows && r - r0 < block_rows) {
       const int32_t l = a.start[r + 1] - a.start[r];
-      if (l > block_nnz || nnz + l > block_nnz) break;
+      if (l > long_row || l > block_nnz || nnz + l > block_nnz) break;
       nnz += l;
       ++r;
     }
@@ -183,7 +184,8 @@ std::vector<RowBlock> row_blocks(const HostCsr& a, int32_t block_nnz, int32_t bl
   std::stable_sort(blocks.begin(), blocks.end(), [&](const RowBlock& x, const RowBlock& y) {
     const int32_t nx = a.start[x.row_end] - a.start[x.row_begin];
     const int32_t ny = a.start[y.row_end] - a.start[y.row_begin];
-    const bool lx = nx > block_nnz, ly = ny > block_nnz;
+    const bool lx = nx > block_nnz || (x.row_end - x.row_begin == 1 && nx > long_row);
+    const bool ly = ny > block_nnz || (y.row_end - y.row_begin == 1 && ny > long_row);
     if (lx != ly) return lx;
     if (lx) return nx > ny;
     return false;

@@ -72,7 +72,9 @@ struct RowBlock {
   int32_t row_begin;
   int32_t row_end;
 };
-std::vector<RowBlock> row_blocks(const HostCsr& a, int32_t block_nnz, int32_t block_rows);
+// Rows longer than long_row (or than block_nnz) get a block each.
+std::vector<RowBlock> row_blocks(const HostCsr& a, int32_t block_nnz, int32_t block_rows,
+                                 int32_t long_row);
 
 // Segment schedule of the case-stack product (see seg_kernel): every row
 // cut into segments of at most seg_nnz nonzeros (a longer row into

@@ -195,6 +195,8 @@ def spmv_leg(iterations, device, peak, only=None):
         b = algorithmic_bytes_per_iteration(nnz, m, n, 1, size, size)
         out[name] = {"setup_ms": {k: round(r.phases[k] * 1e3, 2)
                                   for k in ("scaling", "matrix_norm")},
+                     "tile_trial_ms": round(r.tile_trial_seconds * 1e3, 2),
+                     "product_threads": [r.row_product_threads, r.column_product_threads],
                      "us_per_iteration": per_it * 1e6, "iterations_per_second": 1.0 / per_it,
                      "algorithmic_bytes_per_iteration": b,
                      "achieved_GBps": b / per_it / 1e9, "frac": b / per_it / 1e9 / peak,
@@ -435,6 +437,8 @@ def powerlaw_leg(local_rank, tolerance, precisions, locality, time_limit, peak,
                      "objective_error": abs(r.objective - objective) / abs(objective),
                      "setup_ms": {k: round(r.phases[k] * 1e3, 2)
                                   for k in ("scaling", "matrix_norm")},
+                     "tile_trial_ms": round(r.tile_trial_seconds * 1e3, 2),
+                     "product_threads": [r.row_product_threads, r.column_product_threads],
                      "us_per_iteration_device": us,
                      "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak,
                                   "unit": "GB/s", "frac": achieved / peak if achieved else None,

@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define ANU_PDHG_ABI_VERSION 2
+#define ANU_PDHG_ABI_VERSION 3
 
 /* Return codes. */
 enum {
@@ -193,6 +193,15 @@ typedef struct anu_pdhg_options {
    * scaled matrix and every factor are bit-identical to the host sweeps.
    * 0 = on the host. */
   int32_t scaling_on_device;
+  /* CTA size of the single-LP product kernels (K~ x and K~' y): 128 or 256
+   * fixes it for both. 0 (default): anu_pdhg_create / anu_pdhg_solve on an
+   * LP of at least 2^20 nonzeros runs short trial solves of the LP (4
+   * checks each, results discarded), two for each of the four pairs, and
+   * keeps the pair with the least device time per iteration when it beats
+   * 128/128 by 1%; smaller LPs, case stacks and packed batches take 128. Every
+   * tile size sums every row in the same order, so the choice changes timing
+   * only, never a result. The result reports the pair and the trial time. */
+  int32_t tile_threads;
 } anu_pdhg_options;
 
 /* PdhgResidual, src/anukulan/pdhg.hpp:429-496. */
@@ -252,6 +261,11 @@ typedef struct anu_pdhg_result {
    * full-width chunks only. */
   double device_iteration_seconds;
   int64_t device_iterations;
+  /* CTA size of the single-LP products K~ x (row) and K~' y (column):
+   * options.tile_threads, or the pair the handle's trial solves chose. */
+  int32_t row_product_threads;
+  int32_t column_product_threads;
+  double tile_trial_seconds; /* host time of those trial solves; 0 when none ran */
   char message[160];
 } anu_pdhg_result;
 
