@@ -13,7 +13,9 @@
 // W is chosen by a short autotuning pass at creation unless the caller
 // fixes it. Each candidate W runs W LPs, drawn evenly from the size order,
 // for a fixed number of iterations at once; the W with the most nonzero x
-// iterations per second of wall time wins.
+// iterations per second of wall time wins. The single-LP product tile (128
+// or 256 threads per CTA) is then chosen the same way at that W, unless
+// options.tile_threads fixes it; the tile changes no result.
 #include <algorithm>
 #include <atomic>
 #include <mutex>
@@ -80,10 +82,12 @@ int host_threads() {
   return h == 0 ? 4 : static_cast<int>(h);
 }
 
-// Candidate worker counts, each run briefly on an even sample of the batch.
-int32_t tune_workers(anu_pdhg_packed& h) {
+// Nonzero x iterations per second of `w` workers solving an even sample of
+// w LPs of the batch for a few check periods each (a second pass, timed,
+// after one that fills the sample LPs' memory pools: it measures how w
+// solves share the device, not how w first-time allocations contend).
+double sample_rate(anu_pdhg_packed& h, int w) {
   const int n = static_cast<int>(h.problems.size());
-  const int cap = std::min(n, 2 * host_threads());
   anu_pdhg_options o = h.options;
   o.max_iterations = 4 * o.termination_check_frequency;
   o.polish_feasibility = 0;
@@ -91,33 +95,59 @@ int32_t tune_workers(anu_pdhg_packed& h) {
   o.profile = 0;
   o.tolerance = 1e-300;  // run the whole budget
   o.gap_tolerance = 1e-300;
+  std::vector<int32_t> sample;
+  for (int i = 0; i < w; ++i) sample.push_back(h.order[static_cast<size_t>(i) * n / w]);
+  double work = 0.0;
+  for (int32_t idx : sample)
+    work += static_cast<double>(h.problems[idx]->k.nnz()) * o.max_iterations;
+  auto pass = [&]() {
+    run_queue(sample, w, [&](int32_t idx) {
+      std::vector<CaseResult> r;
+      run_cases(*h.problems[idx], {&h.data[idx]}, o, {nullptr}, {nullptr}, &r, now_seconds());
+    });
+  };
+  pass();
+  const double t0 = now_seconds();
+  pass();
+  return work / std::max(now_seconds() - t0, 1e-9);
+}
+
+// Candidate worker counts, each run briefly on an even sample of the batch.
+int32_t tune_workers(anu_pdhg_packed& h) {
+  const int n = static_cast<int>(h.problems.size());
+  const int cap = std::min(n, 2 * host_threads());
   int32_t best = 1;
   double best_rate = -1.0;
   for (const int w : {1, 2, 4, 8, 12, 16, 24, 32, 48}) {
     if (w > cap) break;
-    std::vector<int32_t> sample;
-    for (int i = 0; i < w; ++i) sample.push_back(h.order[static_cast<size_t>(i) * n / w]);
-    double work = 0.0;
-    for (int32_t idx : sample)
-      work += static_cast<double>(h.problems[idx]->k.nnz()) * o.max_iterations;
-    auto pass = [&]() {
-      run_queue(sample, w, [&](int32_t idx) {
-        std::vector<CaseResult> r;
-        run_cases(*h.problems[idx], {&h.data[idx]}, o, {nullptr}, {nullptr}, &r, now_seconds());
-      });
-    };
-    // A first pass fills the sample LPs' memory pools; the timed second pass
-    // then measures how W solves share the device, not how W first-time
-    // allocations (device and pinned host blocks) contend.
-    pass();
-    const double t0 = now_seconds();
-    pass();
-    const double rate = work / std::max(now_seconds() - t0, 1e-9);
+    const double rate = sample_rate(h, w);
     if (rate > best_rate) {
       best_rate = rate;
       best = w;
     }
   }
+  return best;
+}
+
+void set_tiles(anu_pdhg_packed& h, int32_t threads) {
+  for (auto& p : h.problems) {
+    p->dk.set_tile(threads);
+    p->dkt.set_tile(threads);
+  }
+}
+
+// The product tile of every LP of the batch at `w` workers: each tile's
+// sample rate twice, alternating, keeping the better; 256 threads must beat
+// 128 by kTuneMargin.
+int32_t tune_tile(anu_pdhg_packed& h, int w) {
+  double rate[2] = {0.0, 0.0};
+  for (int rep = 0; rep < 2; ++rep)
+    for (int i = 0; i < 2; ++i) {
+      set_tiles(h, kTileThreads[i]);
+      rate[i] = std::max(rate[i], sample_rate(h, w));
+    }
+  const int32_t best = rate[1] * (1.0 - kTuneMargin) > rate[0] ? kTileThreads[1] : kTileThreads[0];
+  set_tiles(h, best);
   return best;
 }
 
@@ -131,6 +161,8 @@ void fill_packed_result(const Problem& p, const CaseResult& cr, double scaling_s
   out->col_spread_before = p.scaling.col_spread_before;
   out->col_spread_after = p.scaling.col_spread_after;
   out->matrix_norm_estimate = p.matrix_norm;
+  out->row_product_threads = p.dk.tile_threads;
+  out->column_product_threads = p.dkt.tile_threads;
 }
 
 template <class F>
@@ -192,6 +224,7 @@ int anu_pdhg_packed_create(int32_t num_lps, const anu_lp* lps, const anu_pdhg_op
       return h->problems[a]->k.nnz() > h->problems[b]->k.nnz();
     });
     h->workers = workers > 0 ? workers : anu::tune_workers(*h);
+    if (options->tile_threads == 0) anu::tune_tile(*h, h->workers);
     *handle = h.release();
   });
 }

@@ -243,6 +243,7 @@ def packed_leg(local_rank, steps, warmup, workers=0, cpu=True, cpu_sample=32):
         iters += sum(r.iterations for r in res)
     clk = clocks.stop()
     used = solver.workers
+    tile = int(res[0].row_product_threads) if steps else None
     solver.close()
     total = float(np.sum(step_ms))
     nnz = sum(lp.k.nnz for lp in lps)
@@ -253,7 +254,7 @@ def packed_leg(local_rank, steps, warmup, workers=0, cpu=True, cpu_sample=32):
                    "rows_total": int(sum(lp.num_rows for lp in lps)), "nnz_total": int(nnz),
                    "rows_range": [int(min(lp.num_rows for lp in lps)),
                                   int(max(lp.num_rows for lp in lps))],
-                   "tolerance": TOL, "workers": used},
+                   "tolerance": TOL, "workers": used, "product_threads": tile},
         "cases_optimal": solved, "cases_attempted": len(lps) * steps,
         "iterations_per_second": iters / (total / 1e3),
         "step_ms": [round(v, 1) for v in step_ms], "create_seconds": create_s, "clocks": clk,

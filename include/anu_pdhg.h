@@ -198,8 +198,9 @@ typedef struct anu_pdhg_options {
    * LP of at least 2^20 nonzeros runs short trial solves of the LP (4
    * checks each, results discarded), two for each of the four pairs, and
    * keeps the pair with the least device time per iteration when it beats
-   * 128/128 by 1%; smaller LPs, case stacks and packed batches take 128. Every
-   * tile size sums every row in the same order, so the choice changes timing
+   * 128/128 by 1%; smaller LPs and case stacks take 128; packed batches time
+   * both tiles on a sample of their LPs at their worker count. Every tile
+   * size sums every row in the same order, so the choice changes timing
    * only, never a result. The result reports the pair and the trial time. */
   int32_t tile_threads;
 } anu_pdhg_options;
@@ -509,7 +510,10 @@ int anu_pdhg_batch_stream(anu_pdhg_batch* handle, int32_t slots, anu_pdhg_case_s
  *
  * workers: 0 = choose W by a short autotuning run at creation (each
  * candidate W runs W LPs drawn evenly from the batch for a few check
- * periods; the most nonzero-iterations per second wins), else W itself. */
+ * periods; the most nonzero-iterations per second wins), else W itself.
+ * With options.tile_threads 0, the single-LP product tile of every LP (128
+ * or 256 threads per CTA) is then chosen the same way at that W; the tile
+ * changes timing only, never a result. Each result reports it. */
 typedef struct anu_pdhg_packed anu_pdhg_packed;
 int anu_pdhg_packed_create(int32_t num_lps, const anu_lp* lps,
                            const anu_pdhg_options* options, int32_t workers,

@@ -119,10 +119,15 @@ def test_small_lp_takes_default_tile(engine, powerlaw):
 def test_packed_tiles_bit_identical(engine):
     lps = [lp for lp, _ in lpgen.packed_batch(count=12, min_rows=300, max_rows=20_000, seed=78)]
     kw = dict(tolerance=1e-6, precision=PRECISION_FP32)
-    fixed = engine.solve_packed(lps, tile_threads=128, **kw)
+    fixed = {t: engine.solve_packed(lps, tile_threads=t, **kw) for t in (128, 256)}
     tuned = engine.solve_packed(lps, tile_threads=0, **kw)
-    for k, (a, b) in enumerate(zip(fixed, tuned)):
-        assert same(a, b), k
+    chosen = tuned[0].row_product_threads
+    assert chosen in (128, 256)
+    for t in (128, 256):
+        assert all(r.row_product_threads == r.column_product_threads == t for r in fixed[t])
+    for k, (a, b, c) in enumerate(zip(fixed[128], fixed[256], tuned)):
+        assert c.row_product_threads == chosen, k
+        assert same(a, b) and same(a, c), k
 
 
 def test_invalid_tile_rejected(engine, powerlaw):
