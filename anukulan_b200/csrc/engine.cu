@@ -1549,7 +1549,7 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
       if (side) cudaStreamDestroy(side);
     }
   } fk;
-  const bool fork_checks = refine && !sub_run && !slow && K > 1;
+  const bool fork_checks = refine && !sub_run && !slow && (K > 1 || !p.concurrent);
   if (fork_checks) {
     ANU_CUDA(cudaStreamCreateWithFlags(&fk.side, cudaStreamNonBlocking));
     for (cudaEvent_t* e : {&fk.fork, &fk.xcomb, &fk.ycomb, &fk.join})
@@ -1726,12 +1726,12 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
   // the same arguments at every check, so one graph launch replaces a dozen
   // kernel launches. The first call runs directly and sizes the reduction
   // scratch; a graph whose scratch has since been reallocated is captured
-  // again. Only for case stacks: not where the iterate buffers swap (the
-  // host-driven path), not in polishing sub-stacks, whose few checks would
-  // not repay the capture, and not for a single LP, which packed batches run
-  // by the hundred from many host threads at once.
+  // again. Not where the iterate buffers swap (the host-driven path), not in
+  // polishing sub-stacks, whose few checks would not repay the capture, and
+  // not for a single LP of a packed batch, where many host threads would
+  // capture and instantiate graphs at once.
   auto replay = [&](typename Workspace<T>::Replay& r, auto&& body) {
-    if (!o.use_graphs || slow || sub_run || K == 1) {
+    if (!o.use_graphs || slow || sub_run || (K == 1 && p.concurrent)) {
       body();
       return;
     }

@@ -213,6 +213,10 @@ struct Problem : Exec {
   // Original column of each column when the problem is relabelled (empty
   // otherwise); the power iteration's start vector follows it.
   std::vector<int32_t> col_old;
+  // One of many problems that host threads solve at once (a packed batch):
+  // its single-LP checks launch directly, on one stream, instead of as
+  // graphs with a second branch.
+  bool concurrent = false;
   ~Problem();
 };
 

@@ -218,7 +218,10 @@ int anu_pdhg_packed_create(int32_t num_lps, const anu_lp* lps, const anu_pdhg_op
       h->data[i] = anu::make_case(*h->problems[i], lps[i].c, lps[i].q, lps[i].lower,
                                   lps[i].upper, lps[i].objective_scale, lps[i].objective_offset);
     });
-    for (const auto& p : h->problems) anu::choose_tiles(*p, *options, nullptr);
+    for (const auto& p : h->problems) {
+      p->concurrent = true;
+      anu::choose_tiles(*p, *options, nullptr);
+    }
     h->order = all;
     std::stable_sort(h->order.begin(), h->order.end(), [&](int32_t a, int32_t b) {
       return h->problems[a]->k.nnz() > h->problems[b]->k.nnz();

@@ -611,7 +611,7 @@ def fp64_single_case(st, device):
     kept, each case swapped in by anu_pdhg_set_case (the reference's backends
     keep a prepared matrix per SparseMatrix::id() the same way)."""
     from anukulan_b200 import pdhg
-    from anukulan_b200.abi import OPTIMAL, PRECISION_FP64, make_options
+    from anukulan_b200.abi import OPTIMAL, PRECISION_FP32, PRECISION_FP64, make_options
     opts = make_options(precision=PRECISION_FP64, device=device, **STACK_OPTS)
     pdhg.solve_pdhg(st.case(0), opts)  # warm-up: context, module load
     t0 = time.perf_counter()
@@ -630,11 +630,26 @@ def fp64_single_case(st, device):
         ok_h += int(h.run().status == OPTIMAL)
     h.close()
     dt_h = time.perf_counter() - t1
+    # The same handle loop with FP32 iterates, FP64 checks and refinement:
+    # what a caller with one LP at a time (a crossover seed, a node) gets.
+    opts32 = make_options(precision=PRECISION_FP32, device=device, **STACK_OPTS)
+    t2 = time.perf_counter()
+    h = pdhg.PdhgHandle(st.base, opts32)
+    ok_32 = 0
+    for k in range(st.num_cases):
+        h.set_case(st.c[k], st.q[k], st.lower[k], st.upper[k])
+        ok_32 += int(h.run().status == OPTIMAL)
+    h.close()
+    dt_32 = time.perf_counter() - t2
     return {"value": ok_h / dt_h, "unit": "solves/s", "cases": st.num_cases, "optimal": ok_h,
             "seconds": dt_h, "iterations_per_second": iters / dt_h,
             "mode": "engine FP64, one case per run on one handle (matrix prepared once)",
             "fresh_solve_per_case": {"value": ok / dt, "unit": "solves/s", "seconds": dt,
-                                     "mode": "engine FP64, anu_pdhg_solve per case"}}
+                                     "mode": "engine FP64, anu_pdhg_solve per case"},
+            "fp32_handle": {"value": ok_32 / dt_32, "unit": "solves/s", "seconds": dt_32,
+                            "optimal": ok_32,
+                            "mode": "engine FP32 + FP64 checks and refinement, one case per "
+                                    "run on one handle"}}
 
 
 # -------------------------------------------------------------- our arm
