@@ -166,10 +166,11 @@ def flush_l2(torch, buf):
     buf.zero_()
 
 
-def spmv_leg(iterations, device, peak, only=None):
+def spmv_leg(iterations, device, peak, only=None, tile_threads=0):
     """Per-iteration time of the single-LP path on the power-law LP: two fused
     SpMV + step kernels per iteration, graph-captured, timed by the engine's
-    CUDA events around every iteration chunk (`profile`)."""
+    CUDA events around every iteration chunk (`profile`). tile_threads: the
+    products' CTA size (0: chosen by the engine's trial solves)."""
     from anukulan_b200 import lpgen, pdhg
     from anukulan_b200.abi import PRECISION_FP32, PRECISION_FP64, make_options
     lp, _ = lpgen.power_law_lp()
@@ -189,7 +190,7 @@ def spmv_leg(iterations, device, peak, only=None):
             continue
         opts = make_options(tolerance=1e-12, precision=prec, max_iterations=iterations,
                             profile=1, polish_feasibility=0, polish_on_exit=0, device=device,
-                            locality_order=relabel)
+                            locality_order=relabel, tile_threads=tile_threads)
         r = pdhg.solve_pdhg(lp, opts)
         per_it = r.device_iteration_seconds / max(r.device_iterations, 1)
         b = algorithmic_bytes_per_iteration(nnz, m, n, 1, size, size)
@@ -1001,6 +1002,8 @@ def main(argv=None):
     ap.add_argument("--spmv-legs", default="",
                     help="comma list of spmv legs to run with --workload spmv "
                          "(fp32, fp64, fp32_relabelled, fp64_relabelled; default all)")
+    ap.add_argument("--tile-threads", type=int, default=0,
+                    help="--workload spmv: options.tile_threads (0 = tuned, 128, 256)")
     ap.add_argument("--no-side", dest="side", action="store_false",
                     help="skip every side leg of the stack line")
     ap.add_argument("--side-legs", default=",".join(SIDE_LEGS),
@@ -1026,7 +1029,8 @@ def main(argv=None):
             torch.cuda.set_device(local_rank)
             peak, kind = hbm_peak()
             out = spmv_leg(args.spmv_iterations, local_rank, peak,
-                           args.spmv_legs.split(",") if args.spmv_legs else None)
+                           args.spmv_legs.split(",") if args.spmv_legs else None,
+                           args.tile_threads)
             out["peak_source"] = kind
     else:
         out = run_engine(args, rank, world, local_rank)
