@@ -60,6 +60,7 @@ class anu_pdhg_options(C.Structure):
         ("precision", i32), ("refinement", i32), ("device", i32), ("use_graphs", i32),
         ("profile", i32), ("split_stacks", i32), ("persistent_chunks", i32),
         ("locality_order", i32), ("scaling_on_device", i32), ("tile_threads", i32),
+        ("cluster_chunks", i32),
     ]
 
 
@@ -109,6 +110,7 @@ DEFAULTS = dict(
     verbose=0, log_frequency=5000, precision=0, refinement=1,
     device=0, use_graphs=1, profile=0, split_stacks=1,
     persistent_chunks=0, locality_order=0, scaling_on_device=1, tile_threads=0,
+    cluster_chunks=0,
 )
 
 

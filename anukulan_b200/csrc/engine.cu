@@ -102,6 +102,20 @@ void DevCsr::upload(const HostCsr& a, bool with_fp32, cudaStream_t s, int32_t se
                                cudaMemcpyHostToDevice, s));
   }
   set_tile(kRowThreads);
+  auto put_rows = [&](DevBuf<int32_t>& d, const std::vector<int32_t>& h) {
+    d.alloc(std::max<size_t>(h.size(), 1));
+    if (!h.empty())
+      ANU_CUDA(cudaMemcpyAsync(d.p, h.data(), sizeof(int32_t) * h.size(), cudaMemcpyHostToDevice, s));
+  };
+  for (int i = 0; i < 2; ++i) {
+    const ClusterSchedule c = cluster_schedule(a, i == 0 ? 16 : 8, kSerialRow);
+    put_rows(cl_bounds[i], c.bounds);
+    put_rows(cl_warp_start[i], c.warp_start);
+    put_rows(cl_warp_rows[i], c.warp_rows);
+    cl_max_rows[i] = c.max_part_rows;
+    cl_max_nnz[i] = c.max_part_nnz;
+    max_row = c.max_row;
+  }
   const SegmentSchedule sch = segment_schedule(a, seg_nnz, seg_per, kSegRows);
   seg_per_cta = seg_per;
   num_ctas = static_cast<int32_t>(sch.cta_row.size()) - 1;
@@ -123,6 +137,11 @@ void DevCsr::set_tile(int32_t threads) {
   blocks = tile_blocks[i].p;
   num_blocks = tile_num_blocks[i];
   tile_threads = threads;
+}
+
+ClusterRows DevCsr::cluster_rows(int ctas) const {
+  const int i = ctas == 16 ? 0 : 1;
+  return {cl_bounds[i].p, cl_warp_start[i].p, cl_warp_rows[i].p, cl_max_rows[i], cl_max_nnz[i]};
 }
 
 template <>
@@ -480,6 +499,8 @@ void validate_options(const anu_pdhg_options& o) {
   if (o.termination < 0 || o.termination > 2) throw Error(ANU_ERR_INVALID, "unknown termination");
   if (o.tile_threads != 0 && o.tile_threads != kTileThreads[0] && o.tile_threads != kTileThreads[1])
     throw Error(ANU_ERR_INVALID, "tile_threads must be 0 (tuned), 128 or 256");
+  if (o.cluster_chunks != 0 && o.cluster_chunks != 1)
+    throw Error(ANU_ERR_INVALID, "cluster_chunks must be 0 or 1");
 }
 
 // ------------------------------------------------------ product tiles
@@ -1158,6 +1179,23 @@ void run_polish(Problem& p, bool unit, const std::vector<const CaseData*>& paren
                                       states[which[w]].scales);
 }
 
+// The cluster size cluster_chunk_kernel takes a single LP on `p` with, 0
+// where it does not take it: options.cluster_chunks off, a packed batch's
+// LP, a row longer than kLongRow, or y and x_bar too large for one CTA's
+// shared memory.
+template <class T>
+int cluster_shape(Problem& p, const anu_pdhg_options& o) {
+  if (!o.cluster_chunks || p.concurrent || p.m == 0 || p.n == 0) return 0;
+  if (p.dk.max_row > kLongRow || p.dkt.max_row > kLongRow) return 0;
+  if (p.cluster_ctas < 0)
+    p.cluster_ctas =
+        cluster_ctas_for<T>(ClusterLayout::of<T>(p.m, p.n, p.dkt.cluster_rows(16),
+                                                 p.dk.cluster_rows(16)).total,
+                            ClusterLayout::of<T>(p.m, p.n, p.dkt.cluster_rows(8),
+                                                 p.dk.cluster_rows(8)).total);
+  return p.cluster_ctas;
+}
+
 template <class T>
 void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
                  const anu_pdhg_options& o, const std::vector<const std::vector<double>*>& warm_x,
@@ -1513,6 +1551,9 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
   // the rest.
   const bool persistent = o.persistent_chunks != 0 && !slow && o.use_graphs &&
                           chunk_fits<T>(p.dkt, p.dk, K);
+  // A single LP small enough runs each chunk as one cluster-resident launch
+  // (cluster_chunk_kernel); so does a stack's last case once compacted.
+  int cluster_c = (K == 1 && !persistent && !slow) ? cluster_shape<T>(p, o) : 0;
   DevBuf<uint32_t> sync_arrived;
   DevBuf<int32_t> sync_status;
   Pinned<int32_t> h_sync_status(persistent ? 1 : 0);
@@ -1586,6 +1627,18 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
                       GridSync{sync_arrived.p, reinterpret_cast<int*>(sync_status.p)});
       ANU_CUDA(cudaMemcpyAsync(h_sync_status.p, sync_status.p, sizeof(int32_t),
                                cudaMemcpyDeviceToHost, st));
+      return;
+    }
+    if (cluster_c > 0 && K == 1) {
+      PrimalEpi<T> pe{K, 0, base_flags, w.params.p, w.w_table.p, w.x.p, w.x.p, w.c.p, w.lo.p,
+                      w.hi.p, w.x_bar.p, w.anchor_x.p, w.dx.p, w.sum_x.p};
+      DualEpi<T> de{K, 0, base_flags, p.num_eq, w.params.p, w.w_table.p, w.y.p, w.y.p, w.q.p,
+                    w.kx.p, w.kx.p, w.anchor_y.p, w.anchor_kx.p, w.dy.p, nullptr, w.sum_y.p,
+                    ylo_ptr};
+      if (o.profile) ANU_CUDA(cudaEventRecord(ev_begin, st));
+      launch_cluster_chunk<T>(p, cluster_c, p.dkt.view<T>(), p.dkt.cluster_rows(cluster_c),
+                              p.dk.view<T>(), p.dk.cluster_rows(cluster_c), pe, de, len,
+                              base_flags, base_flags | (check_at_end ? kWriteDelta : 0u));
       return;
     }
     if (o.use_graphs) {
@@ -2133,6 +2186,7 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
     for (auto* v : {&vx, &vy, &vc, &vl, &vu, &vq, &oc, &ol, &ou, &oq}) pick(*v);
     K = K2;
     w.K = K2;
+    if (K == 1) cluster_c = cluster_shape<T>(p, o);
     NK = static_cast<size_t>(std::max(n, 1)) * K;
     MK = static_cast<size_t>(std::max(m, 1)) * K;
     ylo_ptr = any_ylo ? w.ylo.p : nullptr;
@@ -2841,6 +2895,7 @@ void anu_pdhg_default_options(anu_pdhg_options* o) {
   o->locality_order = 0;
   o->scaling_on_device = 1;
   o->tile_threads = 0;
+  o->cluster_chunks = 0;
 }
 
 int anu_last_error(char* buf, int32_t size) { return anu::copy_last_error(buf, size); }

@@ -171,8 +171,16 @@ struct DevCsr {
   // kSegPerCtaMax segments per CTA).
   void upload(const HostCsr& a, bool with_fp32, cudaStream_t s, int32_t seg_nnz = kSegNnz,
               int32_t seg_per_cta = kSegPerCta);
+  // Row schedules of the cluster-resident single-LP chunk
+  // (cluster_chunk_kernel) for clusters of 16 and of 8 CTAs, and the
+  // longest row.
+  DevBuf<int32_t> cl_bounds[2], cl_warp_start[2], cl_warp_rows[2];
+  int32_t cl_max_rows[2] = {0, 0}, cl_max_nnz[2] = {0, 0};  // per CTA
+  int32_t max_row = 0;
   // Selects the single-LP product tile of `threads` (one of kTileThreads).
   void set_tile(int32_t threads);
+  // The cluster schedule for clusters of `ctas` (16 or 8) CTAs.
+  ClusterRows cluster_rows(int ctas) const;
   template <class V>
   CsrView<V> view() const;
 };
@@ -217,6 +225,9 @@ struct Problem : Exec {
   // its single-LP checks launch directly, on one stream, instead of as
   // graphs with a second branch.
   bool concurrent = false;
+  // CTAs per cluster cluster_chunk_kernel runs with on this problem (16, 8,
+  // or 0 where it does not fit); -1 until first asked.
+  int cluster_ctas = -1;
   ~Problem();
 };
 

@@ -205,9 +205,10 @@ struct PrimalEpi {
     r.sum = (flags & kAccumulate) ? sum_x[e] : static_cast<T>(0);
     return r;
   }
-  __device__ __forceinline__ void finish(int32_t j, int32_t k, T kty, const Pre& r) const {
+  // Returns the new x_bar entry (0 for a retired case).
+  __device__ __forceinline__ T finish(int32_t j, int32_t k, T kty, const Pre& r) const {
     const StepParams& P = p[k];
-    if (!P.active) return;
+    if (!P.active) return static_cast<T>(0);
     const size_t e = (size_t)j * K + k;
     const T xj = r.x;
     T v = sub(xj, mul(static_cast<T>(P.tau), sub(r.c, kty)));
@@ -215,7 +216,8 @@ struct PrimalEpi {
     if (v > r.hi) v = r.hi;
     const T d = sub(v, xj);
     if (flags & kWriteDelta) dx[e] = d;
-    x_bar[e] = add(v, d);
+    const T xb = add(v, d);
+    x_bar[e] = xb;
     T next = v;
     if (P.gamma != 0.0) next = add(next, mul(static_cast<T>(P.gamma), d));
     const bool reset_now = P.reset_pending && it == 0;
@@ -226,6 +228,7 @@ struct PrimalEpi {
     x_out[e] = next;
     if (P.halpern && reset_now) anchor[e] = next;
     if (flags & kAccumulate) sum_x[e] = add(r.sum, mul(static_cast<T>(P.eta), next));
+    return xb;
   }
   __device__ __forceinline__ void operator()(int32_t j, int32_t k, T kty) const {
     finish(j, k, kty, prefetch(j, k));
@@ -279,9 +282,10 @@ struct DualEpi {
     r.sum = (flags & kAccumulate) ? sum_y[e] : static_cast<T>(0);
     return r;
   }
-  __device__ __forceinline__ void finish(int32_t i, int32_t k, T bar, const Pre& r) const {
+  // Returns the new y entry (0 for a retired case).
+  __device__ __forceinline__ T finish(int32_t i, int32_t k, T bar, const Pre& r) const {
     const StepParams& P = p[k];
-    if (!P.active) return;
+    if (!P.active) return static_cast<T>(0);
     const size_t e = (size_t)i * K + k;
     const T yi = r.y;
     const T kx = r.kx;
@@ -314,6 +318,7 @@ struct DualEpi {
       anchor_kx[e] = next_k;
     }
     if (flags & kAccumulate) sum_y[e] = add(r.sum, mul(static_cast<T>(P.eta), next_y));
+    return next_y;
   }
   __device__ __forceinline__ void operator()(int32_t i, int32_t k, T bar) const {
     finish(i, k, bar, prefetch(i, k));

@@ -9,6 +9,7 @@
 #include <atomic>
 #include <cstdint>
 
+#include "cluster.cuh"
 #include "kernels.cuh"
 
 namespace anu {
@@ -209,6 +210,79 @@ void launch_chunk(Exec& p, const Mat& kt, const Mat& k, const T* y, const T* x_b
     cuda_check(cudaLaunchKernelEx(&cfg, chunk_kernel<T, 2>, vt, vk, y, x_bar, K, len, flags,
                                   last_flags, pe, de, sync),
                "chunk_kernel launch");
+  ++p.launches;
+}
+
+// ------------------------------------------ cluster-resident single-LP chunks
+
+// The most dynamic shared memory cluster_chunk_kernel asks for: its copies of
+// y and x_bar and its slices of the two matrices (ClusterLayout).
+constexpr size_t kClusterSmemMax = 200 * 1024;
+
+// The CTAs per cluster the device runs cluster_chunk_kernel<., T> with: 16
+// where a 16-CTA cluster with smem16 bytes of dynamic shared memory per CTA
+// fits (a non-portable size), else 8 with smem8 bytes, else 0.
+template <class T>
+int cluster_ctas_for(size_t smem16, size_t smem8) {
+  auto fits = [&](auto kernel, int ctas, size_t smem) {
+    if (smem > kClusterSmemMax) return false;
+    if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(kClusterSmemMax)) != cudaSuccess ||
+        (ctas > 8 &&
+         cudaFuncSetAttribute(kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+             cudaSuccess)) {
+      cudaGetLastError();
+      return false;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(ctas);
+    cfg.blockDim = dim3(kClusterThreads);
+    cfg.dynamicSmemBytes = smem;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = ctas;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int clusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&clusters, kernel, &cfg) != cudaSuccess) {
+      cudaGetLastError();
+      return false;
+    }
+    return clusters >= 1;
+  };
+  if (fits(cluster_chunk_kernel<16, T>, 16, smem16)) return 16;
+  if (fits(cluster_chunk_kernel<8, T>, 8, smem8)) return 8;
+  return 0;
+}
+
+// `len` iterations of one LP as one launch of one cluster of `ctas` CTAs
+// (from cluster_ctas_for); the schedules must be the ones for that size.
+template <class T>
+void launch_cluster_chunk(Exec& p, int ctas, const CsrView<T>& kt, const ClusterRows& ktr,
+                          const CsrView<T>& k, const ClusterRows& kr, const PrimalEpi<T>& pe,
+                          const DualEpi<T>& de, int len, uint32_t flags, uint32_t last_flags) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(ctas);
+  cfg.blockDim = dim3(kClusterThreads);
+  cfg.dynamicSmemBytes = ClusterLayout::of<T>(k.rows, kt.rows, ktr, kr).total;
+  cfg.stream = p.stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = ctas;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  if (ctas == 16)
+    cuda_check(cudaLaunchKernelEx(&cfg, cluster_chunk_kernel<16, T>, kt, ktr, k, kr, pe, de, len,
+                                  flags, last_flags),
+               "cluster_chunk_kernel launch");
+  else
+    cuda_check(cudaLaunchKernelEx(&cfg, cluster_chunk_kernel<8, T>, kt, ktr, k, kr, pe, de, len,
+                                  flags, last_flags),
+               "cluster_chunk_kernel launch");
   ++p.launches;
 }
 

@@ -225,4 +225,30 @@ SegmentSchedule segment_schedule(const HostCsr& a, int32_t seg_nnz, int32_t seg_
   return s;
 }
 
+ClusterSchedule cluster_schedule(const HostCsr& a, int32_t parts, int32_t serial_row) {
+  ClusterSchedule c;
+  c.bounds.assign(static_cast<size_t>(parts) + 1, a.rows);
+  c.bounds[0] = 0;
+  const int64_t total = a.nnz();
+  int32_t part = 1;
+  for (int32_t r = 0; r < a.rows && part < parts; ++r) {
+    // Part `part` starts at the first row whose nonzeros begin at or past
+    // its share; a row never splits.
+    while (part < parts && static_cast<int64_t>(a.start[r]) * parts >= total * part)
+      c.bounds[part++] = r;
+  }
+  c.warp_start.assign(static_cast<size_t>(parts) + 1, 0);
+  for (int32_t q = 0; q < parts; ++q) {
+    for (int32_t r = c.bounds[q]; r < c.bounds[q + 1]; ++r) {
+      const int32_t len = a.start[r + 1] - a.start[r];
+      c.max_row = std::max(c.max_row, len);
+      if (len > serial_row) c.warp_rows.push_back(r);
+    }
+    c.warp_start[q + 1] = static_cast<int32_t>(c.warp_rows.size());
+    c.max_part_rows = std::max(c.max_part_rows, c.bounds[q + 1] - c.bounds[q]);
+    c.max_part_nnz = std::max(c.max_part_nnz, a.start[c.bounds[q + 1]] - a.start[c.bounds[q]]);
+  }
+  return c;
+}
+
 }  // namespace anu

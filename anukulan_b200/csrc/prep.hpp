@@ -89,6 +89,20 @@ struct SegmentSchedule {
 SegmentSchedule segment_schedule(const HostCsr& a, int32_t seg_nnz, int32_t seg_per_cta,
                                  int32_t row_max);
 
+// The rows of a matrix dealt to the `parts` CTAs of one thread-block cluster
+// (see cluster_chunk_kernel): contiguous ranges, cut where the running
+// nonzero count crosses each part's even share. Rows of more than
+// serial_row nonzeros are summed by a warp; each part lists its own.
+struct ClusterSchedule {
+  std::vector<int32_t> bounds;      // parts + 1 row bounds
+  std::vector<int32_t> warp_start;  // parts + 1 offsets into warp_rows
+  std::vector<int32_t> warp_rows;   // the rows longer than serial_row, by part
+  int32_t max_row = 0;              // longest row
+  int32_t max_part_rows = 0;        // most rows in one part
+  int32_t max_part_nnz = 0;         // most nonzeros in one part
+};
+ClusterSchedule cluster_schedule(const HostCsr& a, int32_t parts, int32_t serial_row);
+
 double now_seconds();
 
 }  // namespace anu

@@ -203,6 +203,16 @@ typedef struct anu_pdhg_options {
    * size sums every row in the same order, so the choice changes timing
    * only, never a result. The result reports the pair and the trial time. */
   int32_t tile_threads;
+  /* 1: a single LP (or the last case of a stack) whose y, x_bar, matrix
+   * slices and step vectors fit in the shared memory of a cluster's CTAs,
+   * with no row longer than 1,024 nonzeros, runs each check period as ONE
+   * launch of one thread-block cluster of 16 CTAs (8 where 16 does not fit)
+   * that stays resident for the period's iterations, instead of two
+   * launches per iteration. Rows are summed in the same order, so the
+   * iterates are the same bit for bit. Packed batches keep two launches per
+   * iteration. 0 (default): two launches per iteration; measured faster on
+   * the LPs the engine is benchmarked on. */
+  int32_t cluster_chunks;
 } anu_pdhg_options;
 
 /* PdhgResidual, src/anukulan/pdhg.hpp:429-496. */

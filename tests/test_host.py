@@ -133,7 +133,8 @@ def test_defaults_match_reference_pdhg_options():
     mine = abi.options_dict(abi.make_options())
     for k, v in ref.items():
         if k in ("precision", "refinement", "device", "use_graphs", "profile", "split_stacks",
-                 "persistent_chunks", "locality_order", "scaling_on_device"):
+                 "persistent_chunks", "locality_order", "scaling_on_device", "tile_threads",
+                 "cluster_chunks"):
             continue
         assert mine[k] == v, k
 
