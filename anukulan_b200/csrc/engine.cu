@@ -102,20 +102,6 @@ void DevCsr::upload(const HostCsr& a, bool with_fp32, cudaStream_t s, int32_t se
                                cudaMemcpyHostToDevice, s));
   }
   set_tile(kRowThreads);
-  auto put_rows = [&](DevBuf<int32_t>& d, const std::vector<int32_t>& h) {
-    d.alloc(std::max<size_t>(h.size(), 1));
-    if (!h.empty())
-      ANU_CUDA(cudaMemcpyAsync(d.p, h.data(), sizeof(int32_t) * h.size(), cudaMemcpyHostToDevice, s));
-  };
-  for (int i = 0; i < 2; ++i) {
-    const ClusterSchedule c = cluster_schedule(a, i == 0 ? 16 : 8, kSerialRow);
-    put_rows(cl_bounds[i], c.bounds);
-    put_rows(cl_warp_start[i], c.warp_start);
-    put_rows(cl_warp_rows[i], c.warp_rows);
-    cl_max_rows[i] = c.max_part_rows;
-    cl_max_nnz[i] = c.max_part_nnz;
-    max_row = c.max_row;
-  }
   const SegmentSchedule sch = segment_schedule(a, seg_nnz, seg_per, kSegRows);
   seg_per_cta = seg_per;
   num_ctas = static_cast<int32_t>(sch.cta_row.size()) - 1;
@@ -137,6 +123,26 @@ void DevCsr::set_tile(int32_t threads) {
   blocks = tile_blocks[i].p;
   num_blocks = tile_num_blocks[i];
   tile_threads = threads;
+}
+
+void DevCsr::prepare_cluster(const HostCsr& a, cudaStream_t s) {
+  if (cl_ready) return;
+  auto put_rows = [&](DevBuf<int32_t>& d, const std::vector<int32_t>& h) {
+    d.alloc(std::max<size_t>(h.size(), 1));
+    if (!h.empty())
+      ANU_CUDA(cudaMemcpyAsync(d.p, h.data(), sizeof(int32_t) * h.size(), cudaMemcpyHostToDevice, s));
+  };
+  for (int i = 0; i < 2; ++i) {
+    const ClusterSchedule c = cluster_schedule(a, i == 0 ? 16 : 8, kSerialRow);
+    put_rows(cl_bounds[i], c.bounds);
+    put_rows(cl_warp_start[i], c.warp_start);
+    put_rows(cl_warp_rows[i], c.warp_rows);
+    cl_max_rows[i] = c.max_part_rows;
+    cl_max_nnz[i] = c.max_part_nnz;
+    max_row = c.max_row;
+  }
+  ANU_CUDA(cudaStreamSynchronize(s));
+  cl_ready = true;
 }
 
 ClusterRows DevCsr::cluster_rows(int ctas) const {
@@ -1186,6 +1192,8 @@ void run_polish(Problem& p, bool unit, const std::vector<const CaseData*>& paren
 template <class T>
 int cluster_shape(Problem& p, const anu_pdhg_options& o) {
   if (!o.cluster_chunks || p.concurrent || p.m == 0 || p.n == 0) return 0;
+  p.dk.prepare_cluster(p.k, p.stream);
+  p.dkt.prepare_cluster(p.kt, p.stream);
   if (p.dk.max_row > kLongRow || p.dkt.max_row > kLongRow) return 0;
   if (p.cluster_ctas < 0)
     p.cluster_ctas =

@@ -173,10 +173,12 @@ struct DevCsr {
               int32_t seg_per_cta = kSegPerCta);
   // Row schedules of the cluster-resident single-LP chunk
   // (cluster_chunk_kernel) for clusters of 16 and of 8 CTAs, and the
-  // longest row.
+  // longest row; built by prepare_cluster on first use.
   DevBuf<int32_t> cl_bounds[2], cl_warp_start[2], cl_warp_rows[2];
   int32_t cl_max_rows[2] = {0, 0}, cl_max_nnz[2] = {0, 0};  // per CTA
   int32_t max_row = 0;
+  bool cl_ready = false;
+  void prepare_cluster(const HostCsr& a, cudaStream_t s);
   // Selects the single-LP product tile of `threads` (one of kTileThreads).
   void set_tile(int32_t threads);
   // The cluster schedule for clusters of `ctas` (16 or 8) CTAs.
