@@ -982,16 +982,22 @@ struct Workspace {
   }
 };
 
+// Case k's vector src[k] into dst, element (i, k) at i*K + k. The host
+// staging is written in order (each case's vector is read sequentially), and
+// the copy from pageable memory returns once the staging has been taken, so
+// the buffer may go at once (the copy stays ordered on the stream).
 template <class T>
 void upload_interleaved(cudaStream_t s, DevBuf<T>& dst, int32_t len, int K,
                         const std::vector<const std::vector<double>*>& src) {
   std::vector<T> h(static_cast<size_t>(len) * K);
-  for (int k = 0; k < K; ++k)
-    for (int32_t i = 0; i < len; ++i) h[static_cast<size_t>(i) * K + k] = static_cast<T>((*src[k])[i]);
+  std::vector<const double*> col(K);
+  for (int k = 0; k < K; ++k) col[k] = src[k]->data();
+  T* out = h.data();
+  for (int32_t i = 0; i < len; ++i)
+    for (int k = 0; k < K; ++k) *out++ = static_cast<T>(col[k][i]);
   dst.alloc(std::max<size_t>(h.size(), 1));
   if (!h.empty())
     ANU_CUDA(cudaMemcpyAsync(dst.p, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice, s));
-  ANU_CUDA(cudaStreamSynchronize(s));
 }
 
 template <class T>
