@@ -973,6 +973,7 @@ struct Workspace {
     size_t partial2_n = 0;
     int64_t launches = 0;  // kernels in the graph
     int seen = 0;
+    int direct = 0;  // calls run directly (a packed batch's LP, see replay)
   };
   Replay check_replay, recenter_replay;
   ~Workspace() {
@@ -1793,12 +1794,15 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
   // the same arguments at every check, so one graph launch replaces a dozen
   // kernel launches. The first call runs directly and sizes the reduction
   // scratch; a graph whose scratch has since been reallocated is captured
-  // again. Not where the iterate buffers swap (the host-driven path), not in
-  // polishing sub-stacks, whose few checks would not repay the capture, and
-  // not for a single LP of a packed batch, where many host threads would
-  // capture and instantiate graphs at once.
+  // again. Not where the iterate buffers swap (the host-driven path), and not
+  // in polishing sub-stacks, whose few checks would not repay the capture. A
+  // single LP of a packed batch, where many host threads would capture and
+  // instantiate graphs at once, launches its first kConcurrentDirect checks
+  // directly: most of the batch's LPs end before that, and only the long
+  // ones capture.
   auto replay = [&](typename Workspace<T>::Replay& r, auto&& body) {
-    if (!o.use_graphs || slow || sub_run || (K == 1 && p.concurrent)) {
+    if (!o.use_graphs || slow || sub_run ||
+        (K == 1 && p.concurrent && r.direct++ < kConcurrentDirect)) {
       body();
       return;
     }

@@ -224,8 +224,8 @@ struct Problem : Exec {
   // otherwise); the power iteration's start vector follows it.
   std::vector<int32_t> col_old;
   // One of many problems that host threads solve at once (a packed batch):
-  // its single-LP checks launch directly, on one stream, instead of as
-  // graphs with a second branch.
+  // its single-LP checks run on one stream, without a second branch, and
+  // launch directly for the first kConcurrentDirect checks of a solve.
   bool concurrent = false;
   // CTAs per cluster cluster_chunk_kernel runs with on this problem (16, 8,
   // or 0 where it does not fit); -1 until first asked.
@@ -275,6 +275,10 @@ std::unique_ptr<Problem> clone_problem(const Problem& src);
 // Case stacks of at least this many cases run as two half-stacks at once,
 // unless they run persistent chunks.
 constexpr int kSplitStack = 16;
+
+// Checks a single LP of a packed batch launches directly before its check
+// graphs are captured.
+constexpr int kConcurrentDirect = 100;
 
 // Whether run_cases takes a stack of K cases on `p` through chunk_kernel.
 bool stack_runs_persistent(const Problem& p, int K, const anu_pdhg_options& o);
