@@ -1798,8 +1798,8 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
   // in polishing sub-stacks, whose few checks would not repay the capture. A
   // single LP of a packed batch, where many host threads would capture and
   // instantiate graphs at once, launches its first kConcurrentDirect checks
-  // directly: most of the batch's LPs end before that, and only the long
-  // ones capture.
+  // directly: about half of a batch's LPs end before that, and only the
+  // longer ones capture.
   auto replay = [&](typename Workspace<T>::Replay& r, auto&& body) {
     if (!o.use_graphs || slow || sub_run ||
         (K == 1 && p.concurrent && r.direct++ < kConcurrentDirect)) {
