@@ -64,7 +64,11 @@ TOL = 1e-6
 STACK_GAP_TOL = 5e-7
 STACK_OPTS = dict(tolerance=TOL, gap_tolerance=STACK_GAP_TOL)
 # Side legs of the default stack line, in the order they run.
-SIDE_LEGS = ("spmv", "fp64_single_case", "stream", "exact_stack", "adjoint", "packed", "powerlaw")
+SIDE_LEGS = ("spmv", "fp64_single_case", "stream", "exact_stack", "adjoint", "packed", "powerlaw",
+             "powerlaw_1e8")
+# The power-law LP toward relative KKT 1e-8 (FP32 with refinement, relabelled)
+# under this time cap: the leg reports how far it got.
+POWERLAW_1E8_SECONDS = 45.0
 # DRAM bytes (read + write) per fused seg_kernel launch of 30 cases (one
 # half of the split stack), mean of the primal and dual kernels, from one
 # cold-cache ncu capture (profiles/seg_kernel_refinery_stack.md): 3.04 MB
@@ -850,6 +854,9 @@ def run_engine(args, rank, world, local_rank):
         if "powerlaw" in legs:
             out["powerlaw"] = powerlaw_leg(local_rank, TOL, ["fp32", "fp64"], 1, 300.0, peak,
                                            cpu=args.cpu_baseline)
+        if "powerlaw_1e8" in legs:
+            out["powerlaw_1e8"] = powerlaw_leg(local_rank, 1e-8, ["fp32"], 1,
+                                               POWERLAW_1E8_SECONDS, peak, cpu=False)
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
