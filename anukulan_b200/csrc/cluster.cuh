@@ -50,6 +50,9 @@ namespace anu {
 // CTAs per cluster: 16 (the non-portable maximum) where the device takes a
 // cluster of that size with this shared memory, else 8. Threads per CTA.
 constexpr int kClusterThreads = 256;
+// The longest chunk the kernel takes: its Halpern weights sit in shared
+// memory.
+constexpr int kClusterMaxLen = 1024;
 
 // One matrix's share of the cluster: row bounds per CTA and each CTA's
 // warp-summed rows.
@@ -68,7 +71,7 @@ struct ClusterLayout {
   // ep, ed: the step vectors of the CTA's own columns and rows, kStepVectors
   // arrays of max_rows entries each (StepSlice).
   static constexpr int kStepVectors = 8;
-  size_t ys, xbs, vt, vk, ep, ed, st, it, sk, ik, total;
+  size_t ys, xbs, wt, vt, vk, ep, ed, st, it, sk, ik, total;
   template <class T>
   __host__ __device__ static ClusterLayout of(int32_t m, int32_t n, const ClusterRows& ktr,
                                               const ClusterRows& kr) {
@@ -76,7 +79,8 @@ struct ClusterLayout {
     ClusterLayout l{};
     l.ys = 0;
     l.xbs = up(l.ys + sizeof(T) * m);
-    l.vt = up(l.xbs + sizeof(T) * n);
+    l.wt = up(l.xbs + sizeof(T) * n);
+    l.vt = up(l.wt + sizeof(double) * kClusterMaxLen);
     l.vk = up(l.vt + sizeof(T) * ktr.max_nnz);
     l.ep = up(l.vk + sizeof(T) * kr.max_nnz);
     l.ed = up(l.ep + sizeof(T) * kStepVectors * ktr.max_rows);
@@ -304,7 +308,8 @@ __device__ __forceinline__ void dual_out(const DualEpi<T>& g, const T* s, int32_
   }
 }
 
-// `len` iterations of one LP: K~'y with the primal step, then K~ x_bar with
+// `len` (at most kClusterMaxLen) iterations of one LP: K~'y with the primal
+// step, then K~ x_bar with
 // the dual step, on one cluster of C CTAs (the launch sets the cluster
 // shape). pe and de carry the chunk's first iteration; `flags` is every
 // iteration's epilogue flags, `last_flags` the last one's. Dynamic shared
@@ -334,6 +339,11 @@ __global__ void __launch_bounds__(kClusterThreads)
   T* ed = reinterpret_cast<T*>(cluster_smem + l.ed);
   PrimalEpi<T> lpe = primal_in_smem(pe, ep, ktr.max_rows, st.rb, st.re, accumulate);
   DualEpi<T> lde = dual_in_smem(de, ed, kr.max_rows, sk.rb, sk.re, accumulate);
+  // The chunk's Halpern weights (one case: one per iteration).
+  double* wt = reinterpret_cast<double*>(cluster_smem + l.wt);
+  for (int32_t i = threadIdx.x; i < len; i += kClusterThreads) wt[i] = pe.w_table[i];
+  lpe.w_table = wt;
+  lde.w_table = wt;
   // Every CTA of the cluster is running, and every local copy and slice is
   // filled, before any CTA stores into another's shared memory.
   cluster_barrier();

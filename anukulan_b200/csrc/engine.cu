@@ -1644,7 +1644,7 @@ void run_cases_t(Problem& p, const std::vector<const CaseData*>& initial_cases,
                                cudaMemcpyDeviceToHost, st));
       return;
     }
-    if (cluster_c > 0 && K == 1) {
+    if (cluster_c > 0 && K == 1 && len <= kClusterMaxLen) {
       PrimalEpi<T> pe{K, 0, base_flags, w.params.p, w.w_table.p, w.x.p, w.x.p, w.c.p, w.lo.p,
                       w.hi.p, w.x_bar.p, w.anchor_x.p, w.dx.p, w.sum_x.p};
       DualEpi<T> de{K, 0, base_flags, p.num_eq, w.params.p, w.w_table.p, w.y.p, w.y.p, w.q.p,
