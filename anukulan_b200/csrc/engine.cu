@@ -528,7 +528,10 @@ bool choose_tiles(Problem& p, const anu_pdhg_options& o, const CaseData* trial) 
       p.k.nnz() < kTuneNnz)
     return false;
   anu_pdhg_options t = o;
-  t.max_iterations = kTuneChunks * o.termination_check_frequency;
+  // Chunks of at most 64 iterations, so a long check period does not make
+  // the trials long.
+  t.termination_check_frequency = std::min<int32_t>(o.termination_check_frequency, 64);
+  t.max_iterations = kTuneChunks * t.termination_check_frequency;
   t.tolerance = 0.0;  // runs the whole budget
   t.profile = 1;
   t.verbose = 0;
