@@ -164,6 +164,19 @@ def test_library_version_and_no_fallback_without_device():
     assert e.value.code == 3  # ANU_ERR_NO_DEVICE: no CPU fallback
 
 
+@pytest.mark.parametrize("bad", [dict(tile_threads=64), dict(tile_threads=512),
+                                 dict(cluster_chunks=2), dict(cluster_chunks=-1)])
+def test_engine_options_validated_before_any_device_work(bad):
+    """The C ABI checks the engine's own options first, with or without a
+    device: an invalid tile size or cluster switch is ANU_ERR_INVALID."""
+    from anukulan_b200 import pdhg
+    lp = lp_cases.standard(lp_cases.wyndor())
+    with pytest.raises(pdhg.EngineError) as e:
+        pdhg.solve_pdhg(lp, max_iterations=10, **bad)
+    assert e.value.code == 1
+    assert next(iter(bad)) in str(e.value)
+
+
 def test_struct_layout_roundtrip():
     # The C library writes its defaults into the ctypes struct; a layout
     # mismatch would scramble the fields checked above. Check sizes agree
