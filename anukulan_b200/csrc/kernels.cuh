@@ -637,10 +637,18 @@ __global__ void __launch_bounds__(kMaxThreads)
   }
   const int32_t items = (r1 - r0) * K;
   typename Epi::Pre pre[kPrefetch];
+  // The segment range of each prefetched item's row, also schedule data.
+  int32_t g_lo[kPrefetch], g_hi[kPrefetch];
 #pragma unroll
   for (int q = 0; q < kPrefetch; ++q) {
     const int32_t t = threadIdx.x + q * threads;
-    if (t < items) pre[q] = epi.prefetch(r0 + t / K, t % K);
+    g_lo[q] = g_hi[q] = 0;
+    if (t < items) {
+      const int32_t row = r0 + t / K;
+      pre[q] = epi.prefetch(row, t % K);
+      g_lo[q] = a.row_seg[row];
+      g_hi[q] = a.row_seg[row + 1];
+    }
   }
   // Retired cases skip their gathers too, not only their epilogue: near the
   // end of a stack most lanes belong to retired cases. The per-case flags are
@@ -690,9 +698,20 @@ __global__ void __launch_bounds__(kMaxThreads)
   for (int32_t t = threadIdx.x, q = 0; t < items; t += threads, ++q) {
     const int32_t row = r0 + t / K;
     const int32_t k = t % K;
+    int32_t lo = 0, hi = 0;
+    if (q < kPrefetch) {
+#pragma unroll
+      for (int qq = 0; qq < kPrefetch; ++qq)
+        if (qq == q) {
+          lo = g_lo[qq];
+          hi = g_hi[qq];
+        }
+    } else {
+      lo = a.row_seg[row];
+      hi = a.row_seg[row + 1];
+    }
     Acc sum = 0;
-    for (int32_t g = a.row_seg[row]; g < a.row_seg[row + 1]; ++g)
-      sum = add(sum, part[(g - s0) * kMaxCaseLanes + k]);
+    for (int32_t g = lo; g < hi; ++g) sum = add(sum, part[(g - s0) * kMaxCaseLanes + k]);
     if (q < kPrefetch) {
       typename Epi::Pre r;
 #pragma unroll
