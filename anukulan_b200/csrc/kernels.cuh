@@ -394,6 +394,7 @@ __global__ void __launch_bounds__(kThreads)
   __shared__ Acc prod[Tile::kSlots];
   __shared__ Acc rowsum[Tile::kRows];
   __shared__ int32_t long_rows[Tile::kRows];
+  __shared__ int32_t long_b[Tile::kRows], long_e[Tile::kRows];  // their bounds in the block
   __shared__ int32_t warp_long[kWarps];
   const RowBlockDev blk = a.blocks[blockIdx.x];
   const int32_t r0 = blk.row_begin;
@@ -484,12 +485,17 @@ __global__ void __launch_bounds__(kThreads)
     if (w < warp) before += c;
     nlong += c;
   }
-  if (is_long) long_rows[before + __popc(ballot & ((1u << lane) - 1u))] = t;
+  if (is_long) {
+    const int32_t slot = before + __popc(ballot & ((1u << lane) - 1u));
+    long_rows[slot] = t;
+    long_b[slot] = rb;
+    long_e[slot] = re;
+  }
   __syncthreads();
   for (int32_t i = warp; i < nlong; i += kWarps) {
     const int32_t row = long_rows[i];
-    const int32_t b = a.start[r0 + row] - nz0;
-    const int32_t e = a.start[r0 + row + 1] - nz0;
+    const int32_t b = long_b[i];
+    const int32_t e = long_e[i];
     Acc s = 0;
     for (int32_t k = b + lane; k < e; k += 32) s = add(s, prod[prod_slot(k)]);
 #pragma unroll
