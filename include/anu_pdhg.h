@@ -32,6 +32,9 @@
 extern "C" {
 #endif
 
+/* 2: options.stop is a const volatile uint8_t* (std::atomic<bool>'s byte).
+ * 3: options.tile_threads and options.cluster_chunks; the result's
+ *    row_product_threads, column_product_threads and tile_trial_seconds. */
 #define ANU_PDHG_ABI_VERSION 3
 
 /* Return codes. */
