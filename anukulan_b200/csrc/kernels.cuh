@@ -188,6 +188,7 @@ struct PrimalEpi {
   // and are read again in finish().
   struct Pre {
     T x, c, lo, hi, anchor, sum;
+    double w;  // this iteration's Halpern weight (when blending)
   };
   // A retired case's lanes neither gather nor step.
   __device__ __forceinline__ bool live(int32_t k) const { return p[k].active != 0; }
@@ -202,6 +203,7 @@ struct PrimalEpi {
     r.hi = hi[e];
     const bool blend = P.halpern && !(P.reset_pending && it == 0);
     r.anchor = blend ? anchor[e] : static_cast<T>(0);
+    r.w = blend ? w_table[(size_t)it * K + k] : 1.0;
     r.sum = (flags & kAccumulate) ? sum_x[e] : static_cast<T>(0);
     return r;
   }
@@ -222,7 +224,7 @@ struct PrimalEpi {
     if (P.gamma != 0.0) next = add(next, mul(static_cast<T>(P.gamma), d));
     const bool reset_now = P.reset_pending && it == 0;
     if (P.halpern && !reset_now) {
-      const double w = w_table[(size_t)it * K + k];
+      const double w = r.w;
       next = add(mul(static_cast<T>(w), next), mul(static_cast<T>(1.0 - w), r.anchor));
     }
     x_out[e] = next;
@@ -264,6 +266,7 @@ struct DualEpi {
   // The row's vectors, loaded before the kernel waits on the product's input.
   struct Pre {
     T y, q, kx, anchor_y, anchor_kx, floor_v, sum;
+    double w;  // this iteration's Halpern weight (when blending)
   };
   // A retired case's lanes neither gather nor step.
   __device__ __forceinline__ bool live(int32_t k) const { return p[k].active != 0; }
@@ -279,6 +282,7 @@ struct DualEpi {
     const bool blend = P.halpern && !(P.reset_pending && it == 0);
     r.anchor_y = blend ? anchor_y[e] : static_cast<T>(0);
     r.anchor_kx = blend ? anchor_kx[e] : static_cast<T>(0);
+    r.w = blend ? w_table[(size_t)it * K + k] : 1.0;
     r.sum = (flags & kAccumulate) ? sum_y[e] : static_cast<T>(0);
     return r;
   }
@@ -305,7 +309,7 @@ struct DualEpi {
     }
     const bool reset_now = P.reset_pending && it == 0;
     if (P.halpern && !reset_now) {
-      const double w = w_table[(size_t)it * K + k];
+      const double w = r.w;
       const T wt = static_cast<T>(w);
       const T wc = static_cast<T>(1.0 - w);
       next_y = add(mul(wt, next_y), mul(wc, r.anchor_y));
